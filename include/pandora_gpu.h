@@ -1,0 +1,210 @@
+/*
+ * pandora_gpu.h -- C-ABI of the B200 (sm_100a) RK3 time step of the PANDORA 2.0
+ * pseudo-spectral DNS code.
+ *
+ * Plain C, no C++ or CUDA types.  Every entry point returns an int status
+ * (PANDORA_OK == 0, negative on error; pandora_strerror() names it).  The
+ * state that the reference keeps module-global (the f_arrays PETSc Vecs, the
+ * p_arrays particle arrays, bmat/binv in g_domain) lives in one handle, on one
+ * GPU, in HBM.  One handle per host thread; calls on one handle are not
+ * re-entrant; different handles are independent.
+ *
+ * Layout at the boundary is the reference's truncated spectral layout
+ * arr_u*_3w(0:1, k=0..2KK, j=0..2KJ, i=0..KI) (src/pf_arrays.f90:267-280):
+ * in C order [i][j][k][re,im], k fastest, KI = NODES_X/3, KJ = NODES_Y/3,
+ * KK = NODES_Z/3 (integer division, src/pg_domain.f90:220-231).  Negative
+ * wavenumbers sit at indices KJ+1..2KJ (resp. KK+1..2KK) and map to
+ * index-(2K+1) (src/pf_arrays.f90:1770-1804).  FP64 always at the boundary.
+ */
+#ifndef PANDORA_GPU_H
+#define PANDORA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (MPI_Abort sites of the reference become return codes) ---- */
+#define PANDORA_OK                 0
+#define PANDORA_ERR_INVALID_ARG   -1   /* bad pointer, size or parameter value      */
+#define PANDORA_ERR_OOM           -2   /* device allocation failed / budget exceeded */
+#define PANDORA_ERR_CUDA          -3   /* a CUDA runtime call failed                 */
+#define PANDORA_ERR_NAN           -4   /* non-finite value detected in the state     */
+#define PANDORA_ERR_TIMEOUT       -5   /* a bounded device wait gave up              */
+#define PANDORA_ERR_BAD_LAYOUT    -6   /* size not supported by the transform plan   */
+#define PANDORA_ERR_CFL           -7   /* RK3_CFL >= 1 (src/pg_rk3.f90:240-267)      */
+#define PANDORA_ERR_PARTICLE_LOST -8   /* wrap left a particle outside the domain
+                                          (src/pp_control.f90:1514-1518)             */
+#define PANDORA_ERR_NO_DEVICE     -9   /* no CUDA device / extension not usable      */
+#define PANDORA_ERR_UNSUPPORTED  -10   /* option not built in this library           */
+
+/* ---- enum values, identical to src/pg_parameters.f90 ---- */
+#define PANDORA_F_ISOTROPIC          1   /* pg_parameters.f90:131 */
+#define PANDORA_F_SHEAR_DNS          2   /* pg_parameters.f90:132 */
+#define PANDORA_F_ISOTROPIC_DEFORMED 5   /* pg_parameters.f90:135 */
+#define PANDORA_RK3_TIMESTEP_DECIDE  1   /* pg_parameters.f90:211 */
+#define PANDORA_RK3_TIMESTEP_FIXED   2   /* pg_parameters.f90:212 */
+#define PANDORA_RK3_TIMESTEP_CFL     3   /* pg_parameters.f90:213 */
+#define PANDORA_NS_BF_ROT            1   /* pg_parameters.f90:219 */
+#define PANDORA_DEALIASING_23        1   /* 2/3 rule (cube truncation)  */
+#define PANDORA_F_INIT_NULL          0   /* pg_parameters.f90:150 */
+#define PANDORA_F_INIT_GAUSS         3
+#define PANDORA_F_INIT_KERR          4
+#define PANDORA_F_INIT_PULSE         5
+#define PANDORA_F_INIT_SQUARE        6
+#define PANDORA_F_INIT_MINUSFIVETHIRD 8
+#define PANDORA_F_INIT_MATSUMOTO     9
+#define PANDORA_F_INIT_AHMED_ELGHOBASHI 10
+#define PANDORA_P_INIT_RANDOM        2   /* pg_parameters.f90:236 */
+#define PANDORA_PREC_FP64            0
+
+/*
+ * Namelist fields of ip_file.in that the RK3 step reads (src/pg_control.f90:385-436),
+ * mirrored one-to-one.  Seeds replace RANDOM_SEED_FLUID / RANDOM_SEED_PARTICLES:
+ * the reference draws from gfortran's random_number, which cannot be replayed here,
+ * so this library defines one counter-based generator (SplitMix64 finaliser over a
+ * stream index) that the oracle shares; draw ORDER follows the reference.
+ */
+typedef struct pandora_params {
+    /* nl_domain */
+    int32_t nodes_x, nodes_y, nodes_z;
+    int32_t b110, b220, b330;
+    /* nl_fluid */
+    double  f_rho, f_nu;
+    /* nl_flow */
+    int32_t f_type;
+    double  f_deform_s;
+    int32_t f_remesh_t;
+    /* nl_numerics */
+    int32_t rk3_timestep;
+    double  rk3_cfl, rk3_dt;
+    int32_t ns_deformed;
+    int32_t dealiasing;
+    /* nl_control */
+    int32_t tsteps;
+    /* nl_f_init */
+    int32_t f_init_type;
+    double  f_init_u0, f_init_kp, f_init_kv;
+    double  f_init_kstart, f_init_kend, f_init_epsilon;
+    /* nl_force */
+    double  force_tf, force_sigma, force_kf;
+    int32_t force_stop;
+    /* nl_particle / nl_part_properties */
+    int32_t p_track_part;
+    int32_t p_init_type;
+    int64_t p_np_global;
+    int32_t p_interp_order;
+    int32_t p_ts_release;
+    double  p_rho;
+    double  p_dia_vals;     /* single diameter level (P_DIA_LVLS = 1); 0 => tracers */
+    /* random seeds (see above) */
+    uint64_t seed_fluid, seed_force, seed_particles;
+    /* arithmetic of the step: PANDORA_PREC_FP64 */
+    int32_t precision;
+    int32_t reserved[7];
+} pandora_params;
+
+typedef struct pandora_handle pandora_handle;
+
+/* Fills *p with the defaults of conf/ip_file.in for the fields above. */
+int pandora_params_default(pandora_params* p);
+
+/* Library / device queries. */
+const char* pandora_strerror(int status);
+int pandora_device_count(int* count);
+
+/* Sizes of the truncated spectral layout: NKI = KI+1, NKJ = 2KJ+1, NKK = 2KK+1;
+ * S = NKI*NKJ*NKK complex modes per component; kkmax = number of E(k) shells
+ * (src/pf_fluidstats.f90:348-374). */
+int pandora_sizes(const pandora_params* p, int32_t* nki, int32_t* nkj, int32_t* nkk,
+                  int64_t* modes, int32_t* kkmax);
+
+/*
+ * Allocates the device state for one simulation on the current CUDA device
+ * (replaces ProgramInit's f_ArraysInit/f_FftwInit/f_ForceInit,
+ * src/pg_control.f90:52-146).  The state starts at zero.
+ */
+int pandora_create(const pandora_params* p, pandora_handle** out);
+int pandora_destroy(pandora_handle* h);
+
+/* Runs all of this handle's work on a caller-owned cudaStream_t (NULL: the
+ * handle's own stream). */
+int pandora_set_stream(pandora_handle* h, void* cuda_stream);
+
+/* ---- state in / out (host buffers, reference layout, synchronous) ---- */
+int pandora_set_state(pandora_handle* h, const double* u1, const double* u2, const double* u3);
+int pandora_get_state(pandora_handle* h, double* u1, double* u2, double* u3);
+/* RK3 low-storage registers rk3_3w_1..3 (src/pf_arrays.f90:67-72). */
+int pandora_set_rk(pandora_handle* h, const double* r1, const double* r2, const double* r3);
+int pandora_get_rk(pandora_handle* h, double* r1, double* r2, double* r3);
+/* OU forcing coefficients fluid_f1..3(0:1,-NK:NK,-NK:NK,0:NK) as [i][j][k][2]
+ * (src/pf_force.f90:289-300); n = 3 * (NK+1)*(2NK+1)^2 * 2 doubles in total. */
+int pandora_forcing_size(pandora_handle* h, int64_t* ndoubles_per_component);
+int pandora_set_forcing(pandora_handle* h, const double* f1, const double* f2, const double* f3);
+int pandora_get_forcing(pandora_handle* h, double* f1, double* f2, double* f3);
+/* Device pointers of u1..u3 (for zero-copy users; valid until destroy). */
+int pandora_state_device_ptrs(pandora_handle* h, void** u1, void** u2, void** u3);
+
+/* Seeded solenoidal initial field, f_InitialiseFluid (src/pf_initialise.f90:97-512),
+ * computed on the device. */
+int pandora_init_fluid(pandora_handle* h);
+
+/* ---- particles (p_arrays, src/pp_arrays.f90:92-429), SoA-free host view:
+ *      xp[3*np] = (x1,x2,x3) per particle, likewise up, up_rk3, rk3; dp[np]. */
+int pandora_set_particles(pandora_handle* h, int64_t np, const double* xp, const double* up,
+                          const double* up_rk3, const double* rk3, const double* dp);
+int pandora_get_particles(pandora_handle* h, int64_t np, double* xp, double* up,
+                          double* up_rk3, double* rk3, double* dp);
+/* P_INIT_RANDOM positions (src/pp_control.f90:663-707), on the device. */
+int pandora_init_particles(pandora_handle* h);
+
+/*
+ * One RK3 time step, g_RK3Calc (src/pg_rk3.f90:82-129): three stages, each
+ * f_RK3Stage{1,2,3} (src/pf_rk3.f90:40-200) including the E(k)/epsilon
+ * statistics at stage 1, forcing at every stage and the particle advance.
+ * On return *simtime = t0 + dt and *dt holds the step's dt (synchronous).
+ */
+int pandora_rk3_step(pandora_handle* h, int32_t tstep, double* simtime, double* dt);
+/* nsteps steps tstep0 .. tstep0+nsteps-1, enqueued on the stream without host
+ * synchronisation (simtime/dt live on the device); *simtime is updated when
+ * sync != 0. */
+int pandora_rk3_advance(pandora_handle* h, int32_t tstep0, int32_t nsteps, int32_t sync,
+                        double* simtime);
+/* One stage (1..3) of step tstep at time `time`; *dt in/out as in f_RK3Stage*. */
+int pandora_rk3_stage(pandora_handle* h, int32_t stage, int32_t tstep, double time, double* dt);
+
+/*
+ * Statistics of the current state, f_FluidstatsFsPrimaryQuants
+ * (src/pf_fluidstats.f90:1423-1576): ek[kkmax] = shell energy / mode density,
+ * *tke = 0.5 (u1u1+u2u2+u3u3), *eps = f_dis = sum 2 nu k^2 e(k).
+ * *ucfl = max |u1|+|u2|+|u3| of the last stage-1 physical field
+ * (src/pf_fluidstats.f90:913-917).  Any output pointer may be NULL.
+ */
+int pandora_stats(pandora_handle* h, double* ek, int32_t kkmax, double* tke, double* eps,
+                  double* ucfl);
+/* Statistics recorded at stage 1 of the most recent step (state at step start). */
+int pandora_last_step_stats(pandora_handle* h, double* ek, int32_t kkmax, double* tke,
+                            double* eps, double* ucfl);
+
+/* Nonlinear term omega x u of the current state in spectral layout (normalised),
+ * the product of f_RK3PrepareRealSpace + f_RK3RealSpace + the forward
+ * transforms (test hook of src/ptf_rk3.f90:1115-1191). */
+int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, double* n3);
+
+/* Physical-space velocity of the last stage (x fastest, [z][y][x]), as
+ * materialised for particle interpolation (arr_u*_3r, src/pf_rk3.f90:1108-1115). */
+int pandora_get_physical_velocity(pandora_handle* h, double* u1, double* u2, double* u3);
+
+/* Device status word: non-zero bits record NaN detection / bounded-wait timeouts /
+ * lost particles since the last call; clears it. */
+int pandora_check_status(pandora_handle* h);
+
+/* Number of kernel launches the last pandora_rk3_step/advance enqueued per step. */
+int pandora_launches_per_step(pandora_handle* h, int32_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PANDORA_GPU_H */
