@@ -111,8 +111,10 @@ typedef struct pandora_handle pandora_handle;
 /* Fills *p with the defaults of conf/ip_file.in for the fields above. */
 int pandora_params_default(pandora_params* p);
 
-/* Library / device queries. */
+/* Library / device queries.  pandora_params_sizeof() lets a binding check its
+ * mirror of the struct layout (ctypes, iso_c_binding). */
 const char* pandora_strerror(int status);
+int pandora_params_sizeof(void);
 int pandora_device_count(int* count);
 
 /* Sizes of the truncated spectral layout: NKI = KI+1, NKJ = 2KJ+1, NKK = 2KK+1;

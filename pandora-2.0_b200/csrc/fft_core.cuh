@@ -1,0 +1,240 @@
+// fft_core.cuh -- building blocks of the batched FP64 line FFTs of the RK3 step.
+//
+// The reference runs FFTW 1-D plans (src/pf_fftw.f90:199-291): c2c along z and y,
+// c2r/r2c along x, FFTW_BACKWARD (e^{+2 pi i kn/N}) unnormalised for
+// spectral->physical and FFTW_FORWARD (e^{-2 pi i kn/N}) for physical->spectral.
+// Here the same transforms are radix-R Stockham autosort passes (the formulation
+// of Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC 2008) over a tile of L lines held in shared memory
+// in column layout: element n of line l sits at s[n*LP + l] (LP >= L, odd pad
+// so that the transposing global<->shared copies are bank-conflict free).
+// Each pass: load R points of stride N/R, twiddle by W_{Ns R}^{r k}, R-point DFT
+// in registers, store at (j/Ns)*Ns*R + j%Ns + r*Ns.
+//
+// Everything here is __host__ __device__ so that the index arithmetic and the
+// small DFTs are exercised on the CPU by the unit test harness (fft_core_test.cpp)
+// before they run on a GPU.
+#pragma once
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#define PD_HD __host__ __device__ __forceinline__
+#else
+#include <cstddef>
+struct double2 { double x, y; };
+#define PD_HD inline
+#endif
+
+namespace pdfft {
+
+PD_HD double2 mk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
+PD_HD double2 add(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
+PD_HD double2 sub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
+PD_HD double2 scl(double2 a, double s) { return mk(a.x * s, a.y * s); }
+PD_HD double2 cmul(double2 a, double2 b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+PD_HD double2 cmulc(double2 a, double2 b) { return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }
+
+// Sign convention: a DFT of sign S computes X_r = sum_q x_q exp(S * 2 pi i q r / R);
+// S = -1 is FFTW_FORWARD, S = +1 is FFTW_BACKWARD.  Twiddle tables hold
+// tw[e] = exp(-2 pi i e / N); a sign-S pass multiplies by tw (S=-1) or conj(tw).
+template <int S> PD_HD double2 twmul(double2 a, double2 w) { return S < 0 ? cmul(a, w) : cmulc(a, w); }
+// a * (S i)
+template <int S> PD_HD double2 mul_si(double2 a) { return S > 0 ? mk(-a.y, a.x) : mk(a.y, -a.x); }
+// a * (c + S i s)
+template <int S> PD_HD double2 mul_cs(double2 a, double c, double s) {
+    const double ss = S > 0 ? s : -s;
+    return mk(a.x * c - a.y * ss, a.x * ss + a.y * c);
+}
+
+constexpr double kSqrtHalf = 0.7071067811865475244008444;
+constexpr double kSin60 = 0.8660254037844386467637232;
+
+template <int S> PD_HD void dft2(double2* v) {
+    double2 a = v[0], b = v[1];
+    v[0] = add(a, b); v[1] = sub(a, b);
+}
+template <int S> PD_HD void dft3(double2* v) {
+    double2 t = add(v[1], v[2]), d = sub(v[1], v[2]);
+    double2 m = sub(v[0], scl(t, 0.5));
+    double2 e = mul_si<S>(scl(d, kSin60));
+    v[0] = add(v[0], t);
+    v[1] = add(m, e);
+    v[2] = sub(m, e);
+}
+template <int S> PD_HD void dft4(double2* v) {
+    double2 a0 = add(v[0], v[2]), a1 = sub(v[0], v[2]);
+    double2 b0 = add(v[1], v[3]), b1 = mul_si<S>(sub(v[1], v[3]));
+    v[0] = add(a0, b0); v[2] = sub(a0, b0);
+    v[1] = add(a1, b1); v[3] = sub(a1, b1);
+}
+template <int S> PD_HD void dft8(double2* v) {
+    double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<S>(e); dft4<S>(o);
+    o[1] = mul_cs<S>(o[1], kSqrtHalf, kSqrtHalf);
+    o[2] = mul_si<S>(o[2]);
+    o[3] = mul_cs<S>(o[3], -kSqrtHalf, kSqrtHalf);
+#pragma unroll
+    for (int r = 0; r < 4; r++) { v[r] = add(e[r], o[r]); v[r + 4] = sub(e[r], o[r]); }
+}
+template <int S> PD_HD void dft16(double2* v) {
+    double2 e[8], o[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) { e[q] = v[2 * q]; o[q] = v[2 * q + 1]; }
+    dft8<S>(e); dft8<S>(o);
+    constexpr double c1 = 0.9238795325112867561281832, s1 = 0.38268343236508977172846;
+    o[1] = mul_cs<S>(o[1], c1, s1);
+    o[2] = mul_cs<S>(o[2], kSqrtHalf, kSqrtHalf);
+    o[3] = mul_cs<S>(o[3], s1, c1);
+    o[4] = mul_si<S>(o[4]);
+    o[5] = mul_cs<S>(o[5], -s1, c1);
+    o[6] = mul_cs<S>(o[6], -kSqrtHalf, kSqrtHalf);
+    o[7] = mul_cs<S>(o[7], -c1, s1);
+#pragma unroll
+    for (int r = 0; r < 8; r++) { v[r] = add(e[r], o[r]); v[r + 8] = sub(e[r], o[r]); }
+}
+// odd prime R (5, 7): X_r = v0 + sum_{q=1}^{(R-1)/2} [C(qr)(v_q + v_{R-q}) + S i S(qr)(v_q - v_{R-q})]
+template <int R> struct PrimeTab;
+template <> struct PrimeTab<5> {
+    static PD_HD double c(int m) {
+        return m == 0 ? 1.0 : (m == 1 || m == 4) ? 0.3090169943749474241022934 : -0.8090169943749474241022934;
+    }
+    static PD_HD double s(int m) {
+        return m == 0 ? 0.0 : m == 1 ? 0.9510565162951535721164393 : m == 2 ? 0.587785252292473129168706
+             : m == 3 ? -0.587785252292473129168706 : -0.9510565162951535721164393;
+    }
+};
+template <> struct PrimeTab<7> {
+    static PD_HD double c(int m) {
+        return m == 0 ? 1.0 : (m == 1 || m == 6) ? 0.6234898018587335305250049
+             : (m == 2 || m == 5) ? -0.2225209339563144042889026 : -0.9009688679024191262361023;
+    }
+    static PD_HD double s(int m) {
+        return m == 0 ? 0.0 : m == 1 ? 0.7818314824680298087084445 : m == 2 ? 0.9749279121818236070181317
+             : m == 3 ? 0.4338837391175581204757683 : m == 4 ? -0.4338837391175581204757683
+             : m == 5 ? -0.9749279121818236070181317 : -0.7818314824680298087084445;
+    }
+};
+template <int R, int S> PD_HD void dft_prime(double2* v) {
+    double2 sum[(R - 1) / 2], dif[(R - 1) / 2];
+#pragma unroll
+    for (int q = 1; q <= (R - 1) / 2; q++) { sum[q - 1] = add(v[q], v[R - q]); dif[q - 1] = sub(v[q], v[R - q]); }
+    double2 out[R];
+    double2 x0 = v[0];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        double2 acc = x0;
+#pragma unroll
+        for (int q = 1; q <= (R - 1) / 2; q++) {
+            const int m = (q * r) % R;
+            acc = add(acc, scl(sum[q - 1], PrimeTab<R>::c(m)));
+            acc = add(acc, mul_si<S>(scl(dif[q - 1], PrimeTab<R>::s(m))));
+        }
+        out[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = out[r];
+}
+
+template <int R, int S> PD_HD void dft(double2* v) {
+    if constexpr (R == 2) dft2<S>(v);
+    else if constexpr (R == 3) dft3<S>(v);
+    else if constexpr (R == 4) dft4<S>(v);
+    else if constexpr (R == 8) dft8<S>(v);
+    else if constexpr (R == 16) dft16<S>(v);
+    else if constexpr (R == 5 || R == 7) dft_prime<R, S>(v);
+    else static_assert(R == 2, "unsupported radix");
+}
+
+// Radix schedule per transform length.  Supported N: 2^a * {1,3,5,7} up to 1024 that
+// factor into the radices below in at most three passes.
+template <int N> struct Plan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
+#define PD_PLAN(N_, A, B, C) \
+    template <> struct Plan<N_> { static constexpr int r0 = A, r1 = B, r2 = C; };
+PD_PLAN(16, 16, 0, 0)
+PD_PLAN(24, 3, 8, 0)
+PD_PLAN(32, 8, 4, 0)
+PD_PLAN(40, 5, 8, 0)
+PD_PLAN(48, 3, 16, 0)
+PD_PLAN(56, 7, 8, 0)
+PD_PLAN(64, 8, 8, 0)
+PD_PLAN(80, 5, 16, 0)
+PD_PLAN(96, 3, 4, 8)
+PD_PLAN(112, 7, 16, 0)
+PD_PLAN(128, 8, 16, 0)
+PD_PLAN(160, 5, 4, 8)
+PD_PLAN(192, 3, 8, 8)
+PD_PLAN(224, 7, 4, 8)
+PD_PLAN(256, 16, 16, 0)
+PD_PLAN(320, 5, 8, 8)
+PD_PLAN(384, 3, 8, 16)
+PD_PLAN(448, 7, 8, 8)
+PD_PLAN(512, 8, 8, 8)
+PD_PLAN(640, 5, 8, 16)
+PD_PLAN(768, 3, 16, 16)
+PD_PLAN(896, 7, 8, 16)
+PD_PLAN(1024, 16, 8, 8)
+#undef PD_PLAN
+
+template <int N> constexpr bool plan_ok() {
+    return Plan<N>::r0 * (Plan<N>::r1 ? Plan<N>::r1 : 1) * (Plan<N>::r2 ? Plan<N>::r2 : 1) == N;
+}
+
+// One pass, split into a load/compute half and a store half so that a CPU
+// emulator can run all items' first halves before any second half (that is
+// what the __syncthreads() between them does on the GPU).
+template <int N, int R, int NS, int S, int L, int LP>
+PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
+    constexpr int NR = N / R;
+    const int l = w % L, j = w / L;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = s[(j + r * NR) * LP + l];
+    if constexpr (NS > 1) {
+        const int k = j % NS;
+        constexpr int step = N / (NS * R);
+#pragma unroll
+        for (int r = 1; r < R; r++) v[r] = twmul<S>(v[r], tw[r * k * step]);
+    }
+    dft<R, S>(v);
+}
+template <int N, int R, int NS, int L, int LP>
+PD_HD void pass_store(double2* s, int w, const double2* v) {
+    const int l = w % L, j = w / L;
+    const int k = j % NS;
+    const int d = (j / NS) * NS * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) s[(d + r * NS) * LP + l] = v[r];
+}
+
+#if defined(__CUDACC__)
+// In-place pass over a [N][LP] shared tile with NT threads; items w = tid + it*NT.
+template <int N, int R, int NS, int S, int L, int LP, int NT>
+__device__ __forceinline__ void pass(double2* s, const double2* __restrict__ tw, int tid) {
+    constexpr int WORK = (N / R) * L;
+    constexpr int IT = (WORK + NT - 1) / NT;
+    double2 v[IT][R];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = tid + it * NT;
+        if (WORK % NT == 0 || w < WORK) pass_load<N, R, NS, S, L, LP>(s, tw, w, v[it]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = tid + it * NT;
+        if (WORK % NT == 0 || w < WORK) pass_store<N, R, NS, L, LP>(s, w, v[it]);
+    }
+    __syncthreads();
+}
+
+// Full length-N transform of L lines of the tile (caller syncs before).
+template <int N, int S, int L, int LP, int NT>
+__device__ __forceinline__ void fft_tile(double2* s, const double2* __restrict__ tw, int tid) {
+    static_assert(plan_ok<N>(), "no radix plan for this length");
+    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+    pass<N, R0, 1, S, L, LP, NT>(s, tw, tid);
+    if constexpr (R1 != 0) pass<N, R1, R0, S, L, LP, NT>(s, tw, tid);
+    if constexpr (R2 != 0) pass<N, R2, R0 * R1, S, L, LP, NT>(s, tw, tid);
+}
+#endif
+
+}  // namespace pdfft

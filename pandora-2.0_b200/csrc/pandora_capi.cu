@@ -1,0 +1,635 @@
+// pandora_capi.cu -- the extern "C" boundary (include/pandora_gpu.h).
+//
+// Replaces the module-global state and the stage sequencing of g_RK3Calc /
+// f_RK3Stage{1,2,3} (src/pg_rk3.f90:82-129, src/pf_rk3.f90:40-200): one handle
+// owns the resident device fields, the twiddle tables, the clock scalars and a
+// CUDA graph that holds one whole time step.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <new>
+#include <vector>
+#include "pandora_internal.cuh"
+
+using namespace pd;
+
+struct pandora_handle {
+    pandora_params p;
+    Geo g;
+    int dev = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t st = nullptr;
+    Fields F{};
+    double2* fbuf = nullptr;          // u[3], rk[3] contiguous
+    double2* tw = nullptr;            // tw_x | tw_y | tw_z
+    Clock* clock = nullptr;
+    Clock* clock_host = nullptr;      // pinned mirror
+    double* shell_step = nullptr;     // stats of the state at stage 1 of the last step
+    double* shell_now = nullptr;      // stats of pandora_stats()
+    double* shell_host = nullptr;     // pinned
+    std::vector<double> dens_mod;     // [kkmax + 1]
+    long long nforce = 0;             // complex entries per forcing component
+    StepParams sp{};
+    ForceParams fp{};
+    PartParams pp{};
+    Particles P{};
+    double* pbuf = nullptr;
+    double2* nlbuf = nullptr;         // scratch for pandora_nonlinear
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool use_graph = true;
+    int launches_per_step = 0;
+    bool particles_on = false;
+};
+
+static thread_local char g_errmsg[256];
+
+static int cuda_fail(cudaError_t e, const char* where) {
+    snprintf(g_errmsg, sizeof(g_errmsg), "%s: %s", where, cudaGetErrorString(e));
+    return PANDORA_ERR_CUDA;
+}
+#define PD_CK(x)                                          \
+    do {                                                  \
+        cudaError_t _e = (x);                             \
+        if (_e != cudaSuccess) return cuda_fail(_e, #x);  \
+    } while (0)
+
+extern "C" const char* pandora_strerror(int s) {
+    switch (s) {
+    case PANDORA_OK: return "ok";
+    case PANDORA_ERR_INVALID_ARG: return "invalid argument";
+    case PANDORA_ERR_OOM: return "device allocation failed";
+    case PANDORA_ERR_CUDA: return g_errmsg[0] ? g_errmsg : "CUDA error";
+    case PANDORA_ERR_NAN: return "non-finite value in the state";
+    case PANDORA_ERR_TIMEOUT: return "bounded device wait gave up";
+    case PANDORA_ERR_BAD_LAYOUT: return "grid size not supported by the transform plan";
+    case PANDORA_ERR_CFL: return "RK3_CFL >= 1";
+    case PANDORA_ERR_PARTICLE_LOST: return "particle left the domain after the wrap";
+    case PANDORA_ERR_NO_DEVICE: return "no CUDA device";
+    case PANDORA_ERR_UNSUPPORTED: return "option not supported by this library";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int pandora_params_sizeof(void) { return (int)sizeof(pandora_params); }
+
+extern "C" int pandora_device_count(int* count) {
+    if (!count) return PANDORA_ERR_INVALID_ARG;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) { *count = 0; cudaGetLastError(); return PANDORA_ERR_NO_DEVICE; }
+    *count = n;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_params_default(pandora_params* p) {
+    if (!p) return PANDORA_ERR_INVALID_ARG;
+    memset(p, 0, sizeof(*p));
+    p->nodes_x = p->nodes_y = p->nodes_z = 32;
+    p->b110 = p->b220 = p->b330 = 1;
+    p->f_rho = 1.0; p->f_nu = 0.025;
+    p->f_type = PANDORA_F_ISOTROPIC; p->f_deform_s = 28.3; p->f_remesh_t = 32;
+    p->rk3_timestep = PANDORA_RK3_TIMESTEP_DECIDE; p->rk3_cfl = 0.75; p->rk3_dt = 0.01;
+    p->ns_deformed = PANDORA_NS_BF_ROT; p->dealiasing = 1; p->tsteps = 10;
+    p->f_init_type = PANDORA_F_INIT_KERR; p->f_init_u0 = 0.1; p->f_init_kp = 11.0; p->f_init_kv = 20.0;
+    p->f_init_kstart = 5.0; p->f_init_kend = 10.0;
+    p->force_tf = 0.2; p->force_sigma = 0.03743; p->force_kf = 2.829; p->force_stop = 99999;
+    p->p_track_part = 0; p->p_init_type = PANDORA_P_INIT_RANDOM; p->p_np_global = 10;
+    p->p_interp_order = 4; p->p_ts_release = 1000; p->p_rho = 1000.0; p->p_dia_vals = 0.01514314;
+    p->seed_fluid = 1; p->seed_force = 2; p->seed_particles = 3;
+    p->precision = PANDORA_PREC_FP64;
+    return PANDORA_OK;
+}
+
+static int kkmax_of(int ki, int kj, int kk) {
+    const double kmax = sqrt((double)((long long)ki * ki + (long long)kj * kj + (long long)kk * kk));
+    return (int)lround(kmax / 1.0);
+}
+
+extern "C" int pandora_sizes(const pandora_params* p, int32_t* nki, int32_t* nkj, int32_t* nkk, int64_t* modes,
+                             int32_t* kkmax) {
+    if (!p || p->nodes_x < 3 || p->nodes_y < 3 || p->nodes_z < 3) return PANDORA_ERR_INVALID_ARG;
+    const int ki = p->nodes_x / 3, kj = p->nodes_y / 3, kk = p->nodes_z / 3;
+    if (nki) *nki = ki + 1;
+    if (nkj) *nkj = 2 * kj + 1;
+    if (nkk) *nkk = 2 * kk + 1;
+    if (modes) *modes = (int64_t)(ki + 1) * (2 * kj + 1) * (2 * kk + 1);
+    if (kkmax) *kkmax = kkmax_of(ki, kj, kk);
+    return PANDORA_OK;
+}
+
+static long long force_calls(int NK) {
+    return 3LL * ((long long)(NK + 1) * (NK + 1) + (long long)NK * (NK + 1)) +
+           3LL * NK * (2LL * NK + 1) * (2LL * NK + 1);
+}
+
+static void release(pandora_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->dev);
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    cudaFree(h->fbuf); cudaFree(h->F.zb); cudaFree(h->F.yb); cudaFree(h->F.phys);
+    cudaFree(h->F.forcing); cudaFree(h->tw); cudaFree(h->clock); cudaFree(h->shell_step);
+    cudaFree(h->shell_now); cudaFree(h->pbuf); cudaFree(h->nlbuf);
+    if (h->clock_host) cudaFreeHost(h->clock_host);
+    if (h->shell_host) cudaFreeHost(h->shell_host);
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+}
+
+static int validate(const pandora_params* p) {
+    if (!p) return PANDORA_ERR_INVALID_ARG;
+    if (p->precision != PANDORA_PREC_FP64) return PANDORA_ERR_UNSUPPORTED;
+    if (p->f_type != PANDORA_F_ISOTROPIC) return PANDORA_ERR_UNSUPPORTED;
+    if (p->dealiasing != 1) return PANDORA_ERR_UNSUPPORTED;
+    if (!supported_length(p->nodes_x) || !supported_length(p->nodes_y) || !supported_length(p->nodes_z))
+        return PANDORA_ERR_BAD_LAYOUT;
+    if (p->rk3_cfl >= 1.0) return PANDORA_ERR_CFL;   // g_RK3Check, src/pg_rk3.f90:240-267
+    if (p->rk3_timestep < 1 || p->rk3_timestep > 3) return PANDORA_ERR_INVALID_ARG;
+    if (p->force_kf < 0.0 || p->force_kf > 8.0 || p->force_tf <= 0.0) return PANDORA_ERR_INVALID_ARG;
+    if (p->f_nu < 0.0) return PANDORA_ERR_INVALID_ARG;
+    if (p->p_track_part) {
+        if (p->p_np_global < 0 || p->p_interp_order < 1 || p->p_interp_order > 6) return PANDORA_ERR_INVALID_ARG;
+        if (p->p_dia_vals > 0.0 && (p->f_nu <= 0.0 || p->f_rho <= 0.0)) return PANDORA_ERR_INVALID_ARG;
+    }
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
+    if (!out) return PANDORA_ERR_INVALID_ARG;
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return PANDORA_ERR_NO_DEVICE; }
+    pandora_handle* h = new (std::nothrow) pandora_handle();
+    if (!h) return PANDORA_ERR_OOM;
+    h->p = *p;
+    cudaGetDevice(&h->dev);
+    Geo& g = h->g;
+    g.nx = p->nodes_x; g.ny = p->nodes_y; g.nz = p->nodes_z;
+    g.ki = g.nx / 3; g.kj = g.ny / 3; g.kk = g.nz / 3;
+    g.nki = g.ki + 1; g.nkj = 2 * g.kj + 1; g.nkk = 2 * g.kk + 1;
+    g.nkip = (g.nki + 7) / 8 * 8;
+    g.S = (long long)g.nki * g.nkj * g.nkk;
+    g.R = (long long)g.nx * g.ny * g.nz;
+    g.nu = p->f_nu;
+    g.norm = 1.0 / ((double)g.nx * (double)g.ny * (double)g.nz);
+    const double twopi = 6.283185307179586476925286766559005768;
+    g.lx = twopi; g.ly = twopi; g.lz = twopi;
+    g.dx = g.lx / (double)g.nx; g.dy = g.ly / (double)g.ny; g.dz = g.lz / (double)g.nz;
+    g.force_kf = p->force_kf;
+    g.fnk = (int)p->force_kf;
+    g.kkmax = kkmax_of(g.ki, g.kj, g.kk);
+    h->nforce = (long long)(g.fnk + 1) * (2 * g.fnk + 1) * (2 * g.fnk + 1);
+    h->particles_on = p->p_track_part != 0;
+
+    cudaError_t e;
+#define PD_ALLOC(ptr, bytes)                                              \
+    do {                                                                  \
+        e = cudaMalloc((void**)&(ptr), (bytes));                          \
+        if (e != cudaSuccess) { cudaGetLastError(); release(h); return PANDORA_ERR_OOM; } \
+    } while (0)
+    PD_ALLOC(h->fbuf, sizeof(double2) * 6 * (size_t)g.S);
+    for (int c = 0; c < 3; c++) { h->F.u[c] = h->fbuf + c * g.S; h->F.rk[c] = h->fbuf + (3 + c) * g.S; }
+    PD_ALLOC(h->F.zb, sizeof(double2) * 6 * (size_t)g.nz * g.nkj * g.nkip);
+    PD_ALLOC(h->F.yb, sizeof(double2) * 6 * (size_t)g.nz * g.ny * g.nkip);
+    if (h->particles_on) PD_ALLOC(h->F.phys, sizeof(double) * 3 * (size_t)g.R);
+    PD_ALLOC(h->F.forcing, sizeof(double2) * 3 * (size_t)h->nforce);
+    PD_ALLOC(h->tw, sizeof(double2) * (size_t)(g.nx + g.ny + g.nz));
+    PD_ALLOC(h->clock, sizeof(Clock));
+    const size_t nsh = (size_t)2 * (g.kkmax + 1) + 3;
+    PD_ALLOC(h->shell_step, sizeof(double) * nsh);
+    PD_ALLOC(h->shell_now, sizeof(double) * nsh);
+#undef PD_ALLOC
+    if (cudaMallocHost((void**)&h->clock_host, sizeof(Clock)) != cudaSuccess ||
+        cudaMallocHost((void**)&h->shell_host, sizeof(double) * nsh) != cudaSuccess) {
+        cudaGetLastError(); release(h); return PANDORA_ERR_OOM;
+    }
+    if ((e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "cudaStreamCreate");
+    }
+    h->st = h->own;
+    // twiddles tw[e] = exp(-2 pi i e / N), long double on the host
+    std::vector<double2> tw((size_t)(g.nx + g.ny + g.nz));
+    int off = 0;
+    const int lens[3] = {g.nx, g.ny, g.nz};
+    const double2** dst[3] = {&h->F.tw_x, &h->F.tw_y, &h->F.tw_z};
+    for (int d = 0; d < 3; d++) {
+        const int n = lens[d];
+        for (int q = 0; q < n; q++) {
+            const long double a = 6.283185307179586476925286766559005768L * (long double)q / (long double)n;
+            tw[off + q] = make_double2((double)cosl(a), -(double)sinl(a));
+        }
+        *dst[d] = h->tw + off;
+        off += n;
+    }
+    if ((e = cudaMemcpy(h->tw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "twiddles");
+    }
+    // mode density (src/pf_fluidstats.f90:696-780), integer counts -> exact
+    h->dens_mod.assign(g.kkmax + 1, 0.0);
+    {
+        std::vector<long long> cnt(g.kkmax + 2, 0);
+        for (int i = 0; i < g.nki; i++)
+            for (int j = 0; j < g.nkj; j++)
+                for (int k = 0; k < g.nkk; k++) {
+                    const double a = i, b = wvn(j, g.kj), c = wvn(k, g.kk);
+                    const double km = sqrt((a * a) + (b * b) + (c * c));
+                    const int kc = (int)floor(km + 0.5);
+                    for (int q = kc - 1; q <= kc + 1; q++) {
+                        if (q < 1 || q > g.kkmax) continue;
+                        if (km >= (double)q - 0.5 && km < (double)q + 0.5) cnt[q] += (i != 0) ? 2 : 1;
+                    }
+                }
+        const double pi = 3.14159265358979323846264338327950288;
+        for (int q = 1; q <= g.kkmax; q++) {
+            const double up = (double)q + 0.5, lo = (double)q - 0.5;
+            h->dens_mod[q] = (double)cnt[q] / (4.0 / 3.0 * pi * (up * up * up - lo * lo * lo));
+        }
+    }
+    h->F.clock = h->clock;
+    h->F.shell = h->shell_step;
+    h->sp.rk3_timestep = p->rk3_timestep; h->sp.f_type = p->f_type; h->sp.rk3_dt = p->rk3_dt;
+    h->sp.rk3_cfl = p->rk3_cfl; h->sp.force_tf = p->force_tf; h->sp.f_deform_s = p->f_deform_s;
+    h->sp.f_remesh_t = p->f_remesh_t;
+    h->fp.tf = p->force_tf; h->fp.sigma = p->force_sigma; h->fp.stop = p->force_stop;
+    h->fp.key = stream_key(p->seed_force, TAG_FORCE);
+    h->fp.calls_per_stage = force_calls(g.fnk);
+    h->pp.order = p->p_interp_order; h->pp.release = p->p_ts_release; h->pp.f_nu = p->f_nu;
+    h->pp.p_rho = p->p_rho; h->pp.f_rho = p->f_rho;
+    if ((e = configure_kernels(g)) != cudaSuccess) { release(h); return cuda_fail(e, "configure_kernels"); }
+    // zero state (the reference zero-initialises its Vecs and rk3 registers)
+    if ((e = cudaMemsetAsync(h->fbuf, 0, sizeof(double2) * 6 * (size_t)g.S, h->st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->clock, 0, sizeof(Clock), h->st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->shell_step, 0, sizeof(double) * nsh, h->st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(h->st)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "zero state");
+    }
+    if (h->particles_on && p->p_np_global > 0) {
+        const long long np = p->p_np_global;
+        if ((e = cudaMalloc((void**)&h->pbuf, sizeof(double) * 13 * (size_t)np)) != cudaSuccess) {
+            cudaGetLastError(); release(h); return PANDORA_ERR_OOM;
+        }
+        cudaMemsetAsync(h->pbuf, 0, sizeof(double) * 13 * (size_t)np, h->st);
+        h->P.np = np;
+        for (int c = 0; c < 3; c++) {
+            h->P.xp[c] = h->pbuf + (0 + c) * np; h->P.up[c] = h->pbuf + (3 + c) * np;
+            h->P.uprk[c] = h->pbuf + (6 + c) * np; h->P.prk[c] = h->pbuf + (9 + c) * np;
+        }
+        h->P.dp = h->pbuf + 12 * np;
+    }
+    *out = h;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_destroy(pandora_handle* h) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    release(h);
+    return PANDORA_OK;
+}
+
+static void drop_graph(pandora_handle* h) {
+    if (h->exec) { cudaGraphExecDestroy(h->exec); h->exec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+}
+
+extern "C" int pandora_set_stream(pandora_handle* h, void* s) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(cudaStreamSynchronize(h->st));
+    h->st = s ? (cudaStream_t)s : h->own;
+    return PANDORA_OK;
+}
+
+static int copy3(pandora_handle* h, double2* const* dev, const double* a, const double* b, const double* c,
+                 size_t n, bool to_dev) {
+    if (!h || !a || !b || !c) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    const double* src[3] = {a, b, c};
+    for (int q = 0; q < 3; q++) {
+        if (to_dev) PD_CK(cudaMemcpyAsync(dev[q], src[q], sizeof(double2) * n, cudaMemcpyHostToDevice, h->st));
+        else PD_CK(cudaMemcpyAsync((void*)src[q], dev[q], sizeof(double2) * n, cudaMemcpyDeviceToHost, h->st));
+    }
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_set_state(pandora_handle* h, const double* u1, const double* u2, const double* u3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    return copy3(h, h->F.u, u1, u2, u3, (size_t)h->g.S, true);
+}
+extern "C" int pandora_get_state(pandora_handle* h, double* u1, double* u2, double* u3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    return copy3(h, h->F.u, u1, u2, u3, (size_t)h->g.S, false);
+}
+extern "C" int pandora_set_rk(pandora_handle* h, const double* r1, const double* r2, const double* r3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    return copy3(h, h->F.rk, r1, r2, r3, (size_t)h->g.S, true);
+}
+extern "C" int pandora_get_rk(pandora_handle* h, double* r1, double* r2, double* r3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    return copy3(h, h->F.rk, r1, r2, r3, (size_t)h->g.S, false);
+}
+extern "C" int pandora_forcing_size(pandora_handle* h, int64_t* n) {
+    if (!h || !n) return PANDORA_ERR_INVALID_ARG;
+    *n = 2 * h->nforce;
+    return PANDORA_OK;
+}
+extern "C" int pandora_set_forcing(pandora_handle* h, const double* f1, const double* f2, const double* f3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    double2* d[3] = {h->F.forcing, h->F.forcing + h->nforce, h->F.forcing + 2 * h->nforce};
+    return copy3(h, d, f1, f2, f3, (size_t)h->nforce, true);
+}
+extern "C" int pandora_get_forcing(pandora_handle* h, double* f1, double* f2, double* f3) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    double2* d[3] = {h->F.forcing, h->F.forcing + h->nforce, h->F.forcing + 2 * h->nforce};
+    return copy3(h, d, f1, f2, f3, (size_t)h->nforce, false);
+}
+extern "C" int pandora_state_device_ptrs(pandora_handle* h, void** u1, void** u2, void** u3) {
+    if (!h || !u1 || !u2 || !u3) return PANDORA_ERR_INVALID_ARG;
+    *u1 = h->F.u[0]; *u2 = h->F.u[1]; *u3 = h->F.u[2];
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_init_fluid(pandora_handle* h) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    InitParams ip{};
+    ip.type = h->p.f_init_type; ip.u0 = h->p.f_init_u0; ip.kp = h->p.f_init_kp; ip.kv = h->p.f_init_kv;
+    ip.kstart = h->p.f_init_kstart; ip.kend = h->p.f_init_kend; ip.epsilon = h->p.f_init_epsilon;
+    ip.b220 = h->p.b220;
+    ip.key = stream_key(h->p.seed_fluid, TAG_FLUID);
+    PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
+}
+
+// ---- particles ----
+static int part_check(pandora_handle* h, int64_t np) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    if (!h->particles_on || np != h->P.np) return PANDORA_ERR_INVALID_ARG;
+    return PANDORA_OK;
+}
+extern "C" int pandora_set_particles(pandora_handle* h, int64_t np, const double* xp, const double* up,
+                                     const double* up_rk3, const double* rk3, const double* dp) {
+    int rc = part_check(h, np);
+    if (rc) return rc;
+    if (np == 0) return PANDORA_OK;
+    cudaSetDevice(h->dev);
+    std::vector<double> soa((size_t)13 * np, 0.0);
+    // SoA order in pbuf: xp(0..2) up(3..5) uprk(6..8) prk(9..11) dp(12)
+    const double* srcs[4] = {xp, up, up_rk3, rk3};
+    for (int a = 0; a < 4; a++) {
+        if (!srcs[a]) continue;
+        for (int64_t n = 0; n < np; n++)
+            for (int c = 0; c < 3; c++) soa[(size_t)(3 * a + c) * np + n] = srcs[a][3 * n + c];
+    }
+    if (dp) memcpy(&soa[(size_t)12 * np], dp, sizeof(double) * np);
+    PD_CK(cudaMemcpyAsync(h->pbuf, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
+}
+extern "C" int pandora_get_particles(pandora_handle* h, int64_t np, double* xp, double* up, double* up_rk3,
+                                     double* rk3, double* dp) {
+    int rc = part_check(h, np);
+    if (rc) return rc;
+    if (np == 0) return PANDORA_OK;
+    cudaSetDevice(h->dev);
+    std::vector<double> soa((size_t)13 * np);
+    PD_CK(cudaMemcpyAsync(soa.data(), h->pbuf, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    double* dsts[4] = {xp, up, up_rk3, rk3};
+    for (int a = 0; a < 4; a++) {
+        if (!dsts[a]) continue;
+        for (int64_t n = 0; n < np; n++)
+            for (int c = 0; c < 3; c++) dsts[a][3 * n + c] = soa[(size_t)(3 * a + c) * np + n];
+    }
+    if (dp) memcpy(dp, &soa[(size_t)12 * np], sizeof(double) * np);
+    return PANDORA_OK;
+}
+extern "C" int pandora_init_particles(pandora_handle* h) {
+    if (!h || !h->particles_on) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(launch_init_particles(h->g, h->P, stream_key(h->p.seed_particles, TAG_PART), h->p.p_dia_vals, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
+}
+
+// ---- stage sequencing ----
+// f_RK3Stage{s} (src/pf_rk3.f90:40-200): [s=1: statistics of the state],
+// vorticity + z pass, y pass, x pass with NL (and CFL / physical velocity),
+// dt + forcing, particles, forward y, forward z + RK update, time advance.
+static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
+    const Geo& g = h->g;
+    int n = 0;
+    const bool part = h->particles_on && h->P.np > 0;
+    if (stage == 1) {
+        Fields Fs = h->F;
+        Fs.shell = h->shell_step;
+        PD_CK(launch_stats(g, Fs, h->st)); n += 1;   // one kernel (plus a memset node)
+    }
+    PD_CK(launch_zpass_inv(g, h->F, stage, h->st)); n++;
+    PD_CK(launch_ypass_inv(g, h->F, h->st)); n++;
+    PD_CK(launch_xpass(g, h->F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
+    PD_CK(launch_stage_scalars(g, h->F, h->sp, h->fp, stage, h->st)); n++;
+    if (part) { PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->st)); n++; }
+    PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
+    PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n++;
+    PD_CK(launch_advance_time(h->F, stage, h->st)); n++;
+    if (nlaunch) *nlaunch += n;
+    return PANDORA_OK;
+}
+
+static int enqueue_step(pandora_handle* h) {
+    int n = 0;
+    for (int s = 1; s <= 3; s++) {
+        int rc = enqueue_stage(h, s, &n);
+        if (rc) return rc;
+    }
+    h->launches_per_step = n;
+    return PANDORA_OK;
+}
+
+static int build_graph(pandora_handle* h) {
+    if (h->exec) return PANDORA_OK;
+    PD_CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_step(h);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->st, &gr);
+    if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    h->graph = gr;
+    e = cudaGraphInstantiate(&h->exec, gr, 0);
+    if (e != cudaSuccess) { drop_graph(h); return cuda_fail(e, "cudaGraphInstantiate"); }
+    return PANDORA_OK;
+}
+
+static int status_to_rc(unsigned int st) {
+    if (st & PD_ST_NAN) return PANDORA_ERR_NAN;
+    if (st & PD_ST_LOST) return PANDORA_ERR_PARTICLE_LOST;
+    if (st & (PD_ST_POLAR | PD_ST_TIMEOUT)) return PANDORA_ERR_TIMEOUT;
+    return PANDORA_OK;
+}
+
+static int set_clock(pandora_handle* h, int tstep, double simtime) {
+    // keep dt / ucfl / status from the device copy
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    h->clock_host->tstep = tstep;
+    h->clock_host->simtime = simtime;
+    h->clock_host->t0 = simtime;
+    PD_CK(cudaMemcpyAsync(h->clock, h->clock_host, sizeof(Clock), cudaMemcpyHostToDevice, h->st));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_rk3_advance(pandora_handle* h, int32_t tstep0, int32_t nsteps, int32_t sync,
+                                   double* simtime) {
+    if (!h || nsteps < 0 || !simtime) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    int rc = set_clock(h, tstep0, *simtime);
+    if (rc) return rc;
+    if (h->use_graph) {
+        rc = build_graph(h);
+        if (rc) return rc;
+        for (int s = 0; s < nsteps; s++) PD_CK(cudaGraphLaunch(h->exec, h->st));
+    } else {
+        for (int s = 0; s < nsteps; s++) if ((rc = enqueue_step(h))) return rc;
+    }
+    if (!sync) return PANDORA_OK;
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    *simtime = h->clock_host->simtime;
+    return status_to_rc(h->clock_host->status);
+}
+
+extern "C" int pandora_rk3_step(pandora_handle* h, int32_t tstep, double* simtime, double* dt) {
+    if (!h || !simtime) return PANDORA_ERR_INVALID_ARG;
+    int rc = pandora_rk3_advance(h, tstep, 1, 1, simtime);
+    if (dt) *dt = h->clock_host->dt;
+    return rc;
+}
+
+extern "C" int pandora_rk3_stage(pandora_handle* h, int32_t stage, int32_t tstep, double time, double* dt) {
+    if (!h || stage < 1 || stage > 3 || !dt) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    h->clock_host->tstep = tstep;
+    h->clock_host->simtime = time;
+    if (stage == 1) h->clock_host->t0 = time;
+    h->clock_host->dt = *dt;
+    PD_CK(cudaMemcpyAsync(h->clock, h->clock_host, sizeof(Clock), cudaMemcpyHostToDevice, h->st));
+    int rc = enqueue_stage(h, stage, nullptr);
+    if (rc) return rc;
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    *dt = h->clock_host->dt;
+    return status_to_rc(h->clock_host->status);
+}
+
+// ---- statistics ----
+static void finish_stats(pandora_handle* h, const double* sh, double* ek, int32_t kkmax, double* tke,
+                         double* eps) {
+    const int K = h->g.kkmax;
+    const double* se = sh;
+    const double* sd = sh + (K + 1);
+    const double* sp = sh + 2 * (K + 1);
+    double fdis = 0.0;
+    for (int q = 1; q <= K; q++) {
+        if (h->dens_mod[q] != 0.0) {
+            fdis += sd[q];
+            if (ek && q - 1 < kkmax) ek[q - 1] = se[q] / h->dens_mod[q];
+        } else if (ek && q - 1 < kkmax) {
+            ek[q - 1] = se[q];
+        }
+    }
+    if (tke) *tke = 0.5 * (sp[0] + sp[1] + sp[2]);
+    if (eps) *eps = fdis;
+}
+
+extern "C" int pandora_stats(pandora_handle* h, double* ek, int32_t kkmax, double* tke, double* eps,
+                             double* ucfl) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    Fields Fs = h->F;
+    Fs.shell = h->shell_now;
+    PD_CK(launch_stats(h->g, Fs, h->st));
+    const size_t nsh = (size_t)2 * (h->g.kkmax + 1) + 3;
+    PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_now, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    finish_stats(h, h->shell_host, ek, kkmax, tke, eps);
+    if (ucfl) memcpy(ucfl, &h->clock_host->ucfl_bits, sizeof(double));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_last_step_stats(pandora_handle* h, double* ek, int32_t kkmax, double* tke, double* eps,
+                                       double* ucfl) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    const size_t nsh = (size_t)2 * (h->g.kkmax + 1) + 3;
+    PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_step, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    finish_stats(h, h->shell_host, ek, kkmax, tke, eps);
+    if (ucfl) memcpy(ucfl, &h->clock_host->ucfl_bits, sizeof(double));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, double* n3) {
+    if (!h || !n1 || !n2 || !n3) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    if (!h->nlbuf) {
+        if (cudaMalloc((void**)&h->nlbuf, sizeof(double2) * 3 * (size_t)h->g.S) != cudaSuccess) {
+            cudaGetLastError(); return PANDORA_ERR_OOM;
+        }
+    }
+    Fields Fn = h->F;
+    for (int c = 0; c < 3; c++) Fn.rk[c] = h->nlbuf + c * h->g.S;
+    PD_CK(launch_zpass_inv(h->g, Fn, 0, h->st));
+    PD_CK(launch_ypass_inv(h->g, Fn, h->st));
+    PD_CK(launch_xpass(h->g, Fn, 0, 0, h->st));
+    PD_CK(launch_ypass_fwd(h->g, Fn, h->st));
+    PD_CK(launch_zpass_fwd_update(h->g, Fn, 1, 1, h->st));
+    return copy3(h, Fn.rk, n1, n2, n3, (size_t)h->g.S, false);
+}
+
+extern "C" int pandora_get_physical_velocity(pandora_handle* h, double* u1, double* u2, double* u3) {
+    if (!h || !u1 || !u2 || !u3) return PANDORA_ERR_INVALID_ARG;
+    if (!h->F.phys) return PANDORA_ERR_UNSUPPORTED;
+    cudaSetDevice(h->dev);
+    double* d[3] = {u1, u2, u3};
+    for (int c = 0; c < 3; c++)
+        PD_CK(cudaMemcpyAsync(d[c], h->F.phys + c * h->g.R, sizeof(double) * h->g.R, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_check_status(pandora_handle* h) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(launch_check_finite(h->g, h->F, h->st));
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    const unsigned int st = h->clock_host->status;
+    h->clock_host->status = 0;
+    PD_CK(cudaMemcpyAsync(&h->clock->status, &h->clock_host->status, sizeof(unsigned int),
+                          cudaMemcpyHostToDevice, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return status_to_rc(st);
+}
+
+extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
+    if (!h || !n) return PANDORA_ERR_INVALID_ARG;
+    if (!h->launches_per_step) {
+        // count without launching: same sequence as enqueue_step
+        const bool part = h->particles_on && h->P.np > 0;
+        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0));
+    }
+    *n = h->launches_per_step;
+    return PANDORA_OK;
+}

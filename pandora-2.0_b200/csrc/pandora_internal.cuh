@@ -1,0 +1,138 @@
+// pandora_internal.cuh -- device-side structures shared by the kernels and the
+// C-ABI layer.  Not part of the public boundary (include/pandora_gpu.h is).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/pandora_gpu.h"
+
+namespace pd {
+
+// Geometry and constants of one simulation, passed by value to every kernel.
+// Sizes follow g_DomainCalc (src/pg_domain.f90:147-243): KI = NX/3 etc., the
+// stored spectral extents NKI = KI+1, NKJ = 2KJ+1, NKK = 2KK+1.  Intermediate
+// pencils pad the i extent to NKIP (a multiple of 8) so that every tile row
+// starts on a 128-byte boundary.
+struct Geo {
+    int nx, ny, nz;
+    int ki, kj, kk;
+    int nki, nkj, nkk, nkip;
+    long long S;          // modes per component
+    long long R;          // physical points
+    double nu;            // F_NU
+    double norm;          // 1 / (NX NY NZ)
+    double dx, dy, dz, lx, ly, lz;
+    double force_kf;
+    int fnk;              // aint(FORCE_KF)
+    int kkmax;            // E(k) shells
+};
+
+// Scalars of the running step kept in device memory so that a whole step can
+// be replayed from a CUDA graph without host involvement.
+struct Clock {
+    double simtime;                 // time of the current stage (g_RK3Calc's simtime)
+    double t0;                      // time at the start of the step
+    double dt;                      // dt of the step (f_RK3Tstep at stage 1)
+    unsigned long long ucfl_bits;   // max |u1|+|u2|+|u3| of stage 1, as ordered bits
+    int tstep;                      // number of the step being taken
+    unsigned int status;            // PD_ST_* bits
+};
+
+enum : unsigned int {
+    PD_ST_NAN = 1u,
+    PD_ST_POLAR = 2u,       // bounded polar rejection loop gave up
+    PD_ST_LOST = 4u,        // particle outside the domain after the wrap
+    PD_ST_TIMEOUT = 8u,
+};
+
+// ---- project RNG (SplitMix64 finaliser over a stream index; the oracle
+//      restates the same definition) ----
+#define PD_GOLDEN 0x9E3779B97F4A7C15ULL
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ uint64_t stream_key(uint64_t seed, uint64_t tag) {
+    return mix64(seed * PD_GOLDEN + tag * 0xD1B54A32D192ED03ULL + 0x632BE59BD9B4E019ULL);
+}
+__host__ __device__ __forceinline__ double uniform(uint64_t key, uint64_t n) {
+    return (double)(mix64(key + (n + 1) * PD_GOLDEN) >> 11) * 0x1.0p-53;
+}
+enum : uint64_t { TAG_FLUID = 1, TAG_FORCE = 2, TAG_PART = 3 };
+constexpr int kMaxPolarTries = 64;
+
+__host__ __device__ __forceinline__ double wvn(int idx, int K) {
+    return (double)(idx <= K ? idx : idx - (2 * K + 1));
+}
+
+// Launchers (kernels_*.cu).  All enqueue on `st` and return cudaGetLastError().
+struct Fields {
+    double2* u[3];
+    double2* rk[3];
+    double2* zb;        // [6][NZ][NKJ][NKIP]  after the z pass
+    double2* yb;        // [6][NZ][NY][NKIP]   after the y pass; NL written into fields 0..2
+    double* phys;       // [3][NZ][NY][NX]     physical velocity (particles), may be null
+    double2* forcing;   // [3][NK+1][2NK+1][2NK+1]
+    const double2 *tw_x, *tw_y, *tw_z;
+    Clock* clock;
+    double* shell;      // [2*(kkmax+1) + 3] shell sums (e, d) + p11,p22,p33
+};
+
+struct Particles {
+    long long np;
+    double* xp[3];
+    double* up[3];
+    double* uprk[3];
+    double* prk[3];
+    double* dp;
+};
+
+struct ForceParams {
+    double tf, sigma;
+    int stop;
+    uint64_t key;
+    long long calls_per_stage;
+};
+
+struct StepParams {
+    int rk3_timestep;
+    int f_type;
+    double rk3_dt, rk3_cfl, force_tf, f_deform_s;
+    int f_remesh_t;
+};
+
+struct PartParams {
+    int order;
+    int release;
+    double f_nu, p_rho, f_rho;
+};
+
+struct InitParams {
+    int type;
+    double u0, kp, kv, kstart, kend, epsilon;
+    int b220;
+    uint64_t key;
+};
+
+bool supported_length(int n);
+
+cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStream_t st);
+cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st);
+cudaError_t launch_xpass(const Geo& g, const Fields& f, int want_phys, int want_cfl, cudaStream_t st);
+cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st);
+cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, int mode, cudaStream_t st);
+cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st);
+cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams& sp,
+                                 const ForceParams& fp, int stage, cudaStream_t st);
+cudaError_t launch_advance_time(const Fields& f, int stage, cudaStream_t st);
+cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);
+cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp,
+                             int stage, cudaStream_t st);
+cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia,
+                                  cudaStream_t st);
+cudaError_t launch_check_finite(const Geo& g, const Fields& f, cudaStream_t st);
+
+// Shared-memory configuration (set once per process per device).
+cudaError_t configure_kernels(const Geo& g);
+
+}  // namespace pd

@@ -1,0 +1,247 @@
+"""Host-side mirror of the reference's RK3 interface, driving the CUDA library.
+
+The reference keeps its fields module-global and exposes Fortran subroutines
+(src/pg_rk3.f90:82 g_RK3Calc, src/pf_rk3.f90:40,121,161 f_RK3Stage1..3,
+src/pp_control.f90:589 p_ControlInitialiseParticles, src/pf_fluidstats.f90:1293
+f_FluidstatsFs, src/pf_initialise.f90 f_InitialiseInit).  ``Simulation`` owns
+one device handle; the module-level functions with the reference's names act on
+a current simulation set by ``ProgramInit``, the way the Fortran modules act on
+their module state.  Errors that the reference turns into ``MPI_Abort`` or a
+non-zero ``ierr`` raise ``PandoraError`` here.
+
+Arrays use the reference layout: complex128 of shape (NKI, NKJ, NKK) per
+component, NKI = NX/3+1, NKJ = 2(NY/3)+1, NKK = 2(NZ/3)+1.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import Params
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _as_f64(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    if np.iscomplexobj(a):
+        a = np.ascontiguousarray(a.astype(np.complex128, copy=False)).view(np.float64)
+    else:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+    return a
+
+
+class Simulation:
+    """One resident simulation on the current CUDA device."""
+
+    def __init__(self, params: Params):
+        self.L = _lib.load()
+        self.p = params.copy()
+        h = ctypes.c_void_p()
+        _lib.check(self.L.pandora_create(ctypes.byref(self.p), ctypes.byref(h)), "pandora_create")
+        self.h = h
+        nki, nkj, nkk, kk = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        modes = ctypes.c_int64()
+        _lib.check(self.L.pandora_sizes(ctypes.byref(self.p), ctypes.byref(nki), ctypes.byref(nkj),
+                                        ctypes.byref(nkk), ctypes.byref(modes), ctypes.byref(kk)), "pandora_sizes")
+        self.shape = (nki.value, nkj.value, nkk.value)
+        self.modes = modes.value
+        self.kkmax = kk.value
+        nf = ctypes.c_int64()
+        _lib.check(self.L.pandora_forcing_size(self.h, ctypes.byref(nf)), "pandora_forcing_size")
+        nk = int(self.p.force_kf)
+        self.force_shape = (nk + 1, 2 * nk + 1, 2 * nk + 1)
+        self.np = int(self.p.p_np_global) if self.p.p_track_part else 0
+        self.simtime = 0.0
+        self.tstep = 0
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pandora_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None):
+        _lib.check(self.L.pandora_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), "pandora_set_stream")
+
+    # ---- state ----
+    def _put3(self, fn, arrs, name):
+        a = [_as_f64(x) for x in arrs]
+        _lib.check(fn(self.h, *[_dp(x) for x in a]), name)
+
+    def _get3(self, fn, shape, name):
+        out = [np.zeros(shape, np.complex128) for _ in range(3)]
+        _lib.check(fn(self.h, *[_dp(x.view(np.float64)) for x in out]), name)
+        return out
+
+    def set_state(self, u):
+        for c in u:
+            if np.shape(c) != self.shape:
+                raise ValueError(f"state component shape {np.shape(c)} != {self.shape}")
+        self._put3(self.L.pandora_set_state, u, "pandora_set_state")
+
+    def get_state(self):
+        return self._get3(self.L.pandora_get_state, self.shape, "pandora_get_state")
+
+    def set_rk(self, r):
+        self._put3(self.L.pandora_set_rk, r, "pandora_set_rk")
+
+    def get_rk(self):
+        return self._get3(self.L.pandora_get_rk, self.shape, "pandora_get_rk")
+
+    def set_forcing(self, f):
+        self._put3(self.L.pandora_set_forcing, f, "pandora_set_forcing")
+
+    def get_forcing(self):
+        return self._get3(self.L.pandora_get_forcing, self.force_shape, "pandora_get_forcing")
+
+    def init_fluid(self):
+        _lib.check(self.L.pandora_init_fluid(self.h), "pandora_init_fluid")
+
+    # ---- particles ----
+    def init_particles(self):
+        _lib.check(self.L.pandora_init_particles(self.h), "pandora_init_particles")
+
+    def set_particles(self, xp, up=None, up_rk3=None, rk3=None, dp=None):
+        n = len(xp)
+        f = lambda a: None if a is None else _dp(_keep.setdefault(id(a), _as_f64(a)))
+        _keep: dict = {}
+        _lib.check(self.L.pandora_set_particles(self.h, n, f(xp), f(up), f(up_rk3), f(rk3), f(dp)),
+                   "pandora_set_particles")
+
+    def get_particles(self):
+        n = self.np
+        xp, up, ur, pr = (np.zeros((n, 3)) for _ in range(4))
+        dp = np.zeros(n)
+        _lib.check(self.L.pandora_get_particles(self.h, n, _dp(xp), _dp(up), _dp(ur), _dp(pr), _dp(dp)),
+                   "pandora_get_particles")
+        return xp, up, ur, pr, dp
+
+    # ---- stepping ----
+    def step(self, tstep: int | None = None) -> float:
+        """g_RK3Calc: one RK3 step; returns dt."""
+        if tstep is None:
+            tstep = self.tstep + 1
+        t = ctypes.c_double(self.simtime)
+        d = ctypes.c_double(0.0)
+        _lib.check(self.L.pandora_rk3_step(self.h, tstep, ctypes.byref(t), ctypes.byref(d)), "pandora_rk3_step")
+        self.simtime, self.tstep = t.value, tstep
+        return d.value
+
+    def advance(self, nsteps: int, sync: bool = True) -> None:
+        t = ctypes.c_double(self.simtime)
+        _lib.check(self.L.pandora_rk3_advance(self.h, self.tstep + 1, nsteps, 1 if sync else 0, ctypes.byref(t)),
+                   "pandora_rk3_advance")
+        self.tstep += nsteps
+        if sync:
+            self.simtime = t.value
+
+    def stage(self, stage: int, tstep: int, time: float, dt: float) -> float:
+        d = ctypes.c_double(dt)
+        _lib.check(self.L.pandora_rk3_stage(self.h, stage, tstep, time, ctypes.byref(d)), "pandora_rk3_stage")
+        return d.value
+
+    # ---- diagnostics ----
+    def stats(self, last_step: bool = False):
+        ek = np.zeros(self.kkmax)
+        tke, eps, ucfl = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        fn = self.L.pandora_last_step_stats if last_step else self.L.pandora_stats
+        _lib.check(fn(self.h, _dp(ek), self.kkmax, ctypes.byref(tke), ctypes.byref(eps), ctypes.byref(ucfl)),
+                   "pandora_stats")
+        return ek, tke.value, eps.value, ucfl.value
+
+    def nonlinear(self):
+        return self._get3(self.L.pandora_nonlinear, self.shape, "pandora_nonlinear")
+
+    def physical_velocity(self):
+        p = self.p
+        out = [np.zeros((p.nodes_z, p.nodes_y, p.nodes_x)) for _ in range(3)]
+        _lib.check(self.L.pandora_get_physical_velocity(self.h, *[_dp(x) for x in out]),
+                   "pandora_get_physical_velocity")
+        return out
+
+    def check_status(self) -> None:
+        _lib.check(self.L.pandora_check_status(self.h), "pandora_check_status")
+
+    def launches_per_step(self) -> int:
+        n = ctypes.c_int32()
+        _lib.check(self.L.pandora_launches_per_step(self.h, ctypes.byref(n)), "pandora_launches_per_step")
+        return n.value
+
+
+# ---------------------------------------------------------------------------
+# reference-named entry points over a current simulation
+# ---------------------------------------------------------------------------
+_current: Simulation | None = None
+
+
+def ProgramInit(params: Params) -> Simulation:
+    """ProgramInit (src/pg_control.f90:52-146): allocate the resident state and
+    initialise the fluid (and particles) from the seeds."""
+    global _current
+    if _current is not None:
+        _current.close()
+    sim = Simulation(params)
+    f_InitialiseInit(sim)
+    if params.p_track_part:
+        sim.init_particles()
+    _current = sim
+    return sim
+
+
+def _sim(sim: Simulation | None) -> Simulation:
+    s = sim or _current
+    if s is None:
+        raise RuntimeError("no current simulation; call ProgramInit first")
+    return s
+
+
+def f_InitialiseInit(sim: Simulation | None = None) -> None:
+    """f_InitialiseInit: seeded solenoidal field (src/pf_initialise.f90:97-512)."""
+    _sim(sim).init_fluid()
+
+
+def g_RK3Calc(tstep: int, simtime: float, sim: Simulation | None = None) -> float:
+    """g_RK3Calc (src/pg_rk3.f90:82-129): returns the new simtime."""
+    s = _sim(sim)
+    s.simtime = simtime
+    s.step(tstep)
+    return s.simtime
+
+
+def f_RK3Stage1(tstep: int, time: float, dt: float, sim: Simulation | None = None) -> float:
+    return _sim(sim).stage(1, tstep, time, dt)
+
+
+def f_RK3Stage2(tstep: int, time: float, dt: float, sim: Simulation | None = None) -> float:
+    return _sim(sim).stage(2, tstep, time, dt)
+
+
+def f_RK3Stage3(tstep: int, time: float, dt: float, sim: Simulation | None = None) -> float:
+    return _sim(sim).stage(3, tstep, time, dt)
+
+
+def f_FluidstatsFs(sim: Simulation | None = None):
+    """Primary spectral statistics (src/pf_fluidstats.f90:1423-1576): E(k), tke, eps, ucfl."""
+    return _sim(sim).stats()
+
+
+def p_ControlInitialiseParticles(sim: Simulation | None = None) -> None:
+    """P_INIT_RANDOM particle positions (src/pp_control.f90:663-707)."""
+    _sim(sim).init_particles()

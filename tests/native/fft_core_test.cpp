@@ -1,0 +1,73 @@
+// CPU check of the Stockham passes and small DFTs of csrc/fft_core.cuh: every
+// supported length and both signs against a direct O(N^2) DFT in long double,
+// with a tile of several lines in the padded column layout the kernels use.
+// Emulates one CTA: all items' load halves of a pass run before any store half.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include "fft_core.cuh"
+
+using namespace pdfft;
+
+template <int N, int R, int NS, int S, int L, int LP>
+static void emu_pass(std::vector<double2>& s, const std::vector<double2>& tw) {
+    constexpr int WORK = (N / R) * L;
+    std::vector<double2> v((size_t)WORK * R);
+    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP>(s.data(), tw.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP>(s.data(), w, &v[(size_t)w * R]);
+}
+
+template <int N, int S, int L, int LP>
+static double check() {
+    static_assert(plan_ok<N>(), "plan");
+    std::vector<double2> tw(N);
+    for (int e = 0; e < N; e++) {
+        long double a = 6.283185307179586476925286766559005768L * e / N;
+        tw[e] = mk((double)cosl(a), -(double)sinl(a));
+    }
+    std::vector<double2> s((size_t)N * LP), x((size_t)N * L);
+    srand(N * 7 + S + 3);
+    for (int l = 0; l < L; l++)
+        for (int n = 0; n < N; n++) {
+            double2 v = mk(rand() / (double)RAND_MAX - 0.5, rand() / (double)RAND_MAX - 0.5);
+            x[(size_t)l * N + n] = v;
+            s[(size_t)n * LP + l] = v;
+        }
+    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+    emu_pass<N, R0, 1, S, L, LP>(s, tw);
+    if constexpr (R1 != 0) emu_pass<N, R1, R0, S, L, LP>(s, tw);
+    if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, L, LP>(s, tw);
+    double err = 0, mag = 0;
+    for (int l = 0; l < L; l++)
+        for (int k = 0; k < N; k++) {
+            long double re = 0, im = 0;
+            for (int n = 0; n < N; n++) {
+                long double a = S * 6.283185307179586476925286766559005768L * (long double)((long)k * n % N) / N;
+                long double c = cosl(a), sn = sinl(a);
+                double2 v = x[(size_t)l * N + n];
+                re += v.x * c - v.y * sn;
+                im += v.x * sn + v.y * c;
+            }
+            double2 g = s[(size_t)k * LP + l];
+            err = fmax(err, fabs((double)(g.x - re)) + fabs((double)(g.y - im)));
+            mag = fmax(mag, fabs((double)re) + fabs((double)im));
+        }
+    return err / mag;
+}
+
+#define RUN(N)                                                                   \
+    do {                                                                         \
+        double e1 = check<N, -1, 8, 9>(), e2 = check<N, +1, 3, 5>();             \
+        printf("N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                          \
+        if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                  \
+    } while (0)
+
+int main() {
+    int bad = 0;
+    RUN(16); RUN(24); RUN(32); RUN(40); RUN(48); RUN(56); RUN(64); RUN(80); RUN(96);
+    RUN(112); RUN(128); RUN(160); RUN(192); RUN(224); RUN(256); RUN(320); RUN(384);
+    RUN(448); RUN(512); RUN(640); RUN(768); RUN(896); RUN(1024);
+    printf(bad ? "FAIL\n" : "OK\n");
+    return bad ? 1 : 0;
+}

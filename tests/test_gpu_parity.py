@@ -1,0 +1,242 @@
+"""Parity of the CUDA RK3 step with the CPU oracle, through the C-ABI.
+
+Tolerances (FP64 plain form): u within 1e-10 relative L2 after 1 and 10 steps,
+E(k) and epsilon within 1e-8 over 100 steps, particle positions within 1e-10
+after 10 steps, div u at round-off.  Both sides start from the same state.
+"""
+import numpy as np
+import pytest
+
+from helpers import divergence, rel_l2, rel_l2_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(pandora, p, init="oracle"):
+    import oracle as O
+    o = O.Oracle(p)
+    s = pandora.Simulation(p)
+    if init == "oracle":
+        o.init_fluid()
+        s.set_state(o.get_state())
+    else:
+        s.init_fluid()
+        o.set_state(s.get_state())
+    return o, s
+
+
+def test_nonlinear_known_answer(gpu_lib):
+    """src/ptf_rk3.f90:1115-1191: L1 norms of NL-hat = 3/4, 9/8, 11/8."""
+    import oracle as O
+    p = gpu_lib.default_params(32)
+    o = O.Oracle(p)
+    o.init_taylor_green_reverse()
+    with gpu_lib.Simulation(p) as s:
+        s.set_state(o.get_state())
+        nl = s.nonlinear()
+    l1 = [float(np.abs(c.real).sum() + np.abs(c.imag).sum()) for c in nl]
+    assert np.allclose(l1, [0.75, 1.125, 1.375], rtol=1e-12, atol=0), l1
+    assert rel_l2_fields(nl, o.nonlinear()) < 1e-13
+
+
+@pytest.mark.parametrize("n", [16, 24, 32, 48, 64])
+def test_nonlinear_matches_oracle(gpu_lib, n):
+    p = gpu_lib.workload_params("iso_decay", n)
+    o, s = _pair(gpu_lib, p)
+    nl_g = s.nonlinear()
+    nl_o = o.nonlinear()
+    s.close()
+    assert rel_l2_fields(nl_g, nl_o) < 1e-13
+
+
+def test_nonlinear_anisotropic_grid(gpu_lib):
+    p = gpu_lib.workload_params("iso_decay", 32)
+    p.nodes_x, p.nodes_y, p.nodes_z = 32, 48, 64
+    o, s = _pair(gpu_lib, p)
+    e = rel_l2_fields(s.nonlinear(), o.nonlinear())
+    s.close()
+    assert e < 1e-13
+
+
+def test_init_fluid_matches_oracle(gpu_lib):
+    import oracle as O
+    p = gpu_lib.workload_params("iso_decay", 64)
+    o = O.Oracle(p)
+    o.init_fluid()
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        ug = s.get_state()
+    uo = o.get_state()
+    assert rel_l2_fields(ug, uo) < 1e-13
+    # conjugate symmetry of the i=0 plane: u(0,-j,-k) = conj u(0,j,k)
+    for c in ug:
+        pl = c[0]
+        flip = np.conj(np.roll(pl[::-1, ::-1], 1, axis=(0, 1)))
+        assert np.abs(pl - flip).max() < 1e-15
+
+
+@pytest.mark.parametrize("n", [32, 64])
+def test_step_parity_decay(gpu_lib, n):
+    """1 and 10 steps of decaying isotropic turbulence: rel L2 of u < 1e-10."""
+    p = gpu_lib.workload_params("iso_decay", n)
+    o, s = _pair(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 11):
+        t, dt = o.step(step, t)
+        dtg = s.step(step)
+        assert dtg == pytest.approx(dt, rel=0, abs=0)
+        if step in (1, 10):
+            e = rel_l2_fields(s.get_state(), o.get_state())
+            assert e < 1e-10, (step, e)
+    assert s.simtime == pytest.approx(t, rel=1e-15)
+    div = divergence(p, s.get_state())
+    umax = max(np.abs(c).max() for c in s.get_state())
+    assert np.abs(div).max() < 1e-13 * max(umax, 1.0) * (n / 3)
+    # RK registers match too
+    assert rel_l2_fields(s.get_rk(), o.get_rk()) < 1e-10
+    s.close()
+
+
+def test_stats_parity_100_steps(gpu_lib):
+    """E(k) and epsilon within 1e-8 over 100 steps (32^3 decaying turbulence)."""
+    p = gpu_lib.workload_params("iso_decay", 32)
+    o, s = _pair(gpu_lib, p)
+    t = 0.0
+    worst_e, worst_eps = 0.0, 0.0
+    for step in range(1, 101):
+        ek_g, tke_g, eps_g, _ = s.stats()
+        ek_o, tke_o, eps_o = o.stats()
+        worst_e = max(worst_e, rel_l2(ek_g, ek_o))
+        worst_eps = max(worst_eps, abs(eps_g - eps_o) / abs(eps_o))
+        assert tke_g == pytest.approx(tke_o, rel=1e-8)
+        t, _ = o.step(step, t)
+        s.step(step)
+    # the statistics recorded inside the step (stage 1) are those of the state at step start
+    ek_l, tke_l, eps_l, ucfl_l = s.stats(last_step=True)
+    s.close()
+    assert worst_e < 1e-8 and worst_eps < 1e-8, (worst_e, worst_eps)
+    assert ucfl_l > 0
+
+
+def test_forced_parity(gpu_lib):
+    """Forced isotropic turbulence: OU forcing coefficients and u after 10 steps."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_track_part = 0
+    o, s = _pair(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 11):
+        t, _ = o.step(step, t)
+        s.step(step)
+        if step in (1, 10):
+            assert rel_l2_fields(s.get_forcing(), o.get_forcing()) < 1e-13, step
+            assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10, step
+    s.close()
+
+
+def test_particle_parity(gpu_lib):
+    """Tracers: positions within 1e-10 after 10 steps (same initial positions)."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 4096
+    o, s = _pair(gpu_lib, p)
+    s.init_particles()
+    xp, up, ur, pr, dp = s.get_particles()
+    o.set_particles(xp, up, ur, pr, dp)
+    t = 0.0
+    for step in range(1, 11):
+        t, _ = o.step(step, t)
+        s.step(step)
+        if step in (1, 10):
+            xg = s.get_particles()[0]
+            xo = o.get_particles(p.p_np_global)[0]
+            d = np.abs(xg - xo)
+            d = np.minimum(d, 2 * np.pi - d)      # a wrap on one side only is not an error
+            assert d.max() < 1e-10, (step, d.max())
+    # physical velocity materialised for the particles matches the oracle's
+    assert rel_l2_fields(s.physical_velocity(), o.get_physical()) < 1e-12
+    s.check_status()
+    s.close()
+
+
+def test_particle_init_matches_oracle(gpu_lib):
+    import oracle as O
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 10000
+    o = O.Oracle(p)
+    o.init_particles()
+    with gpu_lib.Simulation(p) as s:
+        s.init_particles()
+        xg = s.get_particles()[0]
+    xo = o.get_particles(p.p_np_global)[0]
+    assert np.abs(xg - xo).max() < 1e-14
+    dx = 2 * np.pi / 32
+    assert xg.min() >= -dx / 2 and xg.max() < 2 * np.pi - dx / 2
+
+
+def test_inertial_particles(gpu_lib):
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 1024
+    p.p_dia_vals = 0.01
+    p.p_rho = 1000.0
+    o, s = _pair(gpu_lib, p)
+    s.init_particles()
+    o.set_particles(*s.get_particles())
+    t = 0.0
+    for step in range(1, 6):
+        t, _ = o.step(step, t)
+        s.step(step)
+    xg, ug = s.get_particles()[:2]
+    xo, uo = o.get_particles(p.p_np_global)[:2]
+    s.close()
+    assert rel_l2(ug, uo) < 1e-10
+    d = np.abs(xg - xo)
+    assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
+
+
+def test_stage_api_matches_step(gpu_lib):
+    """f_RK3Stage1..3 called one by one equals g_RK3Calc."""
+    p = gpu_lib.workload_params("iso_decay", 32)
+    a = gpu_lib.Simulation(p)
+    b = gpu_lib.Simulation(p)
+    a.init_fluid()
+    b.init_fluid()
+    a.step(1)
+    dt = 0.0
+    dt = gpu_lib.f_RK3Stage1(1, 0.0, dt, sim=b)
+    dt = gpu_lib.f_RK3Stage2(1, dt / 3, dt, sim=b)
+    dt = gpu_lib.f_RK3Stage3(1, 0.75 * dt, dt, sim=b)
+    e = rel_l2_fields(a.get_state(), b.get_state())
+    a.close()
+    b.close()
+    assert e < 1e-15
+
+
+def test_advance_matches_steps(gpu_lib):
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 512
+    a = gpu_lib.Simulation(p)
+    b = gpu_lib.Simulation(p)
+    for s in (a, b):
+        s.init_fluid()
+        s.init_particles()
+    for _ in range(5):
+        a.step()
+    b.advance(5)
+    assert b.simtime == pytest.approx(a.simtime, rel=1e-15)
+    assert rel_l2_fields(a.get_state(), b.get_state()) < 1e-15
+    assert np.array_equal(a.get_particles()[0], b.get_particles()[0])
+    a.close()
+    b.close()
+
+
+def test_nan_detection(gpu_lib):
+    p = gpu_lib.workload_params("iso_decay", 16)
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        u = s.get_state()
+        u[0][1, 1, 1] = np.nan
+        s.set_state(u)
+        with pytest.raises(gpu_lib.PandoraError) as ei:
+            s.check_status()
+        assert ei.value.status == -4
+        s.init_fluid()
+        s.check_status()   # status word was cleared and the state is finite again
