@@ -1,0 +1,340 @@
+"""Benchmark of the PANDORA 2.0 RK3 time step on B200.
+
+Workload (default): forced isotropic turbulence at 256^3, FP64, OU forcing on
+|k| <= 2.5, 2^20 tracers with 4th-order interpolation advanced at every stage;
+synthetic seeded initial field (Ahmed/Elghobashi spectrum, kp = 3).  A "step" is
+one full RK3 step (three stages, statistics at stage 1, forcing, particles).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas, one process per GPU (launched by torchrun):
+the path has no exchange step on one field, so there is no collective in the
+data path; the barrier and the max-over-ranks timing use torch.distributed.
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pandora-2.0_b200"))
+
+METRIC = "Mpts·RK3steps/s"
+WORKLOAD = "iso_forced_particles"
+# per-launch DRAM traffic (read + write) of the dominant pass, from the ncu capture
+# summarised in profiles/ (None until captured for this workload)
+NCU_TRAFFIC_BYTES = {}
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--np", type=int, default=1 << 20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _params(a):
+    from pandora.params import workload_params
+    p = workload_params(a.workload, a.n)
+    if p.p_track_part:
+        p.p_np_global = a.np
+    return p
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = sorted(v for v in (num(r[1]) for r in self.rows) if v is not None)
+        smax = max((v for v in (num(r[2]) for r in self.rows) if v is not None), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(p, stages: int = 3):
+    """The oracle (CPU restatement of the reference, OpenMP) on the host cores:
+    `stages` RK3 stages of the same workload.  Returns (Mpts*steps/s, cores, secs)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.Oracle(p)
+    o.init_fluid()
+    if p.p_track_part:
+        o.init_particles()
+    dt = 0.0
+    t0 = time.perf_counter()
+    for s in range(1, stages + 1):
+        dt = o.stage(s, 1, dt)
+    secs = time.perf_counter() - t0
+    npts = p.nodes_x * p.nodes_y * p.nodes_z
+    o.close()
+    return npts * (stages / 3.0) / secs / 1e6, O.threads(), secs
+
+
+def run_reference(a, p):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    o = O.Oracle(p)
+    o.init_fluid()
+    if p.p_track_part:
+        o.init_particles()
+    npts = p.nodes_x * p.nodes_y * p.nodes_z
+    dt = 0.0
+    stage = 0
+    # each bench step = one RK3 stage (1/3 of a time step) of the full workload
+    for _ in range(a.warmup):
+        dt = o.stage(stage % 3 + 1, 1 + stage // 3, dt)
+        stage += 1
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        dt = o.stage(stage % 3 + 1, 1 + stage // 3, dt)
+        stage += 1
+    secs = time.perf_counter() - t0
+    value = npts * (a.steps / 3.0) / secs / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps * 3.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Rogallo field, seeded tracers)",
+        "config": _config(a, p),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": O.threads(), "kind": "port",
+                         "sample": f"{a.steps} RK3 stages (1/3 step each) of the full workload; the reference "
+                                   "binary (Fortran+MPI+PETSc+FFTW) has no toolchain on this image, so this "
+                                   "is the C restatement of its algorithm (oracle/pandora_oracle.c)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _config(a, p):
+    return {"workload": f"{a.workload} {p.nodes_x}^3 FP64 plain, OU forcing |k|<=2.5, "
+                        f"{int(p.p_np_global) if p.p_track_part else 0} tracers (order {p.p_interp_order})",
+            "grid": [p.nodes_x, p.nodes_y, p.nodes_z], "nu": p.f_nu, "dt": p.rk3_dt,
+            "particles": int(p.p_np_global) if p.p_track_part else 0, "form": "fp64_plain",
+            "parallelism": f"replicas x{a.gpus}",
+            "l2": "no flush needed: every pass streams > 0.3 GB (working set ~1.6 GB > 126 MB L2)"}
+
+
+def run_ours(a, p):
+    import torch
+    import pandora
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    p.seed_fluid = 1 + rank
+    p.seed_force = 1000 + rank
+    p.seed_particles = 2000 + rank
+    sim = pandora.Simulation(p)
+    sim.init_fluid()
+    if p.p_track_part:
+        sim.init_particles()
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    npts = p.nodes_x * p.nodes_y * p.nodes_z
+
+    # warm-up (builds the CUDA graph of one step)
+    sim.advance(max(a.warmup, 3), sync=True)
+    sim.check_status()
+
+    # ---- device-resident timing ----
+    sampler = ClockSampler(dev)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.advance(a.steps, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    sim.check_status()
+
+    # ---- end to end through the C-ABI: one synchronous g_RK3Calc call per step
+    # (host scalars tstep/simtime in, dt/simtime out) plus the step's statistics
+    # (E(k), tke, eps, ucfl) read back to the host ----
+    n_e2e = max(1, min(a.steps, 200))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        sim.step()
+        sim.stats(last_step=True)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    sampler.stop()
+    clocks = sampler.summary()
+
+    # ---- roofline of the dominant pass, timed alone with CUDA events ----
+    peak, peak_kind = _peaks()
+    passes = {1: "zpass_inv", 2: "ypass_inv", 3: "xpass_nl", 4: "ypass_fwd", 5: "zpass_fwd_update",
+              6: "particles"}
+    per_pass = {}
+    reps = 20
+    for pid, name in passes.items():
+        if pid == 6 and not p.p_track_part:
+            continue
+        sim.profile_pass(pid, 2)
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        sim.profile_pass(pid, reps)
+        q1.record(stream)
+        torch.cuda.synchronize()
+        dur = q0.elapsed_time(q1) / reps / 1e3
+        b = sim.pass_bytes(pid)
+        per_pass[name] = {"ms": dur * 1e3, "gbs": b / dur / 1e9, "bytes": b}
+    dom = max(per_pass, key=lambda k: per_pass[k]["ms"])
+    dom_gbs = per_pass[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": peak, "unit": "GB/s",
+                "frac": dom_gbs / peak, "peak_kind": f"{peak_kind} (burst copy)",
+                "traffic": NCU_TRAFFIC_BYTES.get((a.n, dom)),
+                "per_pass": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)} for k, v in per_pass.items()}}
+    launches = sim.launches_per_step()
+    value = npts * a.steps * ws / (ms / 1e3) / 1e6
+    e2e_value = npts * n_e2e * ws / e2e_s / 1e6
+    kk = sim.kkmax
+    d2h = 48 + 8 * (2 * (kk + 1) + 3) + 48
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Rogallo field, seeded tracers)",
+        "config": _config(a, p),
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": d2h,
+                "steps": n_e2e, "what": "pandora_rk3_step + pandora_last_step_stats per step, host wall clock"},
+        "gpu_launches": launches * a.steps,
+        "roofline": roofline,
+        "step_model_gbs": None,
+    }
+    # whole-step algorithmic bytes (5-pass model incl. particles and stage-1 stats)
+    step_bytes = 0.0
+    for pid in (1, 2, 3, 4, 5):
+        step_bytes += 3 * sim.pass_bytes(pid)
+    if p.p_track_part:
+        step_bytes += 3 * sim.pass_bytes(6)
+    step_bytes += sim.pass_bytes(7)
+    line["step_model_gbs"] = {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms / a.steps / 1e3) / 1e9,
+                              "frac": step_bytes / (ms / a.steps / 1e3) / 1e9 / peak}
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        v, cores, secs = cpu_baseline(_params(a))
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                                "sample": f"one RK3 step (3 stages) of the same workload on the host, "
+                                          f"{secs:.1f} s, OpenMP C restatement (oracle/pandora_oracle.c)"}
+    sim.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    a = _args()
+    p = _params(a)
+    if a.impl == "reference":
+        return run_reference(a, p)
+    return run_ours(a, p)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -633,3 +633,49 @@ extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
     *n = h->launches_per_step;
     return PANDORA_OK;
 }
+
+extern "C" int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps) {
+    if (!h || reps < 0) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    const bool part = h->particles_on && h->P.np > 0;
+    Fields Fs = h->F;
+    Fs.shell = h->shell_now;
+    for (int r = 0; r < reps; r++) {
+        switch (pass) {
+        case 1: PD_CK(launch_zpass_inv(h->g, h->F, 2, h->st)); break;
+        case 2: PD_CK(launch_ypass_inv(h->g, h->F, h->st)); break;
+        case 3: PD_CK(launch_xpass(h->g, h->F, part ? 1 : 0, 0, h->st)); break;
+        case 4: PD_CK(launch_ypass_fwd(h->g, h->F, h->st)); break;
+        case 5: PD_CK(launch_zpass_fwd_update(h->g, h->F, 2, 0, h->st)); break;
+        case 6:
+            if (!part) return PANDORA_ERR_INVALID_ARG;
+            PD_CK(launch_particles(h->g, h->F, h->P, h->pp, 2, h->st));
+            break;
+        case 7: PD_CK(launch_stats(h->g, Fs, h->st)); break;
+        default: return PANDORA_ERR_INVALID_ARG;
+        }
+    }
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes) {
+    if (!h || !bytes) return PANDORA_ERR_INVALID_ARG;
+    const Geo& g = h->g;
+    const double c16 = 16.0;
+    const double S = (double)g.S;
+    const double Z = (double)g.nz * g.nkj * g.nki;
+    const double Y = (double)g.nz * g.ny * g.nki;
+    const double R = (double)g.R;
+    const bool part = h->particles_on && h->P.np > 0;
+    switch (pass) {
+    case 1: *bytes = c16 * (3 * S + 6 * Z); break;
+    case 2: *bytes = c16 * (6 * Z + 6 * Y); break;
+    case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? 8.0 * 3 * R : 0.0); break;
+    case 4: *bytes = c16 * (3 * Y + 3 * Z); break;
+    case 5: *bytes = c16 * (3 * Z + 6 * S + 6 * S); break;
+    case 6: *bytes = part ? 8.0 * (3 * R + 24.0 * (double)h->P.np) : 0.0; break;
+    case 7: *bytes = c16 * 3 * S; break;
+    default: return PANDORA_ERR_INVALID_ARG;
+    }
+    return PANDORA_OK;
+}

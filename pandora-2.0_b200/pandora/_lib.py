@@ -71,6 +71,8 @@ SIGNATURES = {
     "pandora_get_physical_velocity": [_vp, _dp, _dp, _dp],
     "pandora_check_status": [_vp],
     "pandora_launches_per_step": [_vp, ctypes.POINTER(_i32)],
+    "pandora_profile_pass": [_vp, _i32, _i32],
+    "pandora_pass_bytes": [_vp, _i32, _dp],
 }
 _RESTYPES = {"pandora_strerror": ctypes.c_char_p}
 

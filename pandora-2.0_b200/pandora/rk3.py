@@ -120,10 +120,9 @@ class Simulation:
 
     def set_particles(self, xp, up=None, up_rk3=None, rk3=None, dp=None):
         n = len(xp)
-        f = lambda a: None if a is None else _dp(_keep.setdefault(id(a), _as_f64(a)))
-        _keep: dict = {}
-        _lib.check(self.L.pandora_set_particles(self.h, n, f(xp), f(up), f(up_rk3), f(rk3), f(dp)),
-                   "pandora_set_particles")
+        held = [None if a is None else _as_f64(a) for a in (xp, up, up_rk3, rk3, dp)]
+        ptrs = [None if a is None else _dp(a) for a in held]
+        _lib.check(self.L.pandora_set_particles(self.h, n, *ptrs), "pandora_set_particles")
 
     def get_particles(self):
         n = self.np
@@ -178,6 +177,14 @@ class Simulation:
 
     def check_status(self) -> None:
         _lib.check(self.L.pandora_check_status(self.h), "pandora_check_status")
+
+    def profile_pass(self, pass_id: int, reps: int) -> None:
+        _lib.check(self.L.pandora_profile_pass(self.h, pass_id, reps), "pandora_profile_pass")
+
+    def pass_bytes(self, pass_id: int) -> float:
+        b = ctypes.c_double()
+        _lib.check(self.L.pandora_pass_bytes(self.h, pass_id, ctypes.byref(b)), "pandora_pass_bytes")
+        return b.value
 
     def launches_per_step(self) -> int:
         n = ctypes.c_int32()
