@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
         if (i != 0) { q11 *= 2.0; q22 *= 2.0; q33 *= 2.0; }
         p11 += q11; p22 += q22; p33 += q33;
         const double e = 0.5 * (q11 + q22 + q33);
+        if (!isfinite(e)) atomicOr(&F.clock->status, PD_ST_NAN);
         const double d = 2.0 * km * km * g.nu * e;
         const int kc = (int)floor(km + 0.5);
         for (int q = kc - 1; q <= kc + 1; q++) {

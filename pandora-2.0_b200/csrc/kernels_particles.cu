@@ -1,13 +1,18 @@
 // kernels_particles.cu -- Lagrangian particle advance on sm_100a.
 //
-// One thread per particle: tensor-product Neville interpolation of the physical
-// velocity of the current stage (p_InterpInterpolate3D / FindMolecule /
+// One thread per particle: tensor-product Lagrange interpolation of order ORD
+// of the physical velocity of the current stage (the reference evaluates the
+// same polynomial by Neville's scheme, p_InterpInterpolate3D / FindMolecule /
 // Neville3D, src/pp_interp.f90:313-560), the tracer or Stokes-drag RK3 update
 // (p_RK3SolveParticle, src/pp_rk3.f90:57-165, drag 927-946) and the periodic
 // wrap (p_MPICorrectPosition, src/pp_mpi.f90:1011-1057; x3 uses '>' where x1
 // and x2 use '>=').  The reference fetches a halo of NHALO = order/2 planes by
 // DMGlobalToLocal (src/pp_interp.f90:115-264); on one GPU the stencil indices
-// simply wrap modulo N.  Physical velocity layout: [c][z][y][x].
+// wrap modulo N.  Physical velocity layout: [c][z][y][x].
+//
+// Particles are kept sorted by spatial bin (z slowest), re-sorted once per step,
+// so that a wave of threads reads a compact set of velocity rows that stays in
+// L2 instead of gathering at random from a field larger than L2.
 #include <cuda_runtime.h>
 #include "pandora_internal.cuh"
 
@@ -15,7 +20,20 @@ namespace pd {
 
 constexpr int kMaxOrder = 6;
 
-__global__ void __launch_bounds__(256) k_particles(Particles P, Geo g, const double* __restrict__ phys,
+template <int ORD>
+__device__ __forceinline__ void lagrange_weights(double x, const double* nodes, double* w) {
+#pragma unroll
+    for (int m = 0; m < ORD; m++) {
+        double v = 1.0;
+#pragma unroll
+        for (int n = 0; n < ORD; n++)
+            if (n != m) v *= (x - nodes[n]) / (nodes[m] - nodes[n]);
+        w[m] = v;
+    }
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const double* __restrict__ phys,
                                                    Clock* ck, PartParams pp, int stage) {
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int tstep = ck->tstep;
@@ -25,7 +43,7 @@ __global__ void __launch_bounds__(256) k_particles(Particles P, Geo g, const dou
     if (stage == 1) { beta = 0.0; gamma = 1.0 / 3.0; }
     else if (stage == 2) { beta = -(5.0 / 9.0); gamma = 15.0 / 16.0; }
     else { beta = -(153.0 / 128.0); gamma = 8.0 / 15.0; }
-    const int ord = pp.order, nh = ord / 2;
+    constexpr int nh = ORD / 2;
     const double D[3] = {g.dx, g.dy, g.dz};
     const int NN[3] = {g.nx, g.ny, g.nz};
     double xp[3], up[3], ur[3], pr[3];
@@ -33,81 +51,73 @@ __global__ void __launch_bounds__(256) k_particles(Particles P, Geo g, const dou
     for (int c = 0; c < 3; c++) {
         xp[c] = P.xp[c][n]; up[c] = P.up[c][n]; ur[c] = P.uprk[c][n]; pr[c] = P.prk[c][n];
     }
-    // p_InterpFindMolecule: index arithmetic with explicit rounding (no contraction)
-    int i0[3];
-    double nodes[3][kMaxOrder];
+    // p_InterpFindMolecule: stencil start from the same rounded arithmetic
+    double w[3][ORD];
+    int idx[3][ORD];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         double halo = __dmul_rn((double)nh, D[c]);
         double xd;
-        if ((ord & 1) == 0) {
+        if ((ORD & 1) == 0) {
             halo = __dsub_rn(halo, __dmul_rn(0.5, D[c]));
             xd = __dadd_rn(__dadd_rn(__dadd_rn(xp[c], halo), D[c]), __dmul_rn(0.5, D[c]));
         } else {
             xd = __dadd_rn(__dadd_rn(xp[c], halo), __dmul_rn(0.5, D[c]));
         }
-        const int idx = (int)__ddiv_rn(xd, D[c]) - nh - nh;
-        i0[c] = idx;
-        for (int m = 0; m < ord; m++) nodes[c][m] = __dmul_rn((double)(idx + m), D[c]);
+        const int i0 = (int)__ddiv_rn(xd, D[c]) - nh - nh;
+        double nodes[ORD];
+#pragma unroll
+        for (int m = 0; m < ORD; m++) {
+            nodes[m] = __dmul_rn((double)(i0 + m), D[c]);
+            int q = (i0 + m) % NN[c];
+            idx[c][m] = q < 0 ? q + NN[c] : q;
+        }
+        lagrange_weights<ORD>(xp[c], nodes, w[c]);
     }
-    int X[kMaxOrder], Y[kMaxOrder], Z[kMaxOrder];
-    for (int m = 0; m < ord; m++) {
-        X[m] = ((i0[0] + m) % NN[0] + NN[0]) % NN[0];
-        Y[m] = ((i0[1] + m) % NN[1] + NN[1]) % NN[1];
-        Z[m] = ((i0[2] + m) % NN[2] + NN[2]) % NN[2];
-    }
-    // p_InterpNeville3D: along y for every (x, z), then along z for every x, then x.
+    long long rowoff[ORD][ORD];
+#pragma unroll
+    for (int zi = 0; zi < ORD; zi++)
+#pragma unroll
+        for (int yi = 0; yi < ORD; yi++) rowoff[zi][yi] = ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx;
     double uf[3];
+#pragma unroll
     for (int c = 0; c < 3; c++) {
         const double* f = phys + (long long)c * g.R;
-        double vz[kMaxOrder][kMaxOrder];   // [xi][zi] after the y sweep
-        for (int zi = 0; zi < ord; zi++) {
-            for (int xi = 0; xi < ord; xi++) {
-                double v[kMaxOrder];
-                for (int yi = 0; yi < ord; yi++)
-                    v[yi] = __ldg(&f[((long long)Z[zi] * g.ny + Y[yi]) * g.nx + X[xi]]);
-                for (int col = 1; col <= ord - 1; col++)
-                    for (int nv = 0; nv < ord - col; nv++) {
-                        const double d1 = xp[1] - nodes[1][nv + col], d2 = nodes[1][nv] - xp[1];
-                        const double d3 = nodes[1][nv] - nodes[1][nv + col];
-                        v[nv] = ((d1 * v[nv]) + (d2 * v[nv + 1])) / d3;
-                    }
-                vz[xi][zi] = v[0];
+        double acc_z = 0.0;
+#pragma unroll
+        for (int zi = 0; zi < ORD; zi++) {
+            double acc_y = 0.0;
+#pragma unroll
+            for (int yi = 0; yi < ORD; yi++) {
+                const double* row = f + rowoff[zi][yi];
+                double acc_x = 0.0;
+#pragma unroll
+                for (int xi = 0; xi < ORD; xi++) acc_x += w[0][xi] * __ldg(row + idx[0][xi]);
+                acc_y += w[1][yi] * acc_x;
             }
+            acc_z += w[2][zi] * acc_y;
         }
-        double vx[kMaxOrder];
-        for (int xi = 0; xi < ord; xi++) {
-            for (int col = 1; col <= ord - 1; col++)
-                for (int nv = 0; nv < ord - col; nv++) {
-                    const double d1 = xp[2] - nodes[2][nv + col], d2 = nodes[2][nv] - xp[2];
-                    const double d3 = nodes[2][nv] - nodes[2][nv + col];
-                    vz[xi][nv] = ((d1 * vz[xi][nv]) + (d2 * vz[xi][nv + 1])) / d3;
-                }
-            vx[xi] = vz[xi][0];
-        }
-        for (int col = 1; col <= ord - 1; col++)
-            for (int nv = 0; nv < ord - col; nv++) {
-                const double d1 = xp[0] - nodes[0][nv + col], d2 = nodes[0][nv] - xp[0];
-                const double d3 = nodes[0][nv] - nodes[0][nv + col];
-                vx[nv] = ((d1 * vx[nv]) + (d2 * vx[nv + 1])) / d3;
-            }
-        uf[c] = vx[0];
+        uf[c] = acc_z;
     }
     // p_ControlInitPartVelocity at the release step (src/pp_control.f90:378-416)
     if (tstep == pp.release && stage == 1) {
+#pragma unroll
         for (int c = 0; c < 3; c++) { up[c] = uf[c]; pr[c] = 0.0; ur[c] = 0.0; }
     }
     const double dpv = P.dp[n];
     if (dpv > 0.0) {
         const double tau = ((dpv * dpv) / (18.0 * pp.f_nu)) * (pp.p_rho / pp.f_rho);
+#pragma unroll
         for (int c = 0; c < 3; c++) {
             const double acc = (uf[c] - up[c]) / tau;
             pr[c] = (beta * pr[c]) + acc;
             up[c] = up[c] + (gamma * dt * pr[c]);
         }
     } else {
+#pragma unroll
         for (int c = 0; c < 3; c++) up[c] = uf[c];
     }
+#pragma unroll
     for (int c = 0; c < 3; c++) {
         ur[c] = (beta * ur[c]) + up[c];
         xp[c] = xp[c] + (gamma * dt * ur[c]);
@@ -140,14 +150,106 @@ __global__ void k_init_particles(Particles P, Geo g, uint64_t key, double dia) {
         P.up[c][n] = 0.0; P.uprk[c][n] = 0.0; P.prk[c][n] = 0.0;
     }
     P.dp[n] = dia;
+    P.pid[n] = n;
+}
+
+// ---------------------------------------------------------------------------
+// Spatial sort: counting sort by bin (z slowest, then y, then x).  Bins are
+// whole blocks of cells; positions lie in [-d/2, L-d/2) after the wrap, so
+// x + d/2 is in [0, L).  Order inside a bin follows atomics; every particle's
+// update is independent of the order, and pid keeps the caller's numbering.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int bin_of(double x, double d, int cells, int nb) {
+    int b = (int)floor((x + 0.5 * d) / (d * cells));
+    return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+}
+
+__global__ void k_part_key(Particles P, Geo g, PartSort s) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.np) return;
+    const int bx = bin_of(P.xp[0][n], g.dx, s.bin_cells[0], s.nb[0]);
+    const int by = bin_of(P.xp[1][n], g.dy, s.bin_cells[1], s.nb[1]);
+    const int bz = bin_of(P.xp[2][n], g.dz, s.bin_cells[2], s.nb[2]);
+    const unsigned k = ((unsigned)bz * s.nb[1] + by) * s.nb[0] + bx;
+    s.key[n] = k;
+    atomicAdd(&s.count[k], 1u);
+}
+
+// exclusive scan of count[0..n) in place: per-block scan of 1024 entries ...
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* warp_tot, unsigned& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned t = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        warp_tot[lane] = t;   // inclusive prefix of warp totals
+    }
+    __syncthreads();
+    total = warp_tot[(blockDim.x >> 5) - 1];
+    const unsigned base = wid ? warp_tot[wid - 1] : 0u;
+    return base + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(unsigned* a, unsigned* sums, long long n) {
+    __shared__ unsigned wt[32];
+    const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+    const unsigned v = i < n ? a[i] : 0u;
+    unsigned total;
+    const unsigned ex = block_exclusive_scan(v, wt, total);
+    if (i < n) a[i] = ex;
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+// ... one block scans the block totals (at most 1024 of them) ...
+__global__ void __launch_bounds__(1024) k_scan_sums(unsigned* sums, int nblocks) {
+    __shared__ unsigned wt[32];
+    const unsigned v = threadIdx.x < (unsigned)nblocks ? sums[threadIdx.x] : 0u;
+    unsigned total;
+    const unsigned ex = block_exclusive_scan(v, wt, total);
+    if (threadIdx.x < (unsigned)nblocks) sums[threadIdx.x] = ex;
+}
+
+// ... and the block offsets are added back.
+__global__ void __launch_bounds__(1024) k_scan_add(unsigned* a, const unsigned* sums, long long n) {
+    const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+    if (i < n) a[i] += sums[blockIdx.x];
+}
+
+__global__ void k_part_scatter(Particles src, PartSort s) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= src.np) return;
+    const long long d = atomicAdd(&s.count[s.key[n]], 1u);
+    const Particles& t = s.tmp;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        t.xp[c][d] = src.xp[c][n]; t.up[c][d] = src.up[c][n];
+        t.uprk[c][d] = src.uprk[c][n]; t.prk[c][d] = src.prk[c][n];
+    }
+    t.dp[d] = src.dp[n];
+    t.pid[d] = src.pid[n];
 }
 
 cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp, int stage,
                              cudaStream_t st) {
     if (p.np == 0) return cudaSuccess;
-    if (pp.order < 1 || pp.order > kMaxOrder) return cudaErrorInvalidValue;
-    const long long nb = (p.np + 255) / 256;
-    k_particles<<<(unsigned)nb, 256, 0, st>>>(p, g, f.phys, f.clock, pp, stage);
+    const unsigned nb = (unsigned)((p.np + 255) / 256);
+    switch (pp.order) {
+#define PD_ORD(O) case O: k_particles<O><<<nb, 256, 0, st>>>(p, g, f.phys, f.clock, pp, stage); break;
+        PD_ORD(1) PD_ORD(2) PD_ORD(3) PD_ORD(4) PD_ORD(5) PD_ORD(6)
+#undef PD_ORD
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
@@ -156,6 +258,29 @@ cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key
     const long long nb = (p.np + 255) / 256;
     k_init_particles<<<(unsigned)nb, 256, 0, st>>>(p, g, key, dia);
     return cudaGetLastError();
+}
+
+// Sorts P by bin into s.tmp, then copies back into P's storage (so that the
+// pointers captured in the step's CUDA graph stay valid).
+cudaError_t launch_particle_sort(const Geo& g, const Particles& P, const PartSort& s, cudaStream_t st,
+                                 int* nlaunch) {
+    if (P.np == 0) return cudaSuccess;
+    const long long nbins = (long long)s.nb[0] * s.nb[1] * s.nb[2];
+    const int nblk = (int)((nbins + 1023) / 1024);
+    if (nblk > 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(s.count, 0, sizeof(unsigned) * nbins, st);
+    if (e) return e;
+    const unsigned pb = (unsigned)((P.np + 255) / 256);
+    k_part_key<<<pb, 256, 0, st>>>(P, g, s);
+    k_scan_blocks<<<nblk, 1024, 0, st>>>(s.count, s.block_sums, nbins);
+    k_scan_sums<<<1, 1024, 0, st>>>(s.block_sums, nblk);
+    k_scan_add<<<nblk, 1024, 0, st>>>(s.count, s.block_sums, nbins);
+    k_part_scatter<<<pb, 256, 0, st>>>(P, s);
+    if ((e = cudaGetLastError())) return e;
+    // the 13 double arrays and pid are contiguous in both buffers (14 * np words)
+    e = cudaMemcpyAsync(P.xp[0], s.tmp.xp[0], sizeof(double) * 14 * (size_t)P.np, cudaMemcpyDeviceToDevice, st);
+    if (nlaunch) *nlaunch += 5;
+    return e;
 }
 
 }  // namespace pd

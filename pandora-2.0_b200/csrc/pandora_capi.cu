@@ -35,7 +35,9 @@ struct pandora_handle {
     ForceParams fp{};
     PartParams pp{};
     Particles P{};
-    double* pbuf = nullptr;
+    double* pbuf = nullptr;           // 13 * np doubles + np pid
+    double* pbuf2 = nullptr;          // sort destination, same layout
+    PartSort sort{};
     double2* nlbuf = nullptr;         // scratch for pandora_nonlinear
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -132,7 +134,8 @@ static void release(pandora_handle* h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     cudaFree(h->fbuf); cudaFree(h->F.zb); cudaFree(h->F.yb); cudaFree(h->F.phys);
     cudaFree(h->F.forcing); cudaFree(h->tw); cudaFree(h->clock); cudaFree(h->shell_step);
-    cudaFree(h->shell_now); cudaFree(h->pbuf); cudaFree(h->nlbuf);
+    cudaFree(h->shell_now); cudaFree(h->pbuf); cudaFree(h->pbuf2); cudaFree(h->nlbuf);
+    cudaFree(h->sort.key); cudaFree(h->sort.count); cudaFree(h->sort.block_sums);
     if (h->clock_host) cudaFreeHost(h->clock_host);
     if (h->shell_host) cudaFreeHost(h->shell_host);
     if (h->own) cudaStreamDestroy(h->own);
@@ -271,16 +274,41 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     }
     if (h->particles_on && p->p_np_global > 0) {
         const long long np = p->p_np_global;
-        if ((e = cudaMalloc((void**)&h->pbuf, sizeof(double) * 13 * (size_t)np)) != cudaSuccess) {
+        PartSort& so = h->sort;
+        const int lens[3] = {g.nx, g.ny, g.nz};
+        long long nbins = 1;
+        for (int d = 0; d < 3; d++) {
+            int cells = 4;
+            while ((lens[d] + cells - 1) / cells > 64) cells *= 2;
+            so.bin_cells[d] = cells;
+            so.nb[d] = (lens[d] + cells - 1) / cells;
+            nbins *= so.nb[d];
+        }
+        const size_t pbytes = sizeof(double) * 14 * (size_t)np;
+        if (cudaMalloc((void**)&h->pbuf, pbytes) != cudaSuccess ||
+            cudaMalloc((void**)&h->pbuf2, pbytes) != cudaSuccess ||
+            cudaMalloc((void**)&so.key, sizeof(unsigned) * (size_t)np) != cudaSuccess ||
+            cudaMalloc((void**)&so.count, sizeof(unsigned) * (size_t)nbins) != cudaSuccess ||
+            cudaMalloc((void**)&so.block_sums, sizeof(unsigned) * 1024) != cudaSuccess) {
             cudaGetLastError(); release(h); return PANDORA_ERR_OOM;
         }
-        cudaMemsetAsync(h->pbuf, 0, sizeof(double) * 13 * (size_t)np, h->st);
-        h->P.np = np;
-        for (int c = 0; c < 3; c++) {
-            h->P.xp[c] = h->pbuf + (0 + c) * np; h->P.up[c] = h->pbuf + (3 + c) * np;
-            h->P.uprk[c] = h->pbuf + (6 + c) * np; h->P.prk[c] = h->pbuf + (9 + c) * np;
+        cudaMemsetAsync(h->pbuf, 0, pbytes, h->st);
+        auto bind = [np](Particles& P, double* b) {
+            P.np = np;
+            for (int c = 0; c < 3; c++) {
+                P.xp[c] = b + (0 + c) * np; P.up[c] = b + (3 + c) * np;
+                P.uprk[c] = b + (6 + c) * np; P.prk[c] = b + (9 + c) * np;
+            }
+            P.dp = b + 12 * np;
+            P.pid = (long long*)(b + 13 * np);
+        };
+        bind(h->P, h->pbuf);
+        bind(so.tmp, h->pbuf2);
+        std::vector<long long> ids((size_t)np);
+        for (long long n = 0; n < np; n++) ids[(size_t)n] = n;
+        if (cudaMemcpy(h->P.pid, ids.data(), sizeof(long long) * np, cudaMemcpyHostToDevice) != cudaSuccess) {
+            release(h); return PANDORA_ERR_CUDA;
         }
-        h->P.dp = h->pbuf + 12 * np;
     }
     *out = h;
     return PANDORA_OK;
@@ -389,7 +417,10 @@ extern "C" int pandora_set_particles(pandora_handle* h, int64_t np, const double
             for (int c = 0; c < 3; c++) soa[(size_t)(3 * a + c) * np + n] = srcs[a][3 * n + c];
     }
     if (dp) memcpy(&soa[(size_t)12 * np], dp, sizeof(double) * np);
+    std::vector<long long> ids((size_t)np);
+    for (int64_t n = 0; n < np; n++) ids[(size_t)n] = n;
     PD_CK(cudaMemcpyAsync(h->pbuf, soa.data(), sizeof(double) * soa.size(), cudaMemcpyHostToDevice, h->st));
+    PD_CK(cudaMemcpyAsync(h->P.pid, ids.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
     return PANDORA_OK;
 }
@@ -400,15 +431,21 @@ extern "C" int pandora_get_particles(pandora_handle* h, int64_t np, double* xp, 
     if (np == 0) return PANDORA_OK;
     cudaSetDevice(h->dev);
     std::vector<double> soa((size_t)13 * np);
+    std::vector<long long> ids((size_t)np);
     PD_CK(cudaMemcpyAsync(soa.data(), h->pbuf, sizeof(double) * soa.size(), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaMemcpyAsync(ids.data(), h->P.pid, sizeof(long long) * np, cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
+    // the device keeps particles sorted by bin; pid maps back to the caller's order
     double* dsts[4] = {xp, up, up_rk3, rk3};
-    for (int a = 0; a < 4; a++) {
-        if (!dsts[a]) continue;
-        for (int64_t n = 0; n < np; n++)
-            for (int c = 0; c < 3; c++) dsts[a][3 * n + c] = soa[(size_t)(3 * a + c) * np + n];
+    for (int64_t n = 0; n < np; n++) {
+        const long long q = ids[(size_t)n];
+        if (q < 0 || q >= np) return PANDORA_ERR_INVALID_ARG;
+        for (int a = 0; a < 4; a++) {
+            if (!dsts[a]) continue;
+            for (int c = 0; c < 3; c++) dsts[a][3 * q + c] = soa[(size_t)(3 * a + c) * np + n];
+        }
+        if (dp) dp[q] = soa[(size_t)12 * np + n];
     }
-    if (dp) memcpy(dp, &soa[(size_t)12 * np], sizeof(double) * np);
     return PANDORA_OK;
 }
 extern "C" int pandora_init_particles(pandora_handle* h) {
@@ -427,6 +464,9 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     const Geo& g = h->g;
     int n = 0;
     const bool part = h->particles_on && h->P.np > 0;
+    if (stage == 1 && part) {
+        PD_CK(launch_particle_sort(g, h->P, h->sort, h->st, &n));
+    }
     if (stage == 1) {
         Fields Fs = h->F;
         Fs.shell = h->shell_step;
@@ -628,7 +668,7 @@ extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
     if (!h->launches_per_step) {
         // count without launching: same sequence as enqueue_step
         const bool part = h->particles_on && h->P.np > 0;
-        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0));
+        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0)) + (part ? 5 : 0);
     }
     *n = h->launches_per_step;
     return PANDORA_OK;

@@ -78,6 +78,8 @@ struct Fields {
     double* shell;      // [2*(kkmax+1) + 3] shell sums (e, d) + p11,p22,p33
 };
 
+// Particle arrays, structure of arrays: 13 doubles + the particle's index in
+// the caller's order (pid).  The device keeps them sorted by spatial bin.
 struct Particles {
     long long np;
     double* xp[3];
@@ -85,6 +87,17 @@ struct Particles {
     double* uprk[3];
     double* prk[3];
     double* dp;
+    long long* pid;
+};
+
+// Scratch of the per-step spatial sort of the particles.
+struct PartSort {
+    int nb[3];                 // bins per direction
+    int bin_cells[3];          // cells per bin per direction
+    unsigned* key;             // [np]
+    unsigned* count;           // [nbins] counts, then exclusive offsets
+    unsigned* block_sums;      // [ceil(nbins/1024)]
+    Particles tmp;             // destination of the scatter
 };
 
 struct ForceParams {
@@ -130,6 +143,8 @@ cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, 
                              int stage, cudaStream_t st);
 cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia,
                                   cudaStream_t st);
+cudaError_t launch_particle_sort(const Geo& g, const Particles& p, const PartSort& s, cudaStream_t st,
+                                 int* nlaunch);
 cudaError_t launch_check_finite(const Geo& g, const Fields& f, cudaStream_t st);
 
 // Shared-memory configuration (set once per process per device).
