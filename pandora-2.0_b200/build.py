@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpandora_gpu.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu"]
+SOURCES = ["kernels_passes.cu", "kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu"]
 HEADERS = ["fft_core.cuh", "pandora_internal.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -46,7 +46,7 @@ def _compile(src: str) -> tuple[str, str]:
     return obj, r.stderr
 
 
-def build(force: bool = False, jobs: int = 3) -> str:
+def build(force: bool = False, jobs: int = 4) -> str:
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= _deps_mtime():
         return OUT
     os.makedirs(BUILD, exist_ok=True)

@@ -179,15 +179,21 @@ template <int N> constexpr bool plan_ok() {
     return Plan<N>::r0 * (Plan<N>::r1 ? Plan<N>::r1 : 1) * (Plan<N>::r2 ? Plan<N>::r2 : 1) == N;
 }
 
+// Row of element n in a tile: with PS > 0 one pad row follows every 2^PS rows,
+// which spreads the stride-R stores of the first passes over distinct banks
+// when a warp owns a single line.
+template <int PS> PD_HD int prow(int n) { return PS > 0 ? n + (n >> PS) : n; }
+template <int N, int PS> constexpr int tile_rows() { return PS > 0 ? N + (N >> PS) : N; }
+
 // One pass, split into a load/compute half and a store half so that a CPU
 // emulator can run all items' first halves before any second half (that is
 // what the __syncthreads() between them does on the GPU).
-template <int N, int R, int NS, int S, int L, int LP>
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0>
 PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
     constexpr int NR = N / R;
     const int l = w % L, j = w / L;
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = s[(j + r * NR) * LP + l];
+    for (int r = 0; r < R; r++) v[r] = s[prow<PS>(j + r * NR) * LP + l];
     if constexpr (NS > 1) {
         const int k = j % NS;
         constexpr int step = N / (NS * R);
@@ -196,16 +202,72 @@ PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
     }
     dft<R, S>(v);
 }
-template <int N, int R, int NS, int L, int LP>
+template <int N, int R, int NS, int L, int LP, int PS = 0>
 PD_HD void pass_store(double2* s, int w, const double2* v) {
     const int l = w % L, j = w / L;
     const int k = j % NS;
     const int d = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) s[(d + r * NS) * LP + l] = v[r];
+    for (int r = 0; r < R; r++) s[prow<PS>(d + r * NS) * LP + l] = v[r];
+}
+
+// Radix schedule of the warp-level transforms (one line per warp): radix 8 where
+// possible so that a pass has N/8 items, about one per lane.
+template <int N> struct WPlan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
+#define PD_WPLAN(N_, A, B, C) \
+    template <> struct WPlan<N_> { static constexpr int r0 = A, r1 = B, r2 = C; };
+PD_WPLAN(16, 4, 4, 0)
+PD_WPLAN(24, 3, 8, 0)
+PD_WPLAN(32, 4, 8, 0)
+PD_WPLAN(48, 3, 4, 4)
+PD_WPLAN(64, 8, 8, 0)
+PD_WPLAN(96, 3, 4, 8)
+PD_WPLAN(128, 4, 4, 8)
+PD_WPLAN(192, 3, 8, 8)
+PD_WPLAN(256, 4, 8, 8)
+PD_WPLAN(384, 3, 8, 16)
+PD_WPLAN(512, 8, 8, 8)
+PD_WPLAN(768, 3, 16, 16)
+PD_WPLAN(1024, 16, 8, 8)
+#undef PD_WPLAN
+
+template <int N> constexpr bool wplan_ok() {
+    return WPlan<N>::r0 * (WPlan<N>::r1 ? WPlan<N>::r1 : 1) * (WPlan<N>::r2 ? WPlan<N>::r2 : 1) == N;
 }
 
 #if defined(__CUDACC__)
+// One pass of a single line owned by one warp: the line is column 0 of `s`
+// (element n at s[prow<PS>(n)*LP]); only __syncwarp() separates the halves.
+template <int N, int R, int NS, int S, int LP, int PS>
+__device__ __forceinline__ void wpass(double2* s, const double2* __restrict__ tw, int lane) {
+    constexpr int WORK = N / R;
+    constexpr int IT = (WORK + 31) / 32;
+    double2 v[IT][R];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = lane + it * 32;
+        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, 1, LP, PS>(s, tw, w, v[it]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = lane + it * 32;
+        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, 1, LP, PS>(s, w, v[it]);
+    }
+    __syncwarp();
+}
+
+// Full length-N transform of the line at column 0 of `s` by the calling warp
+// (the caller makes the line's data visible to the warp before the call).
+template <int N, int S, int LP, int PS>
+__device__ __forceinline__ void fft_warp(double2* s, const double2* __restrict__ tw, int lane) {
+    static_assert(wplan_ok<N>(), "no warp radix plan for this length");
+    constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
+    wpass<N, R0, 1, S, LP, PS>(s, tw, lane);
+    if constexpr (R1 != 0) wpass<N, R1, R0, S, LP, PS>(s, tw, lane);
+    if constexpr (R2 != 0) wpass<N, R2, R0 * R1, S, LP, PS>(s, tw, lane);
+}
+
 // In-place pass over a [N][LP] shared tile with NT threads; items w = tid + it*NT.
 template <int N, int R, int NS, int S, int L, int LP, int NT>
 __device__ __forceinline__ void pass(double2* s, const double2* __restrict__ tw, int tid) {

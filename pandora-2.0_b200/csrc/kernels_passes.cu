@@ -1,0 +1,468 @@
+// kernels_passes.cu -- the five HBM passes of one RK3 stage on sm_100a.
+//
+// Pass structure per stage (replacing f_RK3PrepareRealSpace, f_RK3RealSpace and
+// f_RK3SolveNavierStokes, src/pf_rk3.f90:205-329, 960-1237, 1996-2142, whose
+// MPI/FFTW pencil transposes collapse into on-chip tile transposes):
+//   K1 zpass_inv   u (3 x S)           -> omega, 6 backward z FFTs             -> zb [6][z][j][i]
+//   K2 ypass_inv   zb                  -> 6 backward y FFTs                    -> yb [6][z][y][i]
+//   K3 xpass       yb (6 half spectra) -> 3 complex c2r (two real lines each), omega x u,
+//                                         2 complex r2c, truncate             -> yb fields 0..2
+//   K4 ypass_fwd   yb fields 0..2      -> 3 forward y FFTs, truncate j       -> zb fields 0..2
+//   K5 zpass_fwd   zb fields 0..2      -> 3 forward z FFTs, x 1/(NX NY NZ), truncate k, then the
+//                                         per-mode RHS + low-storage RK3 + continuity fix on u, rk
+// Every pass reads and writes HBM once, in coalesced rows.  A CTA of 8 warps
+// works on a tile of 8 lines: the tile moves between HBM and shared memory with
+// all 256 threads (rows of 8 consecutive i = 128 bytes), and in between each
+// warp transforms its own line with warp-synchronous Stockham passes, so a tile
+// costs two block barriers whatever the transform length.  The x pass owns
+// whole lines per warp and needs no block barrier at all.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "fft_core.cuh"
+#include "pandora_internal.cuh"
+
+namespace pd {
+
+using pdfft::fft_warp;
+using pdfft::mk;
+using pdfft::prow;
+using pdfft::tile_rows;
+
+constexpr int PS = 3;             // one pad row per 8 rows of a tile (pdfft::prow)
+
+constexpr int NW = 8;             // warps per CTA
+constexpr int NT = 32 * NW;       // threads per CTA
+constexpr int L = NW;             // lines per tile, one per warp
+constexpr int LP = L + 1;         // padded row of the tile (odd: conflict-free transposes)
+
+// K1 double-buffers its tile where shared memory allows; K3 holds three
+// complex lines per warp, so long lines get fewer warps per CTA.
+template <int N> struct Cfg {
+    static constexpr int NB1 = (N <= 512) ? 2 : 1;
+    static constexpr int NWX = (N <= 512) ? 8 : 4;
+    static constexpr int L5 = (N <= 512) ? 8 : 4;     // K5 lines (= warps) per CTA
+    static constexpr int LP5 = L5 + 1;
+};
+
+#define PD_FOR_EACH_N(X) \
+    X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+bool supported_length(int n) {
+    switch (n) {
+#define PD_CASE(N) case N:
+        PD_FOR_EACH_N(PD_CASE)
+#undef PD_CASE
+        return true;
+    default:
+        return false;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K1: spectral velocity and vorticity, backward z transforms.
+// CTA = (i tile of 8 lines, one j); warp w owns line i = i0 + w.  Field f:
+// 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
+// f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
+// f_RK3Derivative 3735-3743).  k is zero-padded into [KK+1, NZ-KK-1] as
+// src/pf_rk3.f90:437-443.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 field_value(const double2* const* u, long long m, int f, double k1,
+                                               double k2, double k3) {
+    if (f < 3) return u[f][m];
+    double2 a, b;
+    double ka, kb;
+    // omega1 = (0 - dv/dz) + dw/dy ; omega2 = du/dz - dw/dx ; omega3 = (-du/dy) + dv/dx
+    if (f == 3) { a = u[2][m]; ka = k2; b = u[1][m]; kb = k3; }
+    else if (f == 4) { a = u[0][m]; ka = k3; b = u[2][m]; kb = k1; }
+    else { a = u[1][m]; ka = k1; b = u[0][m]; kb = k2; }
+    // i*ka*a - i*kb*b, with i*k*v = (-k v.y, k v.x)
+    return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F, Geo g, int stage) {
+    constexpr int NB = Cfg<NZ>::NB1;
+    extern __shared__ double2 smem[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i0 = blockIdx.x * L, j = blockIdx.y;
+    const int i = i0 + w;
+    if (stage == 1 && blockIdx.x == 0 && j == 0 && tid == 0) F.clock->ucfl_bits = 0ull;
+    const double k2 = wvn(j, g.kj);
+    const int KK = g.kk, NKK = g.nkk;
+    const double2* u[3] = {F.u[0], F.u[1], F.u[2]};
+    const long long row = ((long long)i * g.nkj + j) * NKK;
+    for (int f = 0; f < 6; f++) {
+        double2* s = smem + (f % NB) * (tile_rows<NZ, PS>() * LP);
+        if (NB == 1 && f > 0) __syncthreads();           // previous store has read the tile
+        double2* col = s + w;
+        for (int k = lane; k < NKK; k += 32) {
+            const int z = (k <= KK) ? k : NZ - NKK + k;
+            double2 v = mk(0.0, 0.0);
+            if (i < g.nki) v = field_value(u, row + k, f, (double)i, k2, wvn(k, KK));
+            col[prow<PS>(z) * LP] = v;
+        }
+        for (int z = KK + 1 + lane; z < NZ - KK; z += 32) col[prow<PS>(z) * LP] = mk(0.0, 0.0);
+        __syncwarp();
+        fft_warp<NZ, +1, LP, PS>(col, F.tw_z, lane);
+        __syncthreads();
+        double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+        const long long zs = (long long)g.nkj * g.nkip;
+        for (int q = tid; q < NZ * L; q += NT) {
+            const int l = q % L, z = q / L;
+            dst[z * zs + l] = s[prow<PS>(z) * LP + l];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: backward y transforms, j padded into [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs,
+// src/pf_rk3.f90:1458-1473).  CTA = (i tile, z, field).
+// ---------------------------------------------------------------------------
+template <int NY>
+__global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_inv(Fields F, Geo g) {
+    extern __shared__ double2 s[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const int KJ = g.kj, NKJ = g.nkj, npad = NY - NKJ;
+    const double2* src = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
+    for (int q = tid; q < NKJ * L; q += NT) {
+        const int l = q % L, jj = q / L;
+        const int y = (jj <= KJ) ? jj : NY - NKJ + jj;
+        s[prow<PS>(y) * LP + l] = src[(long long)jj * g.nkip + l];
+    }
+    for (int q = tid; q < npad * L; q += NT) {
+        const int l = q % L, y = KJ + 1 + q / L;
+        s[prow<PS>(y) * LP + l] = mk(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_warp<NY, +1, LP, PS>(s + w, F.tw_y, lane);
+    __syncthreads();
+    double2* dst = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
+    for (int q = tid; q < NY * L; q += NT) {
+        const int l = q % L, y = q / L;
+        dst[(long long)y * g.nkip + l] = s[prow<PS>(y) * LP + l];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K4: forward y transforms of the three NL fields, truncate j
+// (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
+// ---------------------------------------------------------------------------
+template <int NY>
+__global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_fwd(Fields F, Geo g) {
+    extern __shared__ double2 s[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const double2* src = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
+    for (int q = tid; q < NY * L; q += NT) {
+        const int l = q % L, y = q / L;
+        s[prow<PS>(y) * LP + l] = src[(long long)y * g.nkip + l];
+    }
+    __syncthreads();
+    fft_warp<NY, -1, LP, PS>(s + w, F.tw_y, lane);
+    __syncthreads();
+    const int KJ = g.kj, NKJ = g.nkj;
+    double2* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
+    for (int q = tid; q < NKJ * L; q += NT) {
+        const int l = q % L, jj = q / L;
+        const int y = (jj <= KJ) ? jj : NY - NKJ + jj;
+        dst[(long long)jj * g.nkip + l] = s[prow<PS>(y) * LP + l];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K3: x pass, one warp per (z,y) line, no block barrier.  The six half spectra
+// of the line become three complex backward FFTs (pairs (u1,u2), (u3,w1),
+// (w2,w3): the c2r of two real lines at once; the Hermitian extension drops Im
+// of the i=0 mode as FFTW's c2r does, src/pf_fftw.f90:646,749-756), then
+// NL = omega x u (f_RK3ComputeNonlinearIsotropic, src/pf_rk3.f90:1597-1628),
+// then two complex forward FFTs ((n1,n2), (n3,0)) split into the r2c outputs,
+// truncated to i = 0..KI (src/pf_fftw.f90:780).  NL overwrites yb fields 0..2 of
+// the same line.  Optionally writes the physical velocity (arr_u*_3r,
+// src/pf_rk3.f90:1108-1115) and the CFL maximum (src/pf_fluidstats.f90:913-917).
+// Warp shared region: element n of array p at s[prow(n)*3 + p].
+// ---------------------------------------------------------------------------
+template <int NX>
+__global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys, int want_cfl) {
+    constexpr int LPX = 3;
+    extern __shared__ double2 smem[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const long long lines = (long long)g.ny * g.nz;
+    const long long q = (long long)blockIdx.x * Cfg<NX>::NWX + w;
+    if (q >= lines) return;                       // whole warp; the kernel has no block barrier
+    double2* s = smem + (size_t)w * tile_rows<NX, PS>() * LPX;
+    const long long fstride = lines * g.nkip;     // distance between fields in yb
+    const int KI = g.ki, NKI = g.nki;
+    double2* b = F.yb + q * g.nkip;
+    for (int m = lane; m < NKI; m += 32) {
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+            double2 X = b[(2 * p) * fstride + m], Y = b[(2 * p + 1) * fstride + m];
+            if (m == 0) { X.y = 0.0; Y.y = 0.0; }
+            s[prow<PS>(m) * LPX + p] = mk(X.x - Y.y, X.y + Y.x);
+            if (m > 0) s[prow<PS>(NX - m) * LPX + p] = mk(X.x + Y.y, -X.y + Y.x);
+        }
+    }
+    for (int n = KI + 1 + lane; n < NX - KI; n += 32) {
+#pragma unroll
+        for (int p = 0; p < 3; p++) s[prow<PS>(n) * LPX + p] = mk(0.0, 0.0);
+    }
+    __syncwarp();
+    fft_warp<NX, +1, LPX, PS>(s + 0, F.tw_x, lane);
+    fft_warp<NX, +1, LPX, PS>(s + 1, F.tw_x, lane);
+    fft_warp<NX, +1, LPX, PS>(s + 2, F.tw_x, lane);
+    double umax = 0.0;
+    for (int n = lane; n < NX; n += 32) {
+        double2* e = s + prow<PS>(n) * LPX;
+        const double2 a = e[0], bb = e[1], c = e[2];
+        const double u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
+        if (want_phys) {
+            F.phys[q * NX + n] = u1;
+            F.phys[g.R + q * NX + n] = u2;
+            F.phys[2 * g.R + q * NX + n] = u3;
+        }
+        if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
+        e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
+        e[1] = mk(u2 * w1 - u1 * w2, 0.0);
+    }
+    if (want_cfl) {
+        for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+        if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong(umax));
+    }
+    __syncwarp();
+    fft_warp<NX, -1, LPX, PS>(s + 0, F.tw_x, lane);
+    fft_warp<NX, -1, LPX, PS>(s + 1, F.tw_x, lane);
+    for (int m = lane; m < g.nkip; m += 32) {
+        double2 n1 = mk(0.0, 0.0), n2 = n1, n3 = n1;
+        if (m < NKI) {
+            const int mc = (NX - m) % NX;
+            const double2 Z = s[prow<PS>(m) * LPX], Zc = s[prow<PS>(mc) * LPX];
+            n1 = mk(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
+            n2 = mk(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
+            const double2 W = s[prow<PS>(m) * LPX + 1], Wc = s[prow<PS>(mc) * LPX + 1];
+            n3 = mk(0.5 * (W.x + Wc.x), 0.5 * (W.y - Wc.y));
+        }
+        b[m] = n1;
+        b[fstride + m] = n2;
+        b[2 * fstride + m] = n3;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K5: forward z transforms x normalisation, truncate k (f_RK3TransformkRs2Fs +
+// f_Fftw_k_Rs2Fs, src/pf_rk3.f90:2242-2316, src/pf_fftw.f90:841-879), then per
+// mode f_RK3FormFIsotropic + f_RK3RungeKutta + f_RK3ContinuityFixIsotropic
+// (src/pf_rk3.f90:2323-2487, 3457-3531).  Warp w transforms line i = i0 + w of
+// each NL field, keeps its truncated values in T, and updates its own modes
+// (u, rk rows along k, coalesced).  mode 1 stores NL-hat into rk instead (the
+// transform test hook of src/ptf_rk3.f90:629-734).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void rk_coeffs(int stage, double& beta, double& gamma) {
+    if (stage == 1) { beta = 0.0; gamma = 1.0 / 3.0; }
+    else if (stage == 2) { beta = -(5.0 / 9.0); gamma = 15.0 / 16.0; }
+    else { beta = -(153.0 / 128.0); gamma = 8.0 / 15.0; }
+}
+
+template <int NZ>
+__global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int stage, int mode) {
+    constexpr int L5 = Cfg<NZ>::L5, LP5 = Cfg<NZ>::LP5, NT5 = 32 * L5;
+    extern __shared__ double2 smem[];
+    double2* s = smem;                                      // tile [rows(NZ)][LP5]
+    double2* T = smem + tile_rows<NZ, PS>() * LP5;          // fields 0, 1: [2][NKK][LP5]
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int i0 = blockIdx.x * L5, j = blockIdx.y;
+    const int KK = g.kk, NKK = g.nkk;
+    for (int f = 0; f < 3; f++) {
+        if (f > 0) __syncthreads();                         // warps are done with the previous tile
+        const double2* src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+        const long long zs = (long long)g.nkj * g.nkip;
+        for (int q = tid; q < NZ * L5; q += NT5) {
+            const int l = q % L5, z = q / L5;
+            s[prow<PS>(z) * LP5 + l] = src[z * zs + l];
+        }
+        __syncthreads();
+        fft_warp<NZ, -1, LP5, PS>(s + w, F.tw_z, lane);
+        if (f < 2) {
+            for (int k = lane; k < NKK; k += 32) {
+                const int z = (k <= KK) ? k : NZ - NKK + k;
+                T[(f * NKK + k) * LP5 + w] = s[prow<PS>(z) * LP5 + w];
+            }
+        }
+    }
+    __syncwarp();
+    const int i = i0 + w;
+    if (i >= g.nki) return;                                 // no block barrier follows
+    const double dt = F.clock->dt;
+    double beta, gamma;
+    rk_coeffs(stage, beta, gamma);
+    const double k1 = (double)i, k2 = wvn(j, g.kj);
+    const int NK = g.fnk, FW = 2 * NK + 1;
+    const long long row = ((long long)i * g.nkj + j) * NKK;
+    for (int k = lane; k < NKK; k += 32) {
+        const long long m = row + k;
+        const int z = (k <= KK) ? k : NZ - NKK + k;
+        double2 nl[3];
+#pragma unroll
+        for (int c = 0; c < 2; c++) nl[c] = T[(c * NKK + k) * LP5 + w];
+        nl[2] = s[prow<PS>(z) * LP5 + w];
+#pragma unroll
+        for (int c = 0; c < 3; c++) nl[c] = mk(nl[c].x * g.norm, nl[c].y * g.norm);
+        if (mode == 1) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) F.rk[c][m] = nl[c];
+            continue;
+        }
+        const double k3 = wvn(k, KK);
+        const double kmag2 = (k1 * k1) + (k2 * k2) + (k3 * k3);
+        if (!(kmag2 > 0.0)) continue;
+        const double kv[3] = {k1, k2, k3};
+        const double2 kdn = mk(k1 * nl[0].x + k2 * nl[1].x + k3 * nl[2].x,
+                               k1 * nl[0].y + k2 * nl[1].y + k3 * nl[2].y);
+        double2 force[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+        const double kmag = sqrt(kmag2);
+        if (kmag <= g.force_kf && kmag > 0.0) {
+            const int jw = (int)k2, kw = (int)k3;
+            if (i <= NK && jw >= -NK && jw <= NK && kw >= -NK && kw <= NK) {
+                double2 fv[3];
+                const long long fi = ((long long)i * FW + (jw + NK)) * FW + (kw + NK);
+                const long long fst = (long long)(NK + 1) * FW * FW;
+#pragma unroll
+                for (int c = 0; c < 3; c++) fv[c] = F.forcing[c * fst + fi];
+                const double2 kdb = mk(k1 * fv[0].x + k2 * fv[1].x + k3 * fv[2].x,
+                                       k1 * fv[0].y + k2 * fv[1].y + k3 * fv[2].y);
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    force[c] = mk(fv[c].x - ((kv[c] / kmag2) * kdb.x), fv[c].y - ((kv[c] / kmag2) * kdb.y));
+            }
+        }
+        double2 uu[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            uu[c] = F.u[c][m];
+            const double2 tot = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
+                                   -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+            double2 r;
+            if (stage == 1) r = tot;   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
+            else {
+                const double2 r0 = F.rk[c][m];
+                r = mk((beta * r0.x) + tot.x, (beta * r0.y) + tot.y);
+            }
+            F.rk[c][m] = r;
+            uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
+        }
+        const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x,
+                               k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            F.u[c][m] = mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+template <int N> static size_t smem_k1() {
+    return sizeof(double2) * (size_t)Cfg<N>::NB1 * tile_rows<N, PS>() * LP;
+}
+template <int N> static size_t smem_ky() { return sizeof(double2) * (size_t)tile_rows<N, PS>() * LP; }
+template <int N> static size_t smem_kx() {
+    return sizeof(double2) * (size_t)Cfg<N>::NWX * tile_rows<N, PS>() * 3;
+}
+template <int N> static size_t smem_k5(const Geo& g) {
+    return sizeof(double2) * ((size_t)tile_rows<N, PS>() + 2 * (size_t)g.nkk) * Cfg<N>::LP5;
+}
+
+template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t configure_kernels(const Geo& g) {
+    cudaError_t e = cudaSuccess;
+#define PD_CFG(N)                                                                     \
+    if (g.nz == N) {                                                                  \
+        if ((e = set_smem(k_zpass_inv<N>, smem_k1<N>()))) return e;                   \
+        if ((e = set_smem(k_zpass_fwd_update<N>, smem_k5<N>(g)))) return e;           \
+    }                                                                                 \
+    if (g.ny == N) {                                                                  \
+        if ((e = set_smem(k_ypass_inv<N>, smem_ky<N>()))) return e;                   \
+        if ((e = set_smem(k_ypass_fwd<N>, smem_ky<N>()))) return e;                   \
+    }                                                                                 \
+    if (g.nx == N) {                                                                  \
+        if ((e = set_smem(k_xpass<N>, smem_kx<N>()))) return e;                       \
+    }
+    PD_FOR_EACH_N(PD_CFG)
+#undef PD_CFG
+    return cudaSuccess;
+}
+
+cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStream_t st) {
+    switch (g.nz) {
+#define PD_L(N)                                                                       \
+    case N:                                                                           \
+        k_zpass_inv<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k1<N>(), st>>>(f, g, stage); \
+        break;
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st) {
+    switch (g.ny) {
+#define PD_L(N)                                                                       \
+    case N:                                                                           \
+        k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), NT, smem_ky<N>(), st>>>(f, g);    \
+        break;
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xpass(const Geo& g, const Fields& f, int want_phys, int want_cfl, cudaStream_t st) {
+    const long long lines = (long long)g.ny * g.nz;
+    switch (g.nx) {
+#define PD_L(N)                                                                             \
+    case N: {                                                                               \
+        const long long nb = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                       \
+        k_xpass<N><<<(unsigned)nb, 32 * Cfg<N>::NWX, smem_kx<N>(), st>>>(f, g, want_phys, want_cfl); \
+        break;                                                                              \
+    }
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
+    switch (g.ny) {
+#define PD_L(N)                                                                       \
+    case N:                                                                           \
+        k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), NT, smem_ky<N>(), st>>>(f, g);    \
+        break;
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, int mode, cudaStream_t st) {
+    switch (g.nz) {
+#define PD_L(N)                                                                             \
+    case N: {                                                                               \
+        dim3 grid((g.nki + Cfg<N>::L5 - 1) / Cfg<N>::L5, g.nkj);                            \
+        k_zpass_fwd_update<N><<<grid, 32 * Cfg<N>::L5, smem_k5<N>(g), st>>>(f, g, stage, mode); \
+        break;                                                                              \
+    }
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pd

@@ -10,15 +10,15 @@
 
 using namespace pdfft;
 
-template <int N, int R, int NS, int S, int L, int LP>
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0>
 static void emu_pass(std::vector<double2>& s, const std::vector<double2>& tw) {
     constexpr int WORK = (N / R) * L;
     std::vector<double2> v((size_t)WORK * R);
-    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP>(s.data(), tw.data(), w, &v[(size_t)w * R]);
-    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP>(s.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP, PS>(s.data(), tw.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP, PS>(s.data(), w, &v[(size_t)w * R]);
 }
 
-template <int N, int S, int L, int LP>
+template <int N, int S, int L, int LP, bool WARP>
 static double check() {
     static_assert(plan_ok<N>(), "plan");
     std::vector<double2> tw(N);
@@ -34,10 +34,24 @@ static double check() {
             x[(size_t)l * N + n] = v;
             s[(size_t)n * LP + l] = v;
         }
-    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
-    emu_pass<N, R0, 1, S, L, LP>(s, tw);
-    if constexpr (R1 != 0) emu_pass<N, R1, R0, S, L, LP>(s, tw);
-    if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, L, LP>(s, tw);
+    if constexpr (WARP) {
+        // warp plan, one line per warp: every line is column l of the tile (offset l, L = 1)
+        constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
+        // padded rows (PS = 3) as the kernels use them
+        for (int l = 0; l < L; l++) {
+            std::vector<double2> col((size_t)tile_rows<N, 3>() * LP);
+            for (int n = 0; n < N; n++) col[(size_t)prow<3>(n) * LP] = s[(size_t)n * LP + l];
+            emu_pass<N, R0, 1, S, 1, LP, 3>(col, tw);
+            if constexpr (R1 != 0) emu_pass<N, R1, R0, S, 1, LP, 3>(col, tw);
+            if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, 1, LP, 3>(col, tw);
+            for (int n = 0; n < N; n++) s[(size_t)n * LP + l] = col[(size_t)prow<3>(n) * LP];
+        }
+    } else {
+        constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+        emu_pass<N, R0, 1, S, L, LP>(s, tw);
+        if constexpr (R1 != 0) emu_pass<N, R1, R0, S, L, LP>(s, tw);
+        if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, L, LP>(s, tw);
+    }
     double err = 0, mag = 0;
     for (int l = 0; l < L; l++)
         for (int k = 0; k < N; k++) {
@@ -58,8 +72,14 @@ static double check() {
 
 #define RUN(N)                                                                   \
     do {                                                                         \
-        double e1 = check<N, -1, 8, 9>(), e2 = check<N, +1, 3, 5>();             \
+        double e1 = check<N, -1, 8, 9, false>(), e2 = check<N, +1, 3, 5, false>(); \
         printf("N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                          \
+        if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                  \
+    } while (0)
+#define RUNW(N)                                                                  \
+    do {                                                                         \
+        double e1 = check<N, -1, 2, 3, true>(), e2 = check<N, +1, 2, 3, true>(); \
+        printf("warp N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                     \
         if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                  \
     } while (0)
 
@@ -68,6 +88,8 @@ int main() {
     RUN(16); RUN(24); RUN(32); RUN(40); RUN(48); RUN(56); RUN(64); RUN(80); RUN(96);
     RUN(112); RUN(128); RUN(160); RUN(192); RUN(224); RUN(256); RUN(320); RUN(384);
     RUN(448); RUN(512); RUN(640); RUN(768); RUN(896); RUN(1024);
+    RUNW(16); RUNW(24); RUNW(32); RUNW(48); RUNW(64); RUNW(96); RUNW(128); RUNW(192); RUNW(256);
+    RUNW(384); RUNW(512); RUNW(768); RUNW(1024);
     printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }
