@@ -184,12 +184,20 @@ def run_reference(a, p):
 
 
 def _config(a, p):
-    return {"workload": f"{a.workload} {p.nodes_x}^3 FP64 plain, OU forcing |k|<=2.5, "
-                        f"{int(p.p_np_global) if p.p_track_part else 0} tracers (order {p.p_interp_order})",
-            "grid": [p.nodes_x, p.nodes_y, p.nodes_z], "nu": p.f_nu, "dt": p.rk3_dt,
-            "particles": int(p.p_np_global) if p.p_track_part else 0, "form": "fp64_plain",
+    npart = int(p.p_np_global) if p.p_track_part else 0
+    if p.f_type == 2:
+        phys = (f"homogeneous shear S={p.f_deform_s} (Rogallo frame, BF-rot), B110={p.b110}, "
+                f"dt=(0.5/S)/{p.f_remesh_t}, no forcing")
+    elif p.force_stop > 0:
+        phys = f"OU forcing |k|<={p.force_kf}, nu={p.f_nu}, dt={p.rk3_dt}"
+    else:
+        phys = f"decaying, nu={p.f_nu}, dt={p.rk3_dt}"
+    ws = (6 * 16 * (p.nodes_x // 3 + 8) * p.nodes_y * p.nodes_z) / 1e9
+    return {"workload": f"{a.workload} {p.nodes_x}^3 FP64 plain, {phys}, {npart} tracers (order {p.p_interp_order})",
+            "grid": [p.nodes_x, p.nodes_y, p.nodes_z], "nu": p.f_nu,
+            "particles": npart, "form": "fp64_plain",
             "parallelism": f"replicas x{a.gpus}",
-            "l2": "no flush needed: every pass streams > 0.3 GB (working set ~1.6 GB > 126 MB L2)"}
+            "l2": f"no flush needed: each pass streams > 126 MB (y-pencil buffer alone {ws:.2f} GB)"}
 
 
 def run_ours(a, p):

@@ -199,6 +199,11 @@ int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, double* n3);
  * materialised for particle interpolation (arr_u*_3r, src/pf_rk3.f90:1108-1115). */
 int pandora_get_physical_velocity(pandora_handle* h, double* u1, double* u2, double* u3);
 
+/* Moving frame of a shear flow: bmat(1,3) and binv(1,3) of g_domain
+ * (src/pg_domain.f90:202-214), as g_RK3UpdateB (src/pg_rk3.f90:280-385) and the
+ * remesh (src/pf_rk3.f90:4056-4178) leave them; both 0 for isotropic flow. */
+int pandora_frame(pandora_handle* h, double* bmat13, double* binv13);
+
 /* Device status word: non-zero bits record NaN detection / bounded-wait timeouts /
  * lost particles since the last call; clears it. */
 int pandora_check_status(pandora_handle* h);

@@ -68,6 +68,10 @@ def lib():
         L.oracle_step.restype = i32
         L.oracle_step.argtypes = [vp, i32, dp, dp]
         L.oracle_threads.restype = i32
+        L.oracle_update_b.argtypes = [vp, i32, ctypes.c_double]
+        L.oracle_get_b.argtypes = [vp, dp, dp]
+        L.oracle_remesh_due.restype = i32
+        L.oracle_remesh_due.argtypes = [vp, i32]
         L.oracle_force_calls_per_stage.restype = i64
         L.oracle_force_calls_per_stage.argtypes = [vp]
         _lib = L
@@ -200,6 +204,17 @@ class Oracle:
         if rc:
             raise RuntimeError(f"oracle_step failed: {rc}")
         return t.value, d.value
+
+    def frame(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self.L.oracle_get_b(self.h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def update_b(self, tstep, simtime):
+        self.L.oracle_update_b(self.h, tstep, simtime)
+
+    def remesh_due(self, tstep):
+        return bool(self.L.oracle_remesh_due(self.h, tstep))
 
     def force_calls_per_stage(self):
         return self.L.oracle_force_calls_per_stage(self.h)

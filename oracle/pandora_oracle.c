@@ -151,7 +151,8 @@ typedef struct oracle {
     /* geometry (src/pg_domain.f90:147-243) */
     double dx, dy, dz, lx, ly, lz;
     double bmat[3][3], binv[3][3], amat[3][3];
-    int bexist[3][3];
+    int bexist[3][3], aexist[3][3];
+    int shear;            /* F_TYPE == F_SHEAR_DNS, BF-rot formulation */
     /* work */
     double* phys[6];      /* physical fields [z][y][x] */
     cx *wa, *wb;          /* pencil work arrays */
@@ -195,11 +196,13 @@ oracle* oracle_create(const pandora_params* p) {
     o->dx = o->lx / (double)o->nx; o->dy = o->ly / (double)o->ny; o->dz = o->lz / (double)o->nz;
     memset(o->bmat, 0, sizeof(o->bmat)); memset(o->binv, 0, sizeof(o->binv));
     memset(o->amat, 0, sizeof(o->amat)); memset(o->bexist, 0, sizeof(o->bexist));
+    memset(o->aexist, 0, sizeof(o->aexist));
     o->binv[0][0] = (double)p->b110; o->binv[1][1] = (double)p->b220; o->binv[2][2] = (double)p->b330;
     o->bexist[0][0] = o->bexist[1][1] = o->bexist[2][2] = 1;
     if (p->f_type != PANDORA_F_ISOTROPIC_DEFORMED) {
-        o->bexist[0][2] = 1; o->amat[0][2] = p->f_deform_s;
+        o->bexist[0][2] = 1; o->amat[0][2] = p->f_deform_s; o->aexist[0][2] = 1;
     }
+    o->shear = (p->f_type == PANDORA_F_SHEAR_DNS);
     o->bmat[0][0] = 1.0 / o->binv[0][0]; o->bmat[1][1] = 1.0 / o->binv[1][1];
     o->bmat[2][2] = 1.0 / o->binv[2][2];
     for (int f = 0; f < 6; f++) o->phys[f] = dalloc(o->R);
@@ -401,6 +404,185 @@ static void nonlinear_iso(oracle* o) {
     }
 }
 
+
+/* BF-rot vorticity of one velocity component n, f_RK3VorticityBFRot
+ * (src/pf_rk3.f90:3786-3843): accumulates into w[0..2]. */
+static void vort_bf_add(const oracle* o, cx un, const double* k, int n, cx* w) {
+    const double(*bm)[3] = o->bmat;
+    const double(*bi)[3] = o->binv;
+    const int(*ex)[3] = o->bexist;
+    for (int m = 0; m < 3; m++) {
+        if (ex[m][0]) {
+            if (ex[2][n]) {
+                w[1].im = w[1].im - (bm[m][0] * bi[2][n] * k[m] * un.re);
+                w[1].re = w[1].re + (bm[m][0] * bi[2][n] * k[m] * un.im);
+            }
+            if (ex[1][n]) {
+                w[2].im = w[2].im + (bm[m][0] * bi[1][n] * k[m] * un.re);
+                w[2].re = w[2].re - (bm[m][0] * bi[1][n] * k[m] * un.im);
+            }
+        }
+        if (ex[m][1]) {
+            if (ex[2][n]) {
+                w[0].im = w[0].im + (bm[m][1] * bi[2][n] * k[m] * un.re);
+                w[0].re = w[0].re - (bm[m][1] * bi[2][n] * k[m] * un.im);
+            }
+            if (ex[0][n]) {
+                w[2].im = w[2].im - (bm[m][1] * bi[0][n] * k[m] * un.re);
+                w[2].re = w[2].re + (bm[m][1] * bi[0][n] * k[m] * un.im);
+            }
+        }
+        if (ex[m][2]) {
+            if (ex[1][n]) {
+                w[0].im = w[0].im - (bm[m][2] * bi[1][n] * k[m] * un.re);
+                w[0].re = w[0].re + (bm[m][2] * bi[1][n] * k[m] * un.im);
+            }
+            if (ex[0][n]) {
+                w[1].im = w[1].im + (bm[m][2] * bi[0][n] * k[m] * un.re);
+                w[1].re = w[1].re - (bm[m][2] * bi[0][n] * k[m] * un.im);
+            }
+        }
+    }
+}
+
+static void vorticity_bf(oracle* o, cx* om[3]) {
+#pragma omp parallel for schedule(static)
+    for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+        int i = (int)(ij / o->nkj), j = (int)(ij % o->nkj);
+        for (int k = 0; k < o->nkk; k++) {
+            long m = ij * o->nkk + k;
+            double kv[3] = {wvn(i, o->ki), wvn(j, o->kj), wvn(k, o->kk)};
+            cx w[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int n = 0; n < 3; n++) vort_bf_add(o, o->u[n][m], kv, n, w);
+            om[0][m] = w[0]; om[1][m] = w[1]; om[2][m] = w[2];
+        }
+    }
+}
+
+/* f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711) */
+static void nonlinear_bf(oracle* o) {
+    const double(*bi)[3] = o->binv;
+    const int(*ex)[3] = o->bexist;
+    double *w1 = o->phys[3], *w2 = o->phys[4], *w3 = o->phys[5];
+#pragma omp parallel for schedule(static)
+    for (long p = 0; p < o->R; p++) {
+        double u[3] = {o->phys[0][p], o->phys[1][p], o->phys[2][p]};
+        double om[3] = {w1[p], w2[p], w3[p]};
+        double n1 = 0.0, n2 = 0.0, n3 = 0.0;
+        for (int m = 0; m < 3; m++) {
+            if (ex[0][m]) { n3 = n3 - (om[1] * bi[0][m] * u[m]); n2 = n2 + (om[2] * bi[0][m] * u[m]); }
+            if (ex[1][m]) { n1 = n1 - (om[2] * bi[1][m] * u[m]); n3 = n3 + (om[0] * bi[1][m] * u[m]); }
+            if (ex[2][m]) { n1 = n1 + (om[1] * bi[2][m] * u[m]); n2 = n2 - (om[0] * bi[2][m] * u[m]); }
+        }
+        w1[p] = n1; w2[p] = n2; w3[p] = n3;
+    }
+}
+
+/* f_RK3FormFBFRot for F_SHEAR_DNS (src/pf_rk3.f90:2494-2673) with
+ * f_RK3BFRotNonlinear 2864-2895, ...Viscous 2903-2937, ...Pressure 2986-3070,
+ * ...Source 3167-3209, then f_RK3RungeKutta and f_RK3ContinuityFixIsotropic. */
+static void form_f_bf(oracle* o, int stage, double dt) {
+    double beta, gamma;
+    void rk_coeffs(int, double*, double*);
+    rk_coeffs(stage, &beta, &gamma);
+    const double nu = o->p.f_nu;
+    const double(*bm)[3] = o->bmat;
+    const double(*bi)[3] = o->binv;
+    const double(*am)[3] = o->amat;
+    const int(*ex)[3] = o->bexist;
+    const int(*ax)[3] = o->aexist;
+#pragma omp parallel for schedule(static)
+    for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+        int i = (int)(ij / o->nkj), j = (int)(ij % o->nkj);
+        for (int kq = 0; kq < o->nkk; kq++) {
+            long m0 = ij * o->nkk + kq;
+            double k[3] = {wvn(i, o->ki), wvn(j, o->kj), wvn(kq, o->kk)};
+            double kmag2 = (k[0] * k[0]) + (k[1] * k[1]) + (k[2] * k[2]);
+            if (!(kmag2 > 0.0)) continue;
+            cx u[3] = {o->u[0][m0], o->u[1][m0], o->u[2][m0]};
+            cx nlr[3] = {o->nl[0][m0], o->nl[1][m0], o->nl[2][m0]};
+            cx nl[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (ex[a][b]) { nl[a].re = nl[a].re + bm[a][b] * nlr[b].re; nl[a].im = nl[a].im + bm[a][b] * nlr[b].im; }
+            /* pressure */
+            double p1[3] = {0, 0, 0}, p4 = 0.0;
+            cx p2 = {0, 0}, p3 = {0, 0};
+            for (int m = 0; m < 3; m++) {
+                p2.re = p2.re + (k[m] * nl[m].re); p2.im = p2.im + (k[m] * nl[m].im);
+                for (int r = 0; r < 3; r++) {
+                    if (!ex[m][r]) continue;
+                    for (int sx = 0; sx < 3; sx++) {
+                        if (!ax[r][sx]) continue;
+                        for (int q = 0; q < 3; q++) {
+                            if (!ex[sx][q]) continue;
+                            double c = k[m] * bm[m][r] * am[r][sx] * bi[sx][q];
+                            p3.re = p3.re + (2.0 * (c * u[q].re));
+                            p3.im = p3.im + (2.0 * (c * u[q].im));
+                        }
+                    }
+                    for (int q = 0; q < 3; q++)
+                        if (ex[q][r]) p4 = p4 + (k[m] * bm[m][r] * bm[q][r] * k[q]);
+                }
+            }
+            for (int a = 0; a < 3; a++)
+                for (int pp = 0; pp < 3; pp++)
+                    if (ex[a][pp])
+                        for (int b = 0; b < 3; b++)
+                            if (ex[b][pp]) p1[a] = p1[a] + bm[a][pp] * bm[b][pp] * k[b];
+            cx press[3];
+            for (int a = 0; a < 3; a++) {
+                if (p4 > 0.0) { press[a].re = (p1[a] / p4) * (p2.re + p3.re); press[a].im = (p1[a] / p4) * (p2.im + p3.im); }
+                else { press[a].re = 0.0; press[a].im = 0.0; }
+            }
+            /* homogeneous source */
+            cx hom[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int a = 0; a < 3; a++)
+                for (int r = 0; r < 3; r++) {
+                    if (!ex[a][r]) continue;
+                    for (int b = 0; b < 3; b++) {
+                        if (!ax[r][b]) continue;
+                        for (int q = 0; q < 3; q++) {
+                            if (!ex[b][q]) continue;
+                            double c = bm[a][r] * am[r][b] * bi[b][q];
+                            hom[a].re = hom[a].re + (2.0 * (c * u[q].re));
+                            hom[a].im = hom[a].im + (2.0 * (c * u[q].im));
+                        }
+                    }
+                }
+            /* viscous */
+            cx visc[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int l = 0; l < 3; l++)
+                for (int jj = 0; jj < 3; jj++) {
+                    if (!ex[l][jj]) continue;
+                    for (int n = 0; n < 3; n++) {
+                        if (!ex[n][jj]) continue;
+                        double c = nu * bm[l][jj] * bm[n][jj] * k[l] * k[n];
+                        for (int a = 0; a < 3; a++) { visc[a].re = visc[a].re - c * u[a].re; visc[a].im = visc[a].im - c * u[a].im; }
+                    }
+                }
+            cx tot[3];
+            for (int a = 0; a < 3; a++) {
+                tot[a].re = visc[a].re - nl[a].re + press[a].re + 0.0 - hom[a].re;
+                tot[a].im = visc[a].im - nl[a].im + press[a].im + 0.0 - hom[a].im;
+            }
+            for (int a = 0; a < 3; a++) {
+                cx* r = &o->rk[a][m0];
+                r->re = (beta * r->re) + tot[a].re;
+                r->im = (beta * r->im) + tot[a].im;
+                u[a].re = u[a].re + (gamma * dt * r->re);
+                u[a].im = u[a].im + (gamma * dt * r->im);
+            }
+            cx kdu = {k[0] * u[0].re + k[1] * u[1].re + k[2] * u[2].re, k[0] * u[0].im + k[1] * u[1].im + k[2] * u[2].im};
+            for (int a = 0; a < 3; a++) {
+                u[a].re = u[a].re - (k[a] * kdu.re / kmag2);
+                u[a].im = u[a].im - (k[a] * kdu.im / kmag2);
+                o->u[a][m0] = u[a];
+            }
+        }
+    }
+}
+
 /* max |u1|+|u2|+|u3| (src/pf_fluidstats.f90:913-917,979) */
 static double cfl_velocity(const oracle* o) {
     double m = 0.0;
@@ -412,14 +594,86 @@ static double cfl_velocity(const oracle* o) {
     return m;
 }
 
+
+/* ------------------------------------------------------------------------- */
+/* Rogallo moving frame (shear): g_RK3UpdateB (src/pg_rk3.f90:280-385) and the */
+/* wave-space remesh f_RK3Remesh / f_RK3RemeshWaveSpace (src/pf_rk3.f90:3958-4178) */
+/* ------------------------------------------------------------------------- */
+void oracle_update_b(oracle* o, int tstep, double simtime) {
+    const pandora_params* p = &o->p;
+    if (p->f_type == PANDORA_F_ISOTROPIC) return;
+    double localtime = simtime;
+    if (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) {
+        if (tstep > p->b110 * p->f_remesh_t) {
+            int a = tstep - (p->b110 * p->f_remesh_t) - 1;
+            int b = 2 * (p->b110 * p->f_remesh_t);
+            int localtstep = a / b;
+            localtime = simtime - ((double)(localtstep + 1) / p->f_deform_s * (double)p->b110);
+        }
+    }
+    o->bmat[0][2] = -o->bmat[0][0] * p->f_deform_s * localtime;
+    o->binv[0][2] = p->f_deform_s * localtime / o->bmat[2][2];
+}
+
+int oracle_remesh_due(const oracle* o, int tstep) {
+    const pandora_params* p = &o->p;
+    if (p->f_type == PANDORA_F_ISOTROPIC || p->rk3_timestep != PANDORA_RK3_TIMESTEP_DECIDE) return 0;
+    int a = tstep - (p->b110 * p->f_remesh_t) - 1;
+    int b = 2 * p->b110 * p->f_remesh_t;
+    return (a % b) == 0;
+}
+
+/* k3 <- k3 - k1 shift, modes below -KK dropped, BF-rot: u1 += u3; then the
+ * frame jumps from S t = +B110/2 to -B110/2 (bmat/binv (1,3) reset). */
+static void remesh_wave_space(oracle* o) {
+    const int KK = o->kk, nodes = 2 * KK + 1, NKK = o->nkk;
+    const double half_b = (double)o->p.b110 * 0.5;
+    o->binv[0][2] = half_b / o->bmat[2][2];
+    o->bmat[0][2] = -o->bmat[0][0] * (-half_b);
+#pragma omp parallel
+    {
+        cx* r[3];
+        for (int c = 0; c < 3; c++) r[c] = calloc_cx(NKK);
+#pragma omp for schedule(static)
+        for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+            int i = (int)(ij / o->nkj);
+            for (int c = 0; c < 3; c++) memset(r[c], 0, sizeof(cx) * NKK);
+            for (int k = 0; k < NKK; k++) {
+                int actualk = k > KK ? k - nodes : k;
+                int knew = actualk - i;
+                if (knew >= -KK) {
+                    if (knew < 0) knew += nodes;
+                    for (int c = 0; c < 3; c++) r[c][knew] = o->u[c][ij * NKK + k];
+                }
+            }
+            for (int k = 0; k < NKK; k++) {
+                cx a = r[0][k], b3 = r[2][k];
+                o->u[0][ij * NKK + k].re = a.re + b3.re;
+                o->u[0][ij * NKK + k].im = a.im + b3.im;
+                o->u[1][ij * NKK + k] = r[1][k];
+                o->u[2][ij * NKK + k] = r[2][k];
+            }
+        }
+        for (int c = 0; c < 3; c++) free(r[c]);
+    }
+    o->binv[0][2] = (-half_b) / o->bmat[2][2];
+}
+
+void oracle_get_b(const oracle* o, double* b13, double* bi13) {
+    *b13 = o->bmat[0][2];
+    *bi13 = o->binv[0][2];
+}
+
 /* transforms + nonlinear term of the current state -> o->nl (normalised) */
 static void compute_nonlinear(oracle* o, int want_cfl) {
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};   /* spectral omega held in nl */
-    vorticity_iso(o, om);
+    if (o->shear) vorticity_bf(o, om);
+    else vorticity_iso(o, om);
     for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
     for (int c = 0; c < 3; c++) spec_to_phys(o, om[c], o->phys[3 + c]);
     if (want_cfl) o->ucfl = cfl_velocity(o);
-    nonlinear_iso(o);
+    if (o->shear) nonlinear_bf(o);
+    else nonlinear_iso(o);
     for (int c = 0; c < 3; c++) phys_to_spec(o, o->phys[3 + c], o->nl[c]);
 }
 
@@ -436,6 +690,7 @@ static inline cx* fref(oracle* o, int c, int i, int j, int k) {
     int NK = o->fnk, W = 2 * NK + 1;
     return &o->ff[c][((long)i * W + (j + NK)) * W + (k + NK)];
 }
+long oracle_force_calls_per_stage(const oracle* o);
 long oracle_force_calls_per_stage(const oracle* o) {
     long NK = o->fnk;
     return 3 * ((NK + 1) * (NK + 1) + NK * (NK + 1)) + 3 * NK * (2 * NK + 1) * (2 * NK + 1);
@@ -503,7 +758,7 @@ static void force_calc(oracle* o, int tstep, int stage, double dt) {
 /* f_RK3FormFIsotropic + f_RK3RungeKutta + f_RK3ContinuityFixIsotropic          */
 /* (src/pf_rk3.f90:2323-2487, 3457-3531)                                        */
 /* ------------------------------------------------------------------------- */
-static void rk_coeffs(int stage, double* beta, double* gamma) {
+void rk_coeffs(int stage, double* beta, double* gamma) {
     if (stage == 1) { *beta = 0.0; *gamma = 1.0 / 3.0; }
     else if (stage == 2) { *beta = -(5.0 / 9.0); *gamma = 15.0 / 16.0; }
     else { *beta = -(153.0 / 128.0); *gamma = 8.0 / 15.0; }
@@ -691,6 +946,42 @@ static void particles_stage(oracle* o, int stage, int tstep, double dt) {
         double* ur = o->uprk + 3 * n;
         double* pr = o->prk + 3 * n;
         double uf[3];
+        if (o->shear) {
+            /* p_RK3SolveParticleBF (src/pp_rk3.f90:169-303): RK3 in the lab frame,
+             * p_RK3Mov2Lab / p_RK3Lab2Mov (src/pp_rk3.f90:989-1042) */
+            double ufm[3], xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};
+            interp3d(o, xp, ufm);
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (o->bexist[a][b]) { xl[a] = xl[a] + o->binv[a][b] * xp[b]; ul[a] = ul[a] + o->binv[a][b] * ufm[b]; }
+            if (init_vel) {   /* p_ControlInitPartVelocityBF (src/pp_control.f90:466-516) */
+                for (int c = 0; c < 3; c++) { up[c] = ul[c]; pr[c] = 0.0; ur[c] = 0.0; }
+            }
+            double dpv = o->dp[n];
+            if (dpv > 0.0) {
+                double tau = ((dpv * dpv) / (18.0 * o->p.f_nu)) * (o->p.p_rho / o->p.f_rho);
+                double hs[3] = {0, 0, 0};   /* p_RK3ComputeHomogeneousSourceTerm (src/pp_rk3.f90:1080-1102) */
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++)
+                        if (o->aexist[a][b]) hs[a] = hs[a] + o->amat[a][b] * up[b];
+                for (int c = 0; c < 3; c++) {
+                    double acc = ((ul[c] - up[c]) / tau) - hs[c];
+                    pr[c] = (beta * pr[c]) + acc;
+                    up[c] = up[c] + (gamma * dt * pr[c]);
+                }
+            } else {
+                for (int c = 0; c < 3; c++) up[c] = ul[c];
+            }
+            for (int c = 0; c < 3; c++) {
+                ur[c] = (beta * ur[c]) + up[c];
+                xl[c] = xl[c] + (gamma * dt * ur[c]);
+            }
+            double xm[3] = {0, 0, 0};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (o->bexist[a][b]) xm[a] = xm[a] + o->bmat[a][b] * xl[b];
+            for (int c = 0; c < 3; c++) xp[c] = xm[c];
+        } else {
         if (init_vel) {   /* p_ControlInitPartVelocity (src/pp_control.f90:378-416) */
             interp3d(o, xp, uf);
             for (int c = 0; c < 3; c++) { up[c] = uf[c]; pr[c] = 0.0; ur[c] = 0.0; }
@@ -711,6 +1002,7 @@ static void particles_stage(oracle* o, int stage, int tstep, double dt) {
             ur[c] = (beta * ur[c]) + up[c];
             xp[c] = xp[c] + (gamma * dt * ur[c]);
         }
+        }
         if (xp[0] < x1min) xp[0] = xp[0] + o->lx;
         if (xp[0] >= x1max) xp[0] = xp[0] - o->lx;
         if (xp[1] < x2min) xp[1] = xp[1] + o->ly;
@@ -722,11 +1014,30 @@ static void particles_stage(oracle* o, int stage, int tstep, double dt) {
     if (lost) o->status |= 4;
 }
 
+
+/* p_ControlRemesh -> p_MPIRemeshPosition (src/pp_mpi.f90:1062-1092): x1 += x3, one wrap */
+static void particles_remesh(oracle* o) {
+    if (!o->p.p_track_part || o->np == 0) return;
+    const double x1min = -0.5 * o->dx, x1max = x1min + o->lx;
+    for (long n = 0; n < o->np; n++) {
+        double* xp = o->xp + 3 * n;
+        xp[0] = xp[0] + xp[2];
+        if (xp[0] < x1min) xp[0] = xp[0] + o->lx;
+        if (xp[0] >= x1max) xp[0] = xp[0] - o->lx;
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* statistics (src/pf_fluidstats.f90:336-374, 696-780, 1423-1576)              */
 /* ------------------------------------------------------------------------- */
 static void mode_density(oracle* o) {
     double kmax = sqrt((double)((long)o->ki * o->ki + (long)o->kj * o->kj + (long)o->kk * o->kk));
+    if (o->p.f_type != PANDORA_F_ISOTROPIC) {
+        const pandora_params* p = &o->p;
+        kmax = sqrt((double)((double)o->ki * o->ki / (double)(p->b110 * p->b110) +
+                             (double)o->kj * o->kj / (double)(p->b220 * p->b220) +
+                             (double)o->kk * o->kk / (double)(p->b330 * p->b330)));
+    }
     double kmin = 1.0;
     o->kkmax = (int)lround(kmax / kmin);
     free(o->dens_mod);
@@ -750,8 +1061,70 @@ static void mode_density(oracle* o) {
     free(cnt);
 }
 
+
+/* lab-frame statistics of the moving-frame state, f_FluidstatsModeDensityBFRot
+ * (src/pf_fluidstats.f90:1977-2229) and f_FluidstatsFsPrimaryQuantsBFRot
+ * (src/pf_fluidstats.f90:1586-1960): k_lab = B^T k, u_lab = B^-1 u, mode density
+ * recomputed for the current B and divided by B110 B220 B330. */
+static void stats_bf(const oracle* o, double* ek, double* tke, double* eps) {
+    const int K = o->kkmax;
+    double* spec = dalloc(K + 1);
+    double* dis = dalloc(K + 1);
+    long* cnt = (long*)calloc((size_t)K + 2, sizeof(long));
+    double s11 = 0, s22 = 0, s33 = 0;
+    const double nu = o->p.f_nu;
+    for (int i = 0; i < o->nki; i++)
+        for (int j = 0; j < o->nkj; j++)
+            for (int k = 0; k < o->nkk; k++) {
+                long m = ((long)i * o->nkj + j) * o->nkk + k;
+                double km_[3] = {wvn(i, o->ki), wvn(j, o->kj), wvn(k, o->kk)};
+                cx um[3] = {o->u[0][m], o->u[1][m], o->u[2][m]};
+                double kl[3] = {0, 0, 0};
+                cx ul[3] = {{0, 0}, {0, 0}, {0, 0}};
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++)
+                        if (o->bexist[a][b]) {
+                            kl[b] = kl[b] + o->bmat[a][b] * km_[a];
+                            ul[a].re = ul[a].re + o->binv[a][b] * um[b].re;
+                            ul[a].im = ul[a].im + o->binv[a][b] * um[b].im;
+                        }
+                double km = sqrt((kl[0] * kl[0]) + (kl[1] * kl[1]) + (kl[2] * kl[2]));
+                double p11 = ul[0].re * ul[0].re + ul[0].im * ul[0].im;
+                double p22 = ul[1].re * ul[1].re + ul[1].im * ul[1].im;
+                double p33 = ul[2].re * ul[2].re + ul[2].im * ul[2].im;
+                if (i != 0) { p11 *= 2.0; p22 *= 2.0; p33 *= 2.0; }
+                s11 += p11; s22 += p22; s33 += p33;
+                double e = 0.5 * (p11 + p22 + p33);
+                double d = 2.0 * km * km * nu * e;
+                int kc = (int)floor(km + 0.5);
+                for (int q = kc - 1; q <= kc + 1; q++) {
+                    if (q < 1 || q > K) continue;
+                    double up = 1.0 * ((double)q + 0.5), lo = 1.0 * ((double)q - 0.5);
+                    if (km >= lo && km < up) { spec[q] += e; dis[q] += d; cnt[q] += (i != 0) ? 2 : 1; }
+                }
+            }
+    const double pi = (double)(3.14159265358979323846264338327950288L);
+    const double bvol = (double)o->p.b110 * (double)o->p.b220 * (double)o->p.b330;
+    double fdis = 0.0;
+    for (int q = 1; q <= K; q++) {
+        double up = (double)q + 0.5, lo = (double)q - 0.5;
+        double dm = (double)cnt[q] / (4.0 / 3.0 * pi * (up * up * up - lo * lo * lo));
+        dm = dm / bvol;
+        if (dm != 0.0) {
+            fdis += dis[q];
+            if (ek) ek[q - 1] = spec[q] / dm;
+        } else if (ek) {
+            ek[q - 1] = spec[q];
+        }
+    }
+    if (tke) *tke = 0.5 * (s11 + s22 + s33);
+    if (eps) *eps = fdis;
+    free(spec); free(dis); free(cnt);
+}
+
 /* ek[0..kkmax-1] = E(k) for shells kk=1..kkmax; tke; eps = f_dis. */
 void oracle_stats(const oracle* o, double* ek, double* tke, double* eps) {
+    if (o->p.f_type != PANDORA_F_ISOTROPIC) { stats_bf(o, ek, tke, eps); return; }
     const int K = o->kkmax;
     double* spec = dalloc(K + 1);
     double* dis = dalloc(K + 1);
@@ -835,7 +1208,7 @@ static double init_spec(const pandora_params* p, double kmag) {
 
 /* Rogallo construction of one mode from three uniform draws (src/pf_initialise.f90:160-205) */
 static void rogallo_mode(const pandora_params* p, double k1, double k2, double k3, double kmag,
-                         double r1, double r2, double r3, cx t[3]) {
+                         double r1, double r2, double r3, cx t[3], double fdiv) {
     const double twopi = (double)(6.283185307179586476925286766559005768L);
     const double fourpi = (double)(12.566370614359172953850573533118011536L);
     r1 = twopi * r1; r2 = twopi * r2; r3 = twopi * r3;
@@ -844,6 +1217,7 @@ static void rogallo_mode(const pandora_params* p, double k1, double k2, double k
     if (!(kmag > 0.0)) return;
     double ek = init_spec(p, kmag);
     double factor = sqrt(ek / (fourpi * kmag * kmag));
+    if (fdiv != 1.0) factor = factor / fdiv;
     cx al = {factor * cos(r1) * cos(r3), factor * sin(r1) * cos(r3)};
     cx be = {factor * cos(r2) * sin(r3), factor * sin(r2) * sin(r3)};
     if (!(k2d > 0.0)) return;
@@ -856,32 +1230,53 @@ static void rogallo_mode(const pandora_params* p, double k1, double k2, double k
     t[2].im = -(be.im * sqrt(k2d)) / kmag;
 }
 
+/* f_InitialiseFluid (src/pf_initialise.f90:97-512) and, when
+ * B110+B220+B330 > 3, f_InitialiseFluidDeformed (src/pf_initialise.f90:520-990):
+ * wavenumbers scaled by 1/B, amplitude by (B110 B220 B330)^-1/2, velocity mapped
+ * through bmat.  Same draw order in both. */
+static void deform_map(const oracle* o, cx t[3]) {
+    cx d[3] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int m = 0; m < 3; m++)
+        for (int n = 0; n < 3; n++)
+            if (o->bexist[m][n]) {
+                d[m].re = d[m].re + o->bmat[m][n] * t[n].re;
+                d[m].im = d[m].im + o->bmat[m][n] * t[n].im;
+            }
+    for (int c = 0; c < 3; c++) t[c] = d[c];
+}
+
 void oracle_init_fluid(oracle* o) {
     const pandora_params* p = &o->p;
     uint64_t key = pd_stream_key(p->seed_fluid, PD_TAG_FLUID);
     uint64_t n = 0;
     const int KJ = o->kj, KK = o->kk, NKJ = o->nkj, NKK = o->nkk, KI = o->ki;
+    const int deformed = (p->b110 + p->b220 + p->b330) > 3;
+    const double b1 = deformed ? (double)p->b110 : 1.0, b2 = deformed ? (double)p->b220 : 1.0;
+    const double b3 = deformed ? (double)p->b330 : 1.0;
+    const double fdiv = deformed ? pow((double)p->b110 * (double)p->b220 * (double)p->b330, 0.5) : 1.0;
     for (int c = 0; c < 3; c++) memset(o->u[c], 0, sizeof(cx) * o->S);
 #define U(c, i, j, k) o->u[c][((long)(i) * NKJ + (j)) * NKK + (k)]
     /* i = 0 plane with conjugate symmetry */
-    double k1 = 0.0;
+    double k1 = wvn(0, KI) / b1;
     for (int j = 0; j <= KJ; j++) {
-        double k2 = wvn(j, KJ);
+        double k2 = wvn(j, KJ) / b2;
         for (int k = 0; k <= KK; k++) {
-            double k3 = wvn(k, KK);
+            double k3 = wvn(k, KK) / b3;
             double r1 = pd_uniform(key, n++), r2 = pd_uniform(key, n++), r3 = pd_uniform(key, n++);
             double kmag = sqrt((k1 * k1) + (k2 * k2) + (k3 * k3));
             cx t[3];
-            rogallo_mode(p, k1, k2, k3, kmag, r1, r2, r3, t);
+            rogallo_mode(p, k1, k2, k3, kmag, r1, r2, r3, t, fdiv);
+            if (deformed) deform_map(o, t);
             int jj = (j != 0) ? NKJ - j : j;
             int kk = (k != 0) ? NKK - k : k;
             for (int c = 0; c < 3; c++) U(c, 0, j, k) = t[c];
             for (int c = 0; c < 3; c++) { U(c, 0, jj, kk).re = t[c].re; U(c, 0, jj, kk).im = -t[c].im; }
             if (k != 0) {
                 double k2n = wvn(jj, KJ);
-                if (p->b220 > 1) k2n = k2n / (double)p->b220;
+                if (deformed || p->b220 > 1) k2n = k2n / (double)p->b220;
                 r1 = pd_uniform(key, n++); r2 = pd_uniform(key, n++); r3 = pd_uniform(key, n++);
-                rogallo_mode(p, k1, k2n, k3, kmag, r1, r2, r3, t);
+                rogallo_mode(p, k1, k2n, k3, kmag, r1, r2, r3, t, fdiv);
+                if (deformed) deform_map(o, t);
                 for (int c = 0; c < 3; c++) U(c, 0, jj, k) = t[c];
                 for (int c = 0; c < 3; c++) { U(c, 0, j, kk).re = t[c].re; U(c, 0, j, kk).im = -t[c].im; }
             }
@@ -889,16 +1284,17 @@ void oracle_init_fluid(oracle* o) {
     }
     /* i >= 1; loops run one index past the stored range (draws consumed) */
     for (int i = 1; i <= o->nki; i++) {
-        double a = wvn(i, KI);
+        double a = wvn(i, KI) / b1;
         for (int j = 0; j <= NKJ; j++) {
-            double b = wvn(j, KJ);
+            double b = wvn(j, KJ) / b2;
             for (int k = 0; k <= NKK; k++) {
-                double c3 = wvn(k, KK);
+                double c3 = wvn(k, KK) / b3;
                 double r1 = pd_uniform(key, n++), r2 = pd_uniform(key, n++), r3 = pd_uniform(key, n++);
                 if (i > KI || j >= NKJ || k >= NKK) continue;
                 double kmag = sqrt((a * a) + (b * b) + (c3 * c3));
                 cx t[3];
-                rogallo_mode(p, a, b, c3, kmag, r1, r2, r3, t);
+                rogallo_mode(p, a, b, c3, kmag, r1, r2, r3, t, fdiv);
+                if (deformed) deform_map(o, t);
                 for (int c = 0; c < 3; c++) U(c, i, j, k) = t[c];
             }
         }
@@ -953,12 +1349,20 @@ static double tstep_dt(const oracle* o, double ucfl) {
 /* ------------------------------------------------------------------------- */
 /* f_RK3Stage{1,2,3} (src/pf_rk3.f90:40-200); *dt in/out */
 int oracle_stage(oracle* o, int stage, int tstep, double* dt) {
-    if (o->p.f_type != PANDORA_F_ISOTROPIC) return PANDORA_ERR_UNSUPPORTED;
+    if (o->p.f_type != PANDORA_F_ISOTROPIC && o->p.f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
+    if (stage == 1 && o->shear && oracle_remesh_due(o, tstep)) {
+        particles_remesh(o);
+        remesh_wave_space(o);
+    }
     compute_nonlinear(o, stage == 1);
     if (stage == 1) *dt = tstep_dt(o, o->ucfl);
     particles_stage(o, stage, tstep, *dt);
-    force_calc(o, tstep, stage, *dt);
-    form_f_iso(o, stage, *dt);
+    if (o->shear) {
+        form_f_bf(o, stage, *dt);
+    } else {
+        force_calc(o, tstep, stage, *dt);
+        form_f_iso(o, stage, *dt);
+    }
     return o->status ? PANDORA_ERR_NAN : 0;
 }
 
@@ -969,10 +1373,13 @@ int oracle_step(oracle* o, int tstep, double* simtime, double* dt) {
     int rc;
     if ((rc = oracle_stage(o, 1, tstep, &sim_dt))) return rc;
     *simtime = t0 + (1.0 / 3.0) * sim_dt;
+    oracle_update_b(o, tstep, *simtime);
     if ((rc = oracle_stage(o, 2, tstep, &sim_dt))) return rc;
     *simtime = t0 + (3.0 / 4.0) * sim_dt;
+    oracle_update_b(o, tstep, *simtime);
     if ((rc = oracle_stage(o, 3, tstep, &sim_dt))) return rc;
     *simtime = t0 + sim_dt;
+    oracle_update_b(o, tstep, *simtime);
     *dt = sim_dt;
     return 0;
 }

@@ -1,0 +1,171 @@
+// bfrot.cuh -- homogeneous shear in Rogallo (moving-frame) coordinates, the
+// "Bardino/Ferziger rotational" (BF-rot, NS_DEFORMED = 1) formulation.
+//
+// Transformation tensors as set by g_DomainCalc (src/pg_domain.f90:187-214):
+// binv = diag(B110, B220, B330) plus binv(1,3); bmat = diag(1/B110, 1/B220,
+// 1/B330) plus bmat(1,3); amat(1,3) = S.  Entries that exist: the diagonal and
+// (1,3) (bvalexist), and amat(1,3) (avalexist).  bmat(1,3), binv(1,3) follow the
+// closed form of g_RK3UpdateB (src/pg_rk3.f90:280-385) and live in the Clock.
+#pragma once
+#include "pandora_internal.cuh"
+
+namespace pd {
+
+struct BF {
+    double bm[3][3];
+    double bi[3][3];
+    double a13;     // amat(1,3) = F_DEFORM_S
+};
+
+__host__ __device__ __forceinline__ constexpr bool bex(int a, int b) { return a == b || (a == 0 && b == 2); }
+
+__device__ __forceinline__ BF make_bf(const Geo& g, const Clock* ck) {
+    BF f;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) { f.bm[a][b] = 0.0; f.bi[a][b] = 0.0; }
+    f.bm[0][0] = g.bdiag[0]; f.bm[1][1] = g.bdiag[1]; f.bm[2][2] = g.bdiag[2];
+    f.bi[0][0] = g.bidiag[0]; f.bi[1][1] = g.bidiag[1]; f.bi[2][2] = g.bidiag[2];
+    f.bm[0][2] = ck->b13;
+    f.bi[0][2] = ck->bi13;
+    f.a13 = g.shear_s;
+    return f;
+}
+
+// f_RK3VorticityBFRot (src/pf_rk3.f90:3786-3843), summed over the three velocity
+// components: w = sum_n omega(u_n).
+__device__ __forceinline__ void vort_bf(const BF& f, const double2* u, const double* k, double2* w) {
+    w[0] = make_double2(0.0, 0.0); w[1] = w[0]; w[2] = w[0];
+#pragma unroll
+    for (int n = 0; n < 3; n++) {
+        const double2 un = u[n];
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            if (bex(m, 0)) {
+                if (bex(2, n)) { const double c = f.bm[m][0] * f.bi[2][n] * k[m]; w[1].y -= c * un.x; w[1].x += c * un.y; }
+                if (bex(1, n)) { const double c = f.bm[m][0] * f.bi[1][n] * k[m]; w[2].y += c * un.x; w[2].x -= c * un.y; }
+            }
+            if (bex(m, 1)) {
+                if (bex(2, n)) { const double c = f.bm[m][1] * f.bi[2][n] * k[m]; w[0].y += c * un.x; w[0].x -= c * un.y; }
+                if (bex(0, n)) { const double c = f.bm[m][1] * f.bi[0][n] * k[m]; w[2].y -= c * un.x; w[2].x += c * un.y; }
+            }
+            if (bex(m, 2)) {
+                if (bex(1, n)) { const double c = f.bm[m][2] * f.bi[1][n] * k[m]; w[0].y -= c * un.x; w[0].x += c * un.y; }
+                if (bex(0, n)) { const double c = f.bm[m][2] * f.bi[0][n] * k[m]; w[1].y += c * un.x; w[1].x -= c * un.y; }
+            }
+        }
+    }
+}
+
+// f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711), pointwise in physical space.
+__device__ __forceinline__ void nl_bf(const BF& f, const double* u, const double* om, double* nl) {
+    double n1 = 0.0, n2 = 0.0, n3 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        if (bex(0, m)) { n3 -= om[1] * f.bi[0][m] * u[m]; n2 += om[2] * f.bi[0][m] * u[m]; }
+        if (bex(1, m)) { n1 -= om[2] * f.bi[1][m] * u[m]; n3 += om[0] * f.bi[1][m] * u[m]; }
+        if (bex(2, m)) { n1 += om[1] * f.bi[2][m] * u[m]; n2 -= om[0] * f.bi[2][m] * u[m]; }
+    }
+    nl[0] = n1; nl[1] = n2; nl[2] = n3;
+}
+
+// Right-hand side of f_RK3FormFBFRot for F_SHEAR_DNS (src/pf_rk3.f90:2494-2673):
+// viscous (2903-2937) - bmat NL (2864-2895) + pressure (2986-3070) - source
+// (3167-3209).  amat has the single entry (1,3).
+__device__ __forceinline__ void rhs_bf(const BF& f, double nu, const double* k, const double2* u,
+                                       const double2* nlr, double2* tot) {
+    double2 nl[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        nl[a] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (bex(a, b)) { nl[a].x += f.bm[a][b] * nlr[b].x; nl[a].y += f.bm[a][b] * nlr[b].y; }
+    }
+    // pressure
+    double p1[3] = {0.0, 0.0, 0.0}, p4 = 0.0;
+    double2 p2 = make_double2(0.0, 0.0), p3 = p2;
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        p2.x += k[m] * nl[m].x; p2.y += k[m] * nl[m].y;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (!bex(m, r)) continue;
+            if (r == 0) {   // amat(r, s) exists only for (r, s) = (1, 3)
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if (!bex(2, q)) continue;
+                    const double c = k[m] * f.bm[m][r] * f.a13 * f.bi[2][q];
+                    p3.x += 2.0 * (c * u[q].x); p3.y += 2.0 * (c * u[q].y);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                if (bex(q, r)) p4 += k[m] * f.bm[m][r] * f.bm[q][r] * k[q];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int pp = 0; pp < 3; pp++)
+            if (bex(a, pp))
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    if (bex(b, pp)) p1[a] += f.bm[a][pp] * f.bm[b][pp] * k[b];
+    // homogeneous source
+    double2 hom[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        hom[a] = make_double2(0.0, 0.0);
+        if (bex(a, 0)) {   // r = 1 is the only row of amat
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                if (!bex(2, q)) continue;
+                const double c = f.bm[a][0] * f.a13 * f.bi[2][q];
+                hom[a].x += 2.0 * (c * u[q].x); hom[a].y += 2.0 * (c * u[q].y);
+            }
+        }
+    }
+    // viscous
+    double vc = 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; l++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+            if (!bex(l, jj)) continue;
+#pragma unroll
+            for (int n = 0; n < 3; n++)
+                if (bex(n, jj)) vc += nu * f.bm[l][jj] * f.bm[n][jj] * k[l] * k[n];
+        }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] / p4) * (p2.x + p3.x), (p1[a] / p4) * (p2.y + p3.y))
+                                      : make_double2(0.0, 0.0);
+        tot[a] = make_double2(-vc * u[a].x - nl[a].x + pr.x - hom[a].x, -vc * u[a].y - nl[a].y + pr.y - hom[a].y);
+    }
+}
+
+// g_RK3UpdateB (src/pg_rk3.f90:280-385): closed-form bmat(1,3), binv(1,3) of a
+// shear flow at stage-end time `simtime` of step `tstep`.
+__host__ __device__ __forceinline__ void update_b(const Geo& g, int tstep, double simtime, double& b13,
+                                                  double& bi13) {
+    double localtime = simtime;
+    if (g.rk3_decide && tstep > g.b110 * g.remesh_t) {
+        const int a = tstep - (g.b110 * g.remesh_t) - 1;
+        const int b = 2 * (g.b110 * g.remesh_t);
+        const int lt = a / b;
+        localtime = simtime - ((double)(lt + 1) / g.shear_s * (double)g.b110);
+    }
+    b13 = -g.bdiag[0] * g.shear_s * localtime;
+    bi13 = g.shear_s * localtime / g.bdiag[2];
+}
+
+__host__ __device__ __forceinline__ bool remesh_due(const Geo& g, int tstep) {
+    if (!g.shear || !g.rk3_decide) return false;
+    const int a = tstep - (g.b110 * g.remesh_t) - 1;
+    const int b = 2 * g.b110 * g.remesh_t;
+    return (a % b) == 0;
+}
+
+}  // namespace pd

@@ -6,6 +6,7 @@
 #include <math.h>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
+#include "bfrot.cuh"
 
 namespace pd {
 
@@ -17,14 +18,24 @@ using pdfft::mk;
 // i != 0), d = 2 k^2 nu e, binned in [kk-1/2, kk+1/2).  Raw sums; the host
 // divides by the mode density.
 // ---------------------------------------------------------------------------
+size_t shell_words(const Geo& g) { return (size_t)3 * (g.kkmax + 1) + 3; }
+
+// Shear flow: the same sums in the laboratory frame, k_lab = B^T k and
+// u_lab = B^-1 u (f_FluidstatsFsPrimaryQuantsBFRot, src/pf_fluidstats.f90:1586-1960),
+// with the per-shell mode counts of f_FluidstatsModeDensityBFRot
+// (src/pf_fluidstats.f90:1977-2229), which change with B every step.
 __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
     extern __shared__ double sh[];
     const int K = g.kkmax;
-    double* se = sh;            // [K+1]
-    double* sd = sh + (K + 1);  // [K+1]
-    double* sp = sh + 2 * (K + 1);
-    for (int q = threadIdx.x; q < 2 * (K + 1) + 3; q += blockDim.x) sh[q] = 0.0;
+    double* se = sh;                // [K+1]
+    double* sd = sh + (K + 1);      // [K+1]
+    double* sp = sh + 2 * (K + 1);  // [3]
+    double* sc = sp + 3;            // [K+1] mode counts
+    const int nsh = 3 * (K + 1) + 3;
+    for (int q = threadIdx.x; q < nsh; q += blockDim.x) sh[q] = 0.0;
     __syncthreads();
+    BF bf;
+    if (g.shear) bf = make_bf(g, F.clock);
     double p11 = 0, p22 = 0, p33 = 0;
     const long long total = g.S;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < total;
@@ -32,11 +43,26 @@ __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
         const int k = (int)(m % g.nkk);
         const long long ij = m / g.nkk;
         const int jj = (int)(ij % g.nkj), i = (int)(ij / g.nkj);
-        const double a = (double)i, b = wvn(jj, g.kj), c = wvn(k, g.kk);
-        const double km = sqrt((a * a) + (b * b) + (c * c));
-        const double2 u1 = F.u[0][m], u2 = F.u[1][m], u3 = F.u[2][m];
-        double q11 = u1.x * u1.x + u1.y * u1.y, q22 = u2.x * u2.x + u2.y * u2.y;
-        double q33 = u3.x * u3.x + u3.y * u3.y;
+        double kv[3] = {(double)i, wvn(jj, g.kj), wvn(k, g.kk)};
+        double2 uv[3] = {F.u[0][m], F.u[1][m], F.u[2][m]};
+        if (g.shear) {
+            double kl[3] = {0.0, 0.0, 0.0};
+            double2 ul[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++)
+                    if (bex(a, b)) {
+                        kl[b] += bf.bm[a][b] * kv[a];
+                        ul[a].x += bf.bi[a][b] * uv[b].x;
+                        ul[a].y += bf.bi[a][b] * uv[b].y;
+                    }
+#pragma unroll
+            for (int a = 0; a < 3; a++) { kv[a] = kl[a]; uv[a] = ul[a]; }
+        }
+        const double km = sqrt((kv[0] * kv[0]) + (kv[1] * kv[1]) + (kv[2] * kv[2]));
+        double q11 = uv[0].x * uv[0].x + uv[0].y * uv[0].y, q22 = uv[1].x * uv[1].x + uv[1].y * uv[1].y;
+        double q33 = uv[2].x * uv[2].x + uv[2].y * uv[2].y;
         if (i != 0) { q11 *= 2.0; q22 *= 2.0; q33 *= 2.0; }
         p11 += q11; p22 += q22; p33 += q33;
         const double e = 0.5 * (q11 + q22 + q33);
@@ -48,6 +74,7 @@ __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
             if (km >= (double)q - 0.5 && km < (double)q + 0.5) {
                 atomicAdd(&se[q], e);
                 atomicAdd(&sd[q], d);
+                if (g.shear) atomicAdd(&sc[q], (i != 0) ? 2.0 : 1.0);
             }
         }
     }
@@ -55,7 +82,7 @@ __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
     atomicAdd(&sp[1], p22);
     atomicAdd(&sp[2], p33);
     __syncthreads();
-    for (int q = threadIdx.x; q < 2 * (K + 1) + 3; q += blockDim.x)
+    for (int q = threadIdx.x; q < nsh; q += blockDim.x)
         if (sh[q] != 0.0) atomicAdd(&F.shell[q], sh[q]);
 }
 
@@ -169,12 +196,13 @@ __global__ void __launch_bounds__(256) k_stage_scalars(Fields F, Geo g, StepPara
 
 // simtime after stage s: t0 + {1/3, 3/4, 1} dt (src/pg_rk3.f90:109-127); the step
 // counter advances after stage 3.
-__global__ void k_advance_time(Fields F, int stage) {
+__global__ void k_advance_time(Fields F, Geo g, int stage) {
     Clock* ck = F.clock;
     if (stage == 1) ck->simtime = ck->t0 + (1.0 / 3.0) * ck->dt;
     else if (stage == 2) ck->simtime = ck->t0 + (3.0 / 4.0) * ck->dt;
-    else {
-        ck->simtime = ck->t0 + ck->dt;
+    else ck->simtime = ck->t0 + ck->dt;
+    if (g.shear) update_b(g, ck->tstep, ck->simtime, ck->b13, ck->bi13);
+    if (stage == 3) {
         ck->t0 = ck->simtime;
         ck->tstep += 1;
     }
@@ -219,7 +247,7 @@ __device__ double init_spec(const InitParams& p, double kmag) {
 }
 
 __device__ void rogallo_mode(const InitParams& p, double k1, double k2, double k3, double kmag, double r1,
-                             double r2, double r3, double2 t[3]) {
+                             double r2, double r3, double2 t[3], double fdiv) {
     const double twopi = 6.283185307179586476925286766559005768;
     const double fourpi = 12.566370614359172953850573533118011536;
     r1 = twopi * r1; r2 = twopi * r2; r3 = twopi * r3;
@@ -227,7 +255,8 @@ __device__ void rogallo_mode(const InitParams& p, double k1, double k2, double k
     t[0] = t[1] = t[2] = mk(0.0, 0.0);
     if (!(kmag > 0.0)) return;
     const double ek = init_spec(p, kmag);
-    const double factor = sqrt(ek / (fourpi * kmag * kmag));
+    double factor = sqrt(ek / (fourpi * kmag * kmag));
+    if (fdiv != 1.0) factor = factor / fdiv;
     const double2 al = mk(factor * cos(r1) * cos(r3), factor * sin(r1) * cos(r3));
     const double2 be = mk(factor * cos(r2) * sin(r3), factor * sin(r2) * sin(r3));
     if (!(k2d > 0.0)) return;
@@ -237,29 +266,42 @@ __device__ void rogallo_mode(const InitParams& p, double k1, double k2, double k
     t[2] = mk(-(be.x * sqrt(k2d)) / kmag, -(be.y * sqrt(k2d)) / kmag);
 }
 
+// Deformed grid (f_InitialiseFluidDeformed, src/pf_initialise.f90:520-990): the
+// construction above in laboratory wavenumbers k/B, amplitude divided by
+// (B110 B220 B330)^(1/2), velocity mapped by bmat (diagonal at t = 0).
+__device__ __forceinline__ void deform_map(const Geo& g, double2 t[3]) {
+    for (int c = 0; c < 3; c++) t[c] = mk(g.bdiag[c] * t[c].x, g.bdiag[c] * t[c].y);
+}
+
 __global__ void k_init_fluid(Fields F, Geo g, InitParams ip) {
     const int KJ = g.kj, KK = g.kk, NKJ = g.nkj, NKK = g.nkk;
     const long long plane0 = (long long)(KJ + 1) * (KK + 1);
     const long long rest = (long long)g.ki * NKJ * NKK;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const double b1 = ip.deformed ? (double)ip.b110 : 1.0, b2 = ip.deformed ? (double)ip.b220 : 1.0;
+    const double b3 = ip.deformed ? (double)ip.b330 : 1.0;
+    const double fdiv = ip.deformed ? pow((double)ip.b110 * (double)ip.b220 * (double)ip.b330, 0.5) : 1.0;
     auto U = [&](int c, int i, int j, int k) -> double2& {
         return F.u[c][((long long)i * NKJ + j) * NKK + k];
     };
     if (idx < plane0) {
         const int j = (int)(idx / (KK + 1)), k = (int)(idx % (KK + 1));
         const uint64_t n = (uint64_t)j * 3 * (2 * KK + 1) + (k == 0 ? 0 : 3 + 6 * (uint64_t)(k - 1));
-        const double k1 = 0.0, k2 = wvn(j, KJ), k3 = wvn(k, KK);
+        const double k1 = 0.0 / b1, k2 = wvn(j, KJ) / b2, k3 = wvn(k, KK) / b3;
         const double kmag = sqrt((k1 * k1) + (k2 * k2) + (k3 * k3));
         double2 t[3];
-        rogallo_mode(ip, k1, k2, k3, kmag, uniform(ip.key, n), uniform(ip.key, n + 1), uniform(ip.key, n + 2), t);
+        rogallo_mode(ip, k1, k2, k3, kmag, uniform(ip.key, n), uniform(ip.key, n + 1), uniform(ip.key, n + 2), t,
+                     fdiv);
+        if (ip.deformed) deform_map(g, t);
         const int jj = (j != 0) ? NKJ - j : j, kk = (k != 0) ? NKK - k : k;
         for (int c = 0; c < 3; c++) U(c, 0, j, k) = t[c];
         for (int c = 0; c < 3; c++) U(c, 0, jj, kk) = mk(t[c].x, -t[c].y);
         if (k != 0) {
             double k2n = wvn(jj, KJ);
-            if (ip.b220 > 1) k2n = k2n / (double)ip.b220;
+            if (ip.deformed || ip.b220 > 1) k2n = k2n / (double)ip.b220;
             rogallo_mode(ip, k1, k2n, k3, kmag, uniform(ip.key, n + 3), uniform(ip.key, n + 4),
-                         uniform(ip.key, n + 5), t);
+                         uniform(ip.key, n + 5), t, fdiv);
+            if (ip.deformed) deform_map(g, t);
             for (int c = 0; c < 3; c++) U(c, 0, jj, k) = t[c];
             for (int c = 0; c < 3; c++) U(c, 0, j, kk) = mk(t[c].x, -t[c].y);
         }
@@ -272,11 +314,66 @@ __global__ void k_init_fluid(Fields F, Geo g, InitParams ip) {
     const int j = (int)(r2 % NKJ), i = 1 + (int)(r2 / NKJ);
     const uint64_t base1 = (uint64_t)(KJ + 1) * 3 * (2 * KK + 1);
     const uint64_t n = base1 + 3 * ((((uint64_t)(i - 1) * (NKJ + 1)) + j) * (NKK + 1) + k);
-    const double a = (double)i, b = wvn(j, KJ), c3 = wvn(k, KK);
+    const double a = (double)i / b1, b = wvn(j, KJ) / b2, c3 = wvn(k, KK) / b3;
     const double kmag = sqrt((a * a) + (b * b) + (c3 * c3));
     double2 t[3];
-    rogallo_mode(ip, a, b, c3, kmag, uniform(ip.key, n), uniform(ip.key, n + 1), uniform(ip.key, n + 2), t);
+    rogallo_mode(ip, a, b, c3, kmag, uniform(ip.key, n), uniform(ip.key, n + 1), uniform(ip.key, n + 2), t, fdiv);
+    if (ip.deformed) deform_map(g, t);
     for (int c = 0; c < 3; c++) U(c, i, j, k) = t[c];
+}
+
+// Wave-space remesh at stage 1 of a remesh step (f_RK3Remesh / f_RK3RemeshWaveSpace,
+// src/pf_rk3.f90:3958-4178): per (i,j) row k3 <- k3 - k1, modes below -KK
+// dropped, BF-rot u1 += u3; the frame jumps from S t = +B110/2 to -B110/2.  The
+// step number is read on the device, so the launch sits in every step's graph
+// and returns at once on the other steps.  One CTA per row, row staged in shared memory.
+__global__ void __launch_bounds__(256) k_remesh(Fields F, Geo g) {
+    Clock* ck = F.clock;
+    if (!remesh_due(g, ck->tstep)) return;
+    extern __shared__ double2 rowbuf[];   // [3][NKK]
+    const long long ij = blockIdx.x;
+    const int i = (int)(ij / g.nkj);
+    const int KK = g.kk, NKK = g.nkk, nodes = 2 * KK + 1;
+    for (int q = threadIdx.x; q < 3 * NKK; q += blockDim.x) rowbuf[q] = mk(0.0, 0.0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < NKK; k += blockDim.x) {
+        const int actualk = k > KK ? k - nodes : k;
+        int knew = actualk - i;
+        if (knew >= -KK) {
+            if (knew < 0) knew += nodes;
+            for (int c = 0; c < 3; c++) rowbuf[c * NKK + knew] = F.u[c][ij * NKK + k];
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < NKK; k += blockDim.x) {
+        const double2 a = rowbuf[k], b3 = rowbuf[2 * NKK + k];
+        F.u[0][ij * NKK + k] = mk(a.x + b3.x, a.y + b3.y);
+        F.u[1][ij * NKK + k] = rowbuf[NKK + k];
+        F.u[2][ij * NKK + k] = b3;
+    }
+    if (ij == 0 && threadIdx.x == 0) {
+        const double half_b = (double)g.b110 * 0.5;
+        ck->b13 = -g.bdiag[0] * (-half_b);
+        ck->bi13 = (-half_b) / g.bdiag[2];
+    }
+}
+
+// Particle positions at the remesh (p_MPIRemeshPosition, src/pp_mpi.f90:1062-1092).
+__global__ void k_remesh_particles(Particles P, Geo g, const Clock* ck) {
+    if (!remesh_due(g, ck->tstep)) return;
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.np) return;
+    const double x1min = -0.5 * g.dx, x1max = x1min + g.lx;
+    double x = P.xp[0][n] + P.xp[2][n];
+    if (x < x1min) x = x + g.lx;
+    if (x >= x1max) x = x - g.lx;
+    P.xp[0][n] = x;
+}
+
+cudaError_t launch_remesh(const Geo& g, const Fields& f, const Particles& p, cudaStream_t st) {
+    if (p.np > 0) k_remesh_particles<<<(unsigned)((p.np + 255) / 256), 256, 0, st>>>(p, g, f.clock);
+    k_remesh<<<(unsigned)((long long)g.nki * g.nkj), 256, sizeof(double2) * 3 * g.nkk, st>>>(f, g);
+    return cudaGetLastError();
 }
 
 // Non-finite check of the spectral state (sets PD_ST_NAN).
@@ -307,7 +404,7 @@ static int sm_count() {
 }
 
 cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st) {
-    const size_t nsh = (size_t)2 * (g.kkmax + 1) + 3;
+    const size_t nsh = shell_words(g);
     cudaError_t e = cudaMemsetAsync(f.shell, 0, sizeof(double) * nsh, st);
     if (e) return e;
     long long nb = (g.S + 255) / 256;
@@ -324,8 +421,8 @@ cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams
     return cudaGetLastError();
 }
 
-cudaError_t launch_advance_time(const Fields& f, int stage, cudaStream_t st) {
-    k_advance_time<<<1, 1, 0, st>>>(f, stage);
+cudaError_t launch_advance_time(const Geo& g, const Fields& f, int stage, cudaStream_t st) {
+    k_advance_time<<<1, 1, 0, st>>>(f, g, stage);
     return cudaGetLastError();
 }
 

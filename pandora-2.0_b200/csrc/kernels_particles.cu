@@ -15,6 +15,7 @@
 // L2 instead of gathering at random from a field larger than L2.
 #include <cuda_runtime.h>
 #include "pandora_internal.cuh"
+#include "bfrot.cuh"
 
 namespace pd {
 
@@ -99,7 +100,22 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
         }
         uf[c] = acc_z;
     }
-    // p_ControlInitPartVelocity at the release step (src/pp_control.f90:378-416)
+    double xw[3] = {xp[0], xp[1], xp[2]};   // frame in which the RK3 update runs
+    if (g.shear) {
+        // p_RK3SolveParticleBF (src/pp_rk3.f90:169-303): velocity and position to
+        // the laboratory frame (p_RK3Mov2Lab, src/pp_rk3.f90:989-1014), RK3 there,
+        // back with p_RK3Lab2Mov (1016-1042) at the same B.
+        const BF bf = make_bf(g, ck);
+        double xl[3] = {0.0, 0.0, 0.0}, ul[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                if (bex(a, b)) { xl[a] += bf.bi[a][b] * xp[b]; ul[a] += bf.bi[a][b] * uf[b]; }
+#pragma unroll
+        for (int c = 0; c < 3; c++) { xw[c] = xl[c]; uf[c] = ul[c]; }
+    }
+    // p_ControlInitPartVelocity(BF) at the release step (src/pp_control.f90:378-516)
     if (tstep == pp.release && stage == 1) {
 #pragma unroll
         for (int c = 0; c < 3; c++) { up[c] = uf[c]; pr[c] = 0.0; ur[c] = 0.0; }
@@ -107,9 +123,12 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
     const double dpv = P.dp[n];
     if (dpv > 0.0) {
         const double tau = ((dpv * dpv) / (18.0 * pp.f_nu)) * (pp.p_rho / pp.f_rho);
+        // shear: minus the homogeneous source amat up (p_RK3ComputeHomogeneousSourceTerm,
+        // src/pp_rk3.f90:1080-1102); amat has the single entry (1,3)
+        const double hs0 = g.shear ? g.shear_s * up[2] : 0.0;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const double acc = (uf[c] - up[c]) / tau;
+            const double acc = ((uf[c] - up[c]) / tau) - (c == 0 ? hs0 : 0.0);
             pr[c] = (beta * pr[c]) + acc;
             up[c] = up[c] + (gamma * dt * pr[c]);
         }
@@ -120,7 +139,21 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         ur[c] = (beta * ur[c]) + up[c];
-        xp[c] = xp[c] + (gamma * dt * ur[c]);
+        xw[c] = xw[c] + (gamma * dt * ur[c]);
+    }
+    if (g.shear) {
+        const BF bf = make_bf(g, ck);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            double v = 0.0;
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                if (bex(a, b)) v += bf.bm[a][b] * xw[b];
+            xp[a] = v;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; c++) xp[c] = xw[c];
     }
     const double x1min = -0.5 * g.dx, x2min = -0.5 * g.dy, x3min = -0.5 * g.dz;
     const double x1max = x1min + g.lx, x2max = x2min + g.ly, x3max = x3min + g.lz;

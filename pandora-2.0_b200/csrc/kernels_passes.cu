@@ -20,6 +20,7 @@
 #include <math.h>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
+#include "bfrot.cuh"
 
 namespace pd {
 
@@ -91,6 +92,8 @@ __global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F,
     const int KK = g.kk, NKK = g.nkk;
     const double2* u[3] = {F.u[0], F.u[1], F.u[2]};
     const long long row = ((long long)i * g.nkj + j) * NKK;
+    BF bf;
+    if (g.shear) bf = make_bf(g, F.clock);
     for (int f = 0; f < 6; f++) {
         double2* s = smem + (f % NB) * (tile_rows<NZ, PS>() * LP);
         if (NB == 1 && f > 0) __syncthreads();           // previous store has read the tile
@@ -98,7 +101,17 @@ __global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F,
         for (int k = lane; k < NKK; k += 32) {
             const int z = (k <= KK) ? k : NZ - NKK + k;
             double2 v = mk(0.0, 0.0);
-            if (i < g.nki) v = field_value(u, row + k, f, (double)i, k2, wvn(k, KK));
+            if (i < g.nki) {
+                if (g.shear && f >= 3) {   // BF-rot vorticity (f_RK3VorticityBFRot)
+                    const double kv[3] = {(double)i, k2, wvn(k, KK)};
+                    const double2 uv[3] = {u[0][row + k], u[1][row + k], u[2][row + k]};
+                    double2 w3[3];
+                    vort_bf(bf, uv, kv, w3);
+                    v = w3[f - 3];
+                } else {
+                    v = field_value(u, row + k, f, (double)i, k2, wvn(k, KK));
+                }
+            }
             col[prow<PS>(z) * LP] = v;
         }
         for (int z = KK + 1 + lane; z < NZ - KK; z += 32) col[prow<PS>(z) * LP] = mk(0.0, 0.0);
@@ -194,6 +207,8 @@ __global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys,
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int KI = g.ki, NKI = g.nki;
     double2* b = F.yb + q * g.nkip;
+    BF bf;
+    if (g.shear) bf = make_bf(g, F.clock);
     for (int m = lane; m < NKI; m += 32) {
 #pragma unroll
         for (int p = 0; p < 3; p++) {
@@ -222,8 +237,16 @@ __global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys,
             F.phys[2 * g.R + q * NX + n] = u3;
         }
         if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
-        e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
-        e[1] = mk(u2 * w1 - u1 * w2, 0.0);
+        if (g.shear) {   // f_RK3ComputeNonlinearBFRot
+            const double uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
+            double nl[3];
+            nl_bf(bf, uu, om, nl);
+            e[0] = mk(nl[0], nl[1]);
+            e[1] = mk(nl[2], 0.0);
+        } else {
+            e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
+            e[1] = mk(u2 * w1 - u1 * w2, 0.0);
+        }
     }
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
@@ -298,6 +321,8 @@ __global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int
     const double k1 = (double)i, k2 = wvn(j, g.kj);
     const int NK = g.fnk, FW = 2 * NK + 1;
     const long long row = ((long long)i * g.nkj + j) * NKK;
+    BF bf;
+    if (g.shear) bf = make_bf(g, F.clock);
     for (int k = lane; k < NKK; k += 32) {
         const long long m = row + k;
         const int z = (k <= KK) ? k : NZ - NKK + k;
@@ -316,6 +341,13 @@ __global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int
         const double kmag2 = (k1 * k1) + (k2 * k2) + (k3 * k3);
         if (!(kmag2 > 0.0)) continue;
         const double kv[3] = {k1, k2, k3};
+        double2 uu[3];
+        double2 tot[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) uu[c] = F.u[c][m];
+        if (g.shear) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
+            rhs_bf(bf, g.nu, kv, uu, nl, tot);
+        } else {
         const double2 kdn = mk(k1 * nl[0].x + k2 * nl[1].x + k3 * nl[2].x,
                                k1 * nl[0].y + k2 * nl[1].y + k3 * nl[2].y);
         double2 force[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
@@ -335,17 +367,18 @@ __global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int
                     force[c] = mk(fv[c].x - ((kv[c] / kmag2) * kdb.x), fv[c].y - ((kv[c] / kmag2) * kdb.y));
             }
         }
-        double2 uu[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
+                        -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+        }
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            uu[c] = F.u[c][m];
-            const double2 tot = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
-                                   -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
             double2 r;
-            if (stage == 1) r = tot;   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
+            if (stage == 1) r = tot[c];   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
             else {
                 const double2 r0 = F.rk[c][m];
-                r = mk((beta * r0.x) + tot.x, (beta * r0.y) + tot.y);
+                r = mk((beta * r0.x) + tot[c].x, (beta * r0.y) + tot[c].y);
             }
             F.rk[c][m] = r;
             uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));

@@ -12,6 +12,7 @@
 #include <new>
 #include <vector>
 #include "pandora_internal.cuh"
+#include "bfrot.cuh"
 
 using namespace pd;
 
@@ -109,6 +110,15 @@ static int kkmax_of(int ki, int kj, int kk) {
     const double kmax = sqrt((double)((long long)ki * ki + (long long)kj * kj + (long long)kk * kk));
     return (int)lround(kmax / 1.0);
 }
+// src/pf_fluidstats.f90:356-366: deformed domains scale k_max by 1/B
+static int kkmax_of(const pandora_params* p) {
+    const int ki = p->nodes_x / 3, kj = p->nodes_y / 3, kk = p->nodes_z / 3;
+    if (p->f_type == PANDORA_F_ISOTROPIC) return kkmax_of(ki, kj, kk);
+    const double kmax = sqrt((double)((double)ki * ki / (double)(p->b110 * p->b110) +
+                                      (double)kj * kj / (double)(p->b220 * p->b220) +
+                                      (double)kk * kk / (double)(p->b330 * p->b330)));
+    return (int)lround(kmax / 1.0);
+}
 
 extern "C" int pandora_sizes(const pandora_params* p, int32_t* nki, int32_t* nkj, int32_t* nkk, int64_t* modes,
                              int32_t* kkmax) {
@@ -118,7 +128,7 @@ extern "C" int pandora_sizes(const pandora_params* p, int32_t* nki, int32_t* nkj
     if (nkj) *nkj = 2 * kj + 1;
     if (nkk) *nkk = 2 * kk + 1;
     if (modes) *modes = (int64_t)(ki + 1) * (2 * kj + 1) * (2 * kk + 1);
-    if (kkmax) *kkmax = kkmax_of(ki, kj, kk);
+    if (kkmax) *kkmax = kkmax_of(p);
     return PANDORA_OK;
 }
 
@@ -145,7 +155,12 @@ static void release(pandora_handle* h) {
 static int validate(const pandora_params* p) {
     if (!p) return PANDORA_ERR_INVALID_ARG;
     if (p->precision != PANDORA_PREC_FP64) return PANDORA_ERR_UNSUPPORTED;
-    if (p->f_type != PANDORA_F_ISOTROPIC) return PANDORA_ERR_UNSUPPORTED;
+    if (p->f_type != PANDORA_F_ISOTROPIC && p->f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
+    if (p->f_type == PANDORA_F_SHEAR_DNS) {
+        if (p->ns_deformed != PANDORA_NS_BF_ROT) return PANDORA_ERR_UNSUPPORTED;
+        if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
+            return PANDORA_ERR_INVALID_ARG;
+    }
     if (p->dealiasing != 1) return PANDORA_ERR_UNSUPPORTED;
     if (!supported_length(p->nodes_x) || !supported_length(p->nodes_y) || !supported_length(p->nodes_z))
         return PANDORA_ERR_BAD_LAYOUT;
@@ -185,7 +200,14 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.dx = g.lx / (double)g.nx; g.dy = g.ly / (double)g.ny; g.dz = g.lz / (double)g.nz;
     g.force_kf = p->force_kf;
     g.fnk = (int)p->force_kf;
-    g.kkmax = kkmax_of(g.ki, g.kj, g.kk);
+    g.kkmax = kkmax_of(p);
+    g.shear = (p->f_type == PANDORA_F_SHEAR_DNS) ? 1 : 0;
+    g.bdiag[0] = 1.0 / (double)p->b110; g.bdiag[1] = 1.0 / (double)p->b220; g.bdiag[2] = 1.0 / (double)p->b330;
+    g.bidiag[0] = (double)p->b110; g.bidiag[1] = (double)p->b220; g.bidiag[2] = (double)p->b330;
+    g.shear_s = p->f_deform_s;
+    g.b110 = p->b110; g.remesh_t = p->f_remesh_t;
+    g.rk3_decide = (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) ? 1 : 0;
+    g.bvol = (double)p->b110 * (double)p->b220 * (double)p->b330;
     h->nforce = (long long)(g.fnk + 1) * (2 * g.fnk + 1) * (2 * g.fnk + 1);
     h->particles_on = p->p_track_part != 0;
 
@@ -203,7 +225,7 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     PD_ALLOC(h->F.forcing, sizeof(double2) * 3 * (size_t)h->nforce);
     PD_ALLOC(h->tw, sizeof(double2) * (size_t)(g.nx + g.ny + g.nz));
     PD_ALLOC(h->clock, sizeof(Clock));
-    const size_t nsh = (size_t)2 * (g.kkmax + 1) + 3;
+    const size_t nsh = shell_words(g);
     PD_ALLOC(h->shell_step, sizeof(double) * nsh);
     PD_ALLOC(h->shell_now, sizeof(double) * nsh);
 #undef PD_ALLOC
@@ -389,7 +411,8 @@ extern "C" int pandora_init_fluid(pandora_handle* h) {
     InitParams ip{};
     ip.type = h->p.f_init_type; ip.u0 = h->p.f_init_u0; ip.kp = h->p.f_init_kp; ip.kv = h->p.f_init_kv;
     ip.kstart = h->p.f_init_kstart; ip.kend = h->p.f_init_kend; ip.epsilon = h->p.f_init_epsilon;
-    ip.b220 = h->p.b220;
+    ip.b110 = h->p.b110; ip.b220 = h->p.b220; ip.b330 = h->p.b330;
+    ip.deformed = (h->p.b110 + h->p.b220 + h->p.b330) > 3 ? 1 : 0;
     ip.key = stream_key(h->p.seed_fluid, TAG_FLUID);
     PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
@@ -464,6 +487,9 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     const Geo& g = h->g;
     int n = 0;
     const bool part = h->particles_on && h->P.np > 0;
+    if (stage == 1 && g.shear) {
+        PD_CK(launch_remesh(g, h->F, h->P, h->st)); n += part ? 2 : 1;
+    }
     if (stage == 1 && part) {
         PD_CK(launch_particle_sort(g, h->P, h->sort, h->st, &n));
     }
@@ -479,7 +505,7 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     if (part) { PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->st)); n++; }
     PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
     PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n++;
-    PD_CK(launch_advance_time(h->F, stage, h->st)); n++;
+    PD_CK(launch_advance_time(g, h->F, stage, h->st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;
 }
@@ -522,6 +548,10 @@ static int set_clock(pandora_handle* h, int tstep, double simtime) {
     h->clock_host->tstep = tstep;
     h->clock_host->simtime = simtime;
     h->clock_host->t0 = simtime;
+    if (h->g.shear) {
+        // the frame of stage 1 of step tstep is the one g_RK3UpdateB set at the end of step tstep-1
+        update_b(h->g, tstep - 1, simtime, h->clock_host->b13, h->clock_host->bi13);
+    }
     PD_CK(cudaMemcpyAsync(h->clock, h->clock_host, sizeof(Clock), cudaMemcpyHostToDevice, h->st));
     return PANDORA_OK;
 }
@@ -578,6 +608,14 @@ static void finish_stats(pandora_handle* h, const double* sh, double* ek, int32_
     const double* se = sh;
     const double* sd = sh + (K + 1);
     const double* sp = sh + 2 * (K + 1);
+    const double* sc = sp + 3;
+    if (h->g.shear) {   // f_FluidstatsModeDensityBFRot: counts of this B, / (B110 B220 B330)
+        const double pi = 3.14159265358979323846264338327950288;
+        for (int q = 1; q <= K; q++) {
+            const double up = (double)q + 0.5, lo = (double)q - 0.5;
+            h->dens_mod[q] = sc[q] / (4.0 / 3.0 * pi * (up * up * up - lo * lo * lo)) / h->g.bvol;
+        }
+    }
     double fdis = 0.0;
     for (int q = 1; q <= K; q++) {
         if (h->dens_mod[q] != 0.0) {
@@ -598,7 +636,7 @@ extern "C" int pandora_stats(pandora_handle* h, double* ek, int32_t kkmax, doubl
     Fields Fs = h->F;
     Fs.shell = h->shell_now;
     PD_CK(launch_stats(h->g, Fs, h->st));
-    const size_t nsh = (size_t)2 * (h->g.kkmax + 1) + 3;
+    const size_t nsh = shell_words(h->g);
     PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_now, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
@@ -611,7 +649,7 @@ extern "C" int pandora_last_step_stats(pandora_handle* h, double* ek, int32_t kk
                                        double* ucfl) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(h->dev);
-    const size_t nsh = (size_t)2 * (h->g.kkmax + 1) + 3;
+    const size_t nsh = shell_words(h->g);
     PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_step, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
@@ -668,7 +706,7 @@ extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
     if (!h->launches_per_step) {
         // count without launching: same sequence as enqueue_step
         const bool part = h->particles_on && h->P.np > 0;
-        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0)) + (part ? 5 : 0);
+        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0)) + (part ? 5 : 0) + (h->g.shear ? (part ? 2 : 1) : 0);
     }
     *n = h->launches_per_step;
     return PANDORA_OK;
@@ -717,5 +755,15 @@ extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes
     case 7: *bytes = c16 * 3 * S; break;
     default: return PANDORA_ERR_INVALID_ARG;
     }
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_frame(pandora_handle* h, double* bmat13, double* binv13) {
+    if (!h || !bmat13 || !binv13) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    *bmat13 = h->clock_host->b13;
+    *binv13 = h->clock_host->bi13;
     return PANDORA_OK;
 }

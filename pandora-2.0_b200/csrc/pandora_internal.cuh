@@ -24,6 +24,13 @@ struct Geo {
     double force_kf;
     int fnk;              // aint(FORCE_KF)
     int kkmax;            // E(k) shells
+    // homogeneous shear (F_TYPE = F_SHEAR_DNS, BF-rot); zero for isotropic flow
+    int shear;
+    double bdiag[3];      // bmat(1,1), bmat(2,2), bmat(3,3) = 1/B110, 1/B220, 1/B330
+    double bidiag[3];     // binv diagonal = B110, B220, B330
+    double shear_s;       // F_DEFORM_S = amat(1,3)
+    int b110, remesh_t, rk3_decide;
+    double bvol;          // B110 B220 B330
 };
 
 // Scalars of the running step kept in device memory so that a whole step can
@@ -35,6 +42,7 @@ struct Clock {
     unsigned long long ucfl_bits;   // max |u1|+|u2|+|u3| of stage 1, as ordered bits
     int tstep;                      // number of the step being taken
     unsigned int status;            // PD_ST_* bits
+    double b13, bi13;               // bmat(1,3), binv(1,3) of the moving frame (shear)
 };
 
 enum : unsigned int {
@@ -75,7 +83,7 @@ struct Fields {
     double2* forcing;   // [3][NK+1][2NK+1][2NK+1]
     const double2 *tw_x, *tw_y, *tw_z;
     Clock* clock;
-    double* shell;      // [2*(kkmax+1) + 3] shell sums (e, d) + p11,p22,p33
+    double* shell;      // [3*(kkmax+1) + 3] shell sums (e, d), p11,p22,p33, mode counts
 };
 
 // Particle arrays, structure of arrays: 13 doubles + the particle's index in
@@ -123,7 +131,8 @@ struct PartParams {
 struct InitParams {
     int type;
     double u0, kp, kv, kstart, kend, epsilon;
-    int b220;
+    int b110, b220, b330;
+    int deformed;       // B110 + B220 + B330 > 3: f_InitialiseFluidDeformed
     uint64_t key;
 };
 
@@ -137,7 +146,7 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, in
 cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st);
 cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams& sp,
                                  const ForceParams& fp, int stage, cudaStream_t st);
-cudaError_t launch_advance_time(const Fields& f, int stage, cudaStream_t st);
+cudaError_t launch_advance_time(const Geo& g, const Fields& f, int stage, cudaStream_t st);
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);
 cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp,
                              int stage, cudaStream_t st);
@@ -146,6 +155,8 @@ cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key
 cudaError_t launch_particle_sort(const Geo& g, const Particles& p, const PartSort& s, cudaStream_t st,
                                  int* nlaunch);
 cudaError_t launch_check_finite(const Geo& g, const Fields& f, cudaStream_t st);
+cudaError_t launch_remesh(const Geo& g, const Fields& f, const Particles& p, cudaStream_t st);
+size_t shell_words(const Geo& g);
 
 // Shared-memory configuration (set once per process per device).
 cudaError_t configure_kernels(const Geo& g);

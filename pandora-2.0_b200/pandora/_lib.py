@@ -73,6 +73,7 @@ SIGNATURES = {
     "pandora_launches_per_step": [_vp, ctypes.POINTER(_i32)],
     "pandora_profile_pass": [_vp, _i32, _i32],
     "pandora_pass_bytes": [_vp, _i32, _dp],
+    "pandora_frame": [_vp, _dp, _dp],
 }
 _RESTYPES = {"pandora_strerror": ctypes.c_char_p}
 

@@ -120,6 +120,19 @@ def workload_params(name: str, n: int | None = None) -> Params:
         p.p_track_part, p.p_init_type, p.p_np_global = 1, P_INIT_RANDOM, 1 << 20
         p.p_interp_order, p.p_ts_release, p.p_dia_vals = 4, 1, 0.0
         return p
+    if name == "shear":
+        # homogeneous shear dU1/dx3 = S in Rogallo (moving-frame) coordinates,
+        # BF-rot formulation, lab box 4pi x 2pi x 2pi (B110 = 2), fixed dt =
+        # (0.5/S)/F_REMESH_T, remesh every S t = B110 (src/pf_rk3.f90:3921-4026)
+        p = default_params(n or 512)
+        p.b110 = 2
+        p.f_type, p.ns_deformed, p.f_deform_s = F_SHEAR_DNS, NS_BF_ROT, 1.0
+        p.rk3_timestep, p.f_remesh_t, p.tsteps = RK3_TIMESTEP_DECIDE, 250, 3000
+        p.f_nu, p.force_stop = 0.005, 0
+        p.f_init_type, p.f_init_kp, p.f_init_u0 = F_INIT_AHMED_ELGHOBASHI, 4.0, (2.0 / 3.0) * 0.5 ** 2
+        p.p_track_part, p.p_init_type, p.p_np_global = 1, P_INIT_RANDOM, 1 << 18
+        p.p_interp_order, p.p_ts_release, p.p_dia_vals = 4, 1, 0.0
+        return p
     raise ValueError(f"unknown workload {name!r}")
 
 

@@ -175,6 +175,12 @@ class Simulation:
                    "pandora_get_physical_velocity")
         return out
 
+    def frame(self):
+        """(bmat(1,3), binv(1,3)) of the moving frame (shear flow)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.L.pandora_frame(self.h, ctypes.byref(a), ctypes.byref(b)), "pandora_frame")
+        return a.value, b.value
+
     def check_status(self) -> None:
         _lib.check(self.L.pandora_check_status(self.h), "pandora_check_status")
 

@@ -1,0 +1,76 @@
+"""Homogeneous shear (Rogallo moving frame, BF-rot formulation) on the GPU
+against the oracle, through the C-ABI: state, statistics in the laboratory
+frame, frame tensors and particles, across a remesh."""
+import numpy as np
+import pytest
+
+from helpers import divergence, rel_l2, rel_l2_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _shear(pandora, n=32, remesh_t=5, npart=0):
+    p = pandora.workload_params("shear", n)
+    p.f_remesh_t = remesh_t          # remesh at step B110*remesh_t + 1, then every 2*B110*remesh_t
+    if npart:
+        p.p_np_global = npart
+    else:
+        p.p_track_part = 0
+    return p
+
+
+def test_deformed_init_matches_oracle(gpu_lib):
+    import oracle as O
+    p = _shear(gpu_lib, 48)
+    o = O.Oracle(p)
+    o.init_fluid()
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-13
+
+
+def test_shear_steps_across_remesh(gpu_lib):
+    import oracle as O
+    p = _shear(gpu_lib, 32, remesh_t=5)
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    o.set_state(s.get_state())
+    t = 0.0
+    for step in range(1, 26):
+        t, dt = o.step(step, t)
+        dtg = s.step(step)
+        assert dtg == dt == pytest.approx((0.5 / p.f_deform_s) / p.f_remesh_t, rel=1e-15)
+        if step in (1, 10, 11, 12, 25):      # 11: first remesh (B110 * F_REMESH_T + 1)
+            e = rel_l2_fields(s.get_state(), o.get_state())
+            assert e < 1e-10, (step, e)
+            gb, ob = s.frame(), o.frame()
+            assert gb == pytest.approx(ob, rel=1e-14, abs=1e-15), (step, gb, ob)
+            ek_g, tke_g, eps_g, _ = s.stats()
+            ek_o, tke_o, eps_o = o.stats()
+            assert rel_l2(ek_g, ek_o) < 1e-8 and abs(eps_g - eps_o) < 1e-8 * abs(eps_o), step
+            assert tke_g == pytest.approx(tke_o, rel=1e-10)
+    assert np.abs(divergence(p, s.get_state())).max() < 1e-14
+    s.close()
+
+
+def test_shear_particles(gpu_lib):
+    p = _shear(gpu_lib, 32, remesh_t=4, npart=2048)
+    import oracle as O
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    s.init_particles()
+    o.set_state(s.get_state())
+    o.set_particles(*s.get_particles())
+    t = 0.0
+    for step in range(1, 13):              # remesh at step 9
+        t, _ = o.step(step, t)
+        s.step(step)
+    xg = s.get_particles()[0]
+    xo = o.get_particles(p.p_np_global)[0]
+    d = np.abs(xg - xo)
+    d = np.minimum(d, 2 * np.pi - d)
+    assert d.max() < 1e-10, d.max()
+    s.check_status()
+    s.close()

@@ -1,0 +1,55 @@
+"""The shear (BF-rot) oracle: closed-form frame, remesh schedule and shift,
+fixed shear time step, solenoidal state (no GPU)."""
+import numpy as np
+import pytest
+
+from helpers import divergence
+
+
+def _o(n=24, remesh_t=5):
+    import oracle as O
+    from pandora.params import workload_params
+    p = workload_params("shear", n)
+    p.f_remesh_t = remesh_t
+    p.p_track_part = 0
+    return p, O.Oracle(p)
+
+
+def test_frame_closed_form_and_remesh_schedule():
+    p, o = _o()
+    b110, frt, S = p.b110, p.f_remesh_t, p.f_deform_s
+    assert [t for t in range(1, 60) if o.remesh_due(t)] == [11, 31, 51]
+    o.update_b(5, 0.3)
+    b13, bi13 = o.frame()
+    assert b13 == pytest.approx(-(1.0 / b110) * S * 0.3) and bi13 == pytest.approx(S * 0.3)
+    # after the first remesh the local time restarts at -B110/(2S) (src/pg_rk3.f90:330-339)
+    o.update_b(12, 1.2)
+    b13, bi13 = o.frame()
+    assert bi13 == pytest.approx(S * (1.2 - b110 / S))
+
+
+def test_remesh_shift_and_frame_jump():
+    p, o = _o(24, remesh_t=2)
+    o.init_fluid()
+    t = 0.0
+    for step in range(1, 5):
+        t, dt = o.step(step, t)
+        assert dt == pytest.approx(0.5 / p.f_deform_s / p.f_remesh_t)
+    before = o.get_state()
+    o.stage(1, 5, dt)                      # step 5 = B110 * F_REMESH_T + 1: remesh first
+    b13, bi13 = o.frame()
+    assert bi13 == pytest.approx(-p.b110 / 2.0)
+    assert b13 == pytest.approx((1.0 / p.b110) * p.b110 / 2.0)
+    after = o.get_state()
+    assert not np.allclose(before[2], after[2])
+
+
+def test_shear_state_stays_solenoidal():
+    p, o = _o(24)
+    o.init_fluid()
+    t = 0.0
+    for step in range(1, 16):
+        t, _ = o.step(step, t)
+    assert np.abs(divergence(p, o.get_state())).max() < 1e-15
+    ek, tke, eps = o.stats()
+    assert np.isfinite(ek).all() and tke > 0 and eps > 0
