@@ -221,6 +221,24 @@ int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps);
  * output written once, at the stored, unpadded extents). */
 int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes);
 
+/*
+ * No counterpart in the reference.  The nonlinear term omega x u of a spectral
+ * velocity field (the output of pandora_nonlinear), for callers that may not
+ * allocate device memory: they pass device buffers u1..u3 (input) and n1..n3
+ * (output), S complex values each in the layout above, and the call allocates
+ * nothing.  Its scratch is a set of fixed __device__ arrays (about 16 MB on every
+ * GPU that loads the library, held until exit), so grids are limited to 64
+ * points per direction (larger sizes return PANDORA_ERR_BAD_LAYOUT) and to
+ * isotropic flow.  All calls share that scratch: calls that overlap on the GPU
+ * race, so serialise them.  The first call on a device sets up the scratch
+ * addresses and should come before any stream capture on that device.  The call
+ * returns after the result is written (it synchronises `cuda_stream`, NULL = the
+ * legacy default stream).
+ */
+int pandora_nonlinear_static(const pandora_params* p, const double* u1, const double* u2,
+                             const double* u3, double* n1, double* n2, double* n3,
+                             void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

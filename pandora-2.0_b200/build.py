@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpandora_gpu.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["kernels_passes.cu", "kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu"]
-HEADERS = ["fft_core.cuh", "pandora_internal.cuh"]
+SOURCES = ["kernels_passes.cu", "kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu", "pandora_static.cu"]
+HEADERS = ["fft_core.cuh", "pandora_internal.cuh", "bfrot.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-v"]

@@ -74,6 +74,7 @@ SIGNATURES = {
     "pandora_profile_pass": [_vp, _i32, _i32],
     "pandora_pass_bytes": [_vp, _i32, _dp],
     "pandora_frame": [_vp, _dp, _dp],
+    "pandora_nonlinear_static": [ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPES = {"pandora_strerror": ctypes.c_char_p}
 
