@@ -200,6 +200,21 @@ def _config(a, p):
             "l2": f"no flush needed: each pass streams > 126 MB (y-pencil buffer alone {ws:.2f} GB)"}
 
 
+def _step_model(p, ms_per_step, peak):
+    ki, kj, kk = p.nodes_x // 3, p.nodes_y // 3, p.nodes_z // 3
+    S = (ki + 1) * (2 * kj + 1) * (2 * kk + 1)
+    Z = (ki + 1) * (2 * kj + 1) * p.nodes_z
+    Y = (ki + 1) * p.nodes_y * p.nodes_z
+    R = p.nodes_x * p.nodes_y * p.nodes_z
+    w = 8.0
+    b = 3 * 2 * w * (15 * S + 18 * Z + 18 * Y) + 2 * w * 3 * S
+    if p.p_track_part:
+        b += 3 * (6 * R * w + 18 * w * p.p_np_global)
+    achieved = b / (ms_per_step / 1e3) / 1e9
+    return {"bytes_per_step": b, "achieved": achieved, "frac": achieved / peak,
+            "model": "3 stages x 16 B x (15S + 18Z + 18Y) + stats 3S + particles 3 x (6R + 18Np) x 8 B"}
+
+
 def run_ours(a, p):
     import torch
     import pandora
@@ -313,15 +328,9 @@ def run_ours(a, p):
         "roofline": roofline,
         "step_model_gbs": None,
     }
-    # whole-step algorithmic bytes (5-pass model incl. particles and stage-1 stats)
-    step_bytes = 0.0
-    for pid in (1, 2, 3, 4, 5):
-        step_bytes += 3 * sim.pass_bytes(pid)
-    if p.p_track_part:
-        step_bytes += 3 * sim.pass_bytes(6)
-    step_bytes += sim.pass_bytes(7)
-    line["step_model_gbs"] = {"bytes_per_step": step_bytes, "achieved": step_bytes / (ms / a.steps / 1e3) / 1e9,
-                              "frac": step_bytes / (ms / a.steps / 1e3) / 1e9 / peak}
+    # whole-step algorithmic bytes: the fused 5-pass model (per stage 15 S + 18 Z + 18 Y
+    # complex words; particles add 6 R + 18 Np words per stage; stage-1 stats read 3 S)
+    line["step_model_gbs"] = _step_model(p, ms / a.steps, peak)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         v, cores, secs = cpu_baseline(_params(a))
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",

@@ -214,7 +214,8 @@ int pandora_launches_per_step(pandora_handle* h, int32_t* n);
 /* Profiling hook: enqueues `reps` launches of one pass of a stage-2 step on the
  * handle's stream, without synchronising (callers bracket it with their own
  * events).  pass: 1 z-inverse, 2 y-inverse, 3 x-pass (NL), 4 y-forward,
- * 5 z-forward + RK update, 6 particles, 7 spectral statistics.  Passes 5 and 6
+ * 5 z-forward then the per-mode RK update (two launches), 6 particles,
+ * 7 spectral statistics.  Passes 5 and 6
  * advance the state; use only on a scratch simulation. */
 int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps);
 /* Algorithmic HBM bytes of one launch of `pass` (each input read once, each

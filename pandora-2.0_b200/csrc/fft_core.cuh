@@ -257,6 +257,36 @@ __device__ __forceinline__ void wpass(double2* s, const double2* __restrict__ tw
     __syncwarp();
 }
 
+// NA lines at columns 0..NA-1 of `s` transformed in lockstep by one warp: each
+// pass has NA times the independent work of a single line.
+template <int N, int R, int NS, int S, int LP, int PS, int NA>
+__device__ __forceinline__ void wpass_n(double2* s, const double2* __restrict__ tw, int lane) {
+    constexpr int WORK = (N / R) * NA;
+    constexpr int IT = (WORK + 31) / 32;
+    double2 v[IT][R];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = lane + it * 32;
+        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS>(s, tw, w, v[it]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int w = lane + it * 32;
+        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS>(s, w, v[it]);
+    }
+    __syncwarp();
+}
+
+template <int N, int S, int LP, int PS, int NA>
+__device__ __forceinline__ void fft_warp_n(double2* s, const double2* __restrict__ tw, int lane) {
+    static_assert(wplan_ok<N>(), "no warp radix plan for this length");
+    constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
+    wpass_n<N, R0, 1, S, LP, PS, NA>(s, tw, lane);
+    if constexpr (R1 != 0) wpass_n<N, R1, R0, S, LP, PS, NA>(s, tw, lane);
+    if constexpr (R2 != 0) wpass_n<N, R2, R0 * R1, S, LP, PS, NA>(s, tw, lane);
+}
+
 // Full length-N transform of the line at column 0 of `s` by the calling warp
 // (the caller makes the line's data visible to the warp before the call).
 template <int N, int S, int LP, int PS>

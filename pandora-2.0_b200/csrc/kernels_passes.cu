@@ -39,11 +39,27 @@ constexpr int LP = L + 1;         // padded row of the tile (odd: conflict-free 
 // K1 double-buffers its tile where shared memory allows; K3 holds three
 // complex lines per warp, so long lines get fewer warps per CTA.
 template <int N> struct Cfg {
-    static constexpr int NB1 = (N <= 512) ? 2 : 1;
+    // resident CTAs per SM asked of the register allocator (64 registers at 4)
+    static constexpr int MINB = (N <= 256) ? 4 : ((N <= 512) ? 2 : 1);
+    static constexpr int NB1 = (N <= 256) ? 1 : ((N <= 512) ? 2 : 1);
     static constexpr int NWX = (N <= 512) ? 8 : 4;
-    static constexpr int L5 = (N <= 512) ? 8 : 4;     // K5 lines (= warps) per CTA
-    static constexpr int LP5 = L5 + 1;
+    static constexpr int MINBX = (N <= 256) ? 2 : 1;   // K3 CTAs per SM (shared memory allows 2 up to 256)
+    static constexpr int NAX = 1;                      // K3 arrays transformed in lockstep per warp
 };
+
+// Twiddle table staged in shared memory (after the tiles) where it fits; the
+// per-item twiddle reads of a pass then hit shared memory instead of L1.
+template <int N> constexpr bool tw_smem() { return N <= 512; }
+template <int N>
+__device__ __forceinline__ const double2* stage_twiddles(double2* dst, const double2* __restrict__ src) {
+    if constexpr (!tw_smem<N>()) {
+        return src;
+    } else {
+        for (int q = threadIdx.x; q < N; q += blockDim.x) dst[q] = src[q];
+        __syncthreads();
+        return dst;
+    }
+}
 
 #define PD_FOR_EACH_N(X) \
     X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
@@ -81,13 +97,14 @@ __device__ __forceinline__ double2 field_value(const double2* const* u, long lon
 }
 
 template <int NZ>
-__global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F, Geo g, int stage) {
+__global__ void __launch_bounds__(NT, Cfg<NZ>::MINB) k_zpass_inv(Fields F, Geo g, int stage) {
     constexpr int NB = Cfg<NZ>::NB1;
     extern __shared__ double2 smem[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int i0 = blockIdx.x * L, j = blockIdx.y;
     const int i = i0 + w;
     if (stage == 1 && blockIdx.x == 0 && j == 0 && tid == 0) F.clock->ucfl_bits = 0ull;
+    const double2* tw = stage_twiddles<NZ>(smem + NB * (tile_rows<NZ, PS>() * LP), F.tw_z);
     const double k2 = wvn(j, g.kj);
     const int KK = g.kk, NKK = g.nkk;
     const double2* u[3] = {F.u[0], F.u[1], F.u[2]};
@@ -116,7 +133,7 @@ __global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F,
         }
         for (int z = KK + 1 + lane; z < NZ - KK; z += 32) col[prow<PS>(z) * LP] = mk(0.0, 0.0);
         __syncwarp();
-        fft_warp<NZ, +1, LP, PS>(col, F.tw_z, lane);
+        fft_warp<NZ, +1, LP, PS>(col, tw, lane);
         __syncthreads();
         double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
         const long long zs = (long long)g.nkj * g.nkip;
@@ -132,11 +149,12 @@ __global__ void __launch_bounds__(NT, (NZ <= 512) ? 2 : 1) k_zpass_inv(Fields F,
 // src/pf_rk3.f90:1458-1473).  CTA = (i tile, z, field).
 // ---------------------------------------------------------------------------
 template <int NY>
-__global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_inv(Fields F, Geo g) {
+__global__ void __launch_bounds__(NT, Cfg<NY>::MINB) k_ypass_inv(Fields F, Geo g) {
     extern __shared__ double2 s[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
     const int KJ = g.kj, NKJ = g.nkj, npad = NY - NKJ;
+    const double2* tw = stage_twiddles<NY>(s + tile_rows<NY, PS>() * LP, F.tw_y);
     const double2* src = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
     for (int q = tid; q < NKJ * L; q += NT) {
         const int l = q % L, jj = q / L;
@@ -148,7 +166,7 @@ __global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_inv(Fields F,
         s[prow<PS>(y) * LP + l] = mk(0.0, 0.0);
     }
     __syncthreads();
-    fft_warp<NY, +1, LP, PS>(s + w, F.tw_y, lane);
+    fft_warp<NY, +1, LP, PS>(s + w, tw, lane);
     __syncthreads();
     double2* dst = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
     for (int q = tid; q < NY * L; q += NT) {
@@ -162,17 +180,18 @@ __global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_inv(Fields F,
 // (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
 // ---------------------------------------------------------------------------
 template <int NY>
-__global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_fwd(Fields F, Geo g) {
+__global__ void __launch_bounds__(NT, Cfg<NY>::MINB) k_ypass_fwd(Fields F, Geo g) {
     extern __shared__ double2 s[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const double2* tw = stage_twiddles<NY>(s + tile_rows<NY, PS>() * LP, F.tw_y);
     const double2* src = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
     for (int q = tid; q < NY * L; q += NT) {
         const int l = q % L, y = q / L;
         s[prow<PS>(y) * LP + l] = src[(long long)y * g.nkip + l];
     }
     __syncthreads();
-    fft_warp<NY, -1, LP, PS>(s + w, F.tw_y, lane);
+    fft_warp<NY, -1, LP, PS>(s + w, tw, lane);
     __syncthreads();
     const int KJ = g.kj, NKJ = g.nkj;
     double2* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
@@ -196,13 +215,14 @@ __global__ void __launch_bounds__(NT, (NY <= 512) ? 2 : 1) k_ypass_fwd(Fields F,
 // Warp shared region: element n of array p at s[prow(n)*3 + p].
 // ---------------------------------------------------------------------------
 template <int NX>
-__global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys, int want_cfl) {
+__global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, int want_phys, int want_cfl) {
     constexpr int LPX = 3;
     extern __shared__ double2 smem[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const long long lines = (long long)g.ny * g.nz;
+    const double2* tw = stage_twiddles<NX>(smem + (size_t)Cfg<NX>::NWX * tile_rows<NX, PS>() * LPX, F.tw_x);
     const long long q = (long long)blockIdx.x * Cfg<NX>::NWX + w;
-    if (q >= lines) return;                       // whole warp; the kernel has no block barrier
+    if (q >= lines) return;                       // whole warp; no block barrier follows
     double2* s = smem + (size_t)w * tile_rows<NX, PS>() * LPX;
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int KI = g.ki, NKI = g.nki;
@@ -223,9 +243,13 @@ __global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys,
         for (int p = 0; p < 3; p++) s[prow<PS>(n) * LPX + p] = mk(0.0, 0.0);
     }
     __syncwarp();
-    fft_warp<NX, +1, LPX, PS>(s + 0, F.tw_x, lane);
-    fft_warp<NX, +1, LPX, PS>(s + 1, F.tw_x, lane);
-    fft_warp<NX, +1, LPX, PS>(s + 2, F.tw_x, lane);
+    if constexpr (Cfg<NX>::NAX == 3) {
+        pdfft::fft_warp_n<NX, +1, LPX, PS, 3>(s, tw, lane);
+    } else {
+        fft_warp<NX, +1, LPX, PS>(s + 0, tw, lane);
+        fft_warp<NX, +1, LPX, PS>(s + 1, tw, lane);
+        fft_warp<NX, +1, LPX, PS>(s + 2, tw, lane);
+    }
     double umax = 0.0;
     for (int n = lane; n < NX; n += 32) {
         double2* e = s + prow<PS>(n) * LPX;
@@ -253,8 +277,12 @@ __global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys,
         if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong(umax));
     }
     __syncwarp();
-    fft_warp<NX, -1, LPX, PS>(s + 0, F.tw_x, lane);
-    fft_warp<NX, -1, LPX, PS>(s + 1, F.tw_x, lane);
+    if constexpr (Cfg<NX>::NAX == 3) {
+        pdfft::fft_warp_n<NX, -1, LPX, PS, 2>(s, tw, lane);
+    } else {
+        fft_warp<NX, -1, LPX, PS>(s + 0, tw, lane);
+        fft_warp<NX, -1, LPX, PS>(s + 1, tw, lane);
+    }
     for (int m = lane; m < g.nkip; m += 32) {
         double2 n1 = mk(0.0, 0.0), n2 = n1, n3 = n1;
         if (m < NKI) {
@@ -273,12 +301,11 @@ __global__ void __launch_bounds__(NT, 1) k_xpass(Fields F, Geo g, int want_phys,
 
 // ---------------------------------------------------------------------------
 // K5: forward z transforms x normalisation, truncate k (f_RK3TransformkRs2Fs +
-// f_Fftw_k_Rs2Fs, src/pf_rk3.f90:2242-2316, src/pf_fftw.f90:841-879), then per
-// mode f_RK3FormFIsotropic + f_RK3RungeKutta + f_RK3ContinuityFixIsotropic
-// (src/pf_rk3.f90:2323-2487, 3457-3531).  Warp w transforms line i = i0 + w of
-// each NL field, keeps its truncated values in T, and updates its own modes
-// (u, rk rows along k, coalesced).  mode 1 stores NL-hat into rk instead (the
-// transform test hook of src/ptf_rk3.f90:629-734).
+// f_Fftw_k_Rs2Fs, src/pf_rk3.f90:2242-2316, src/pf_fftw.f90:841-879) into NL-hat
+// (K5a), then the per-mode update (K5b).  NL-hat goes to the y-pencil buffer,
+// which K4 has finished with; mode 1 writes it into rk instead and stops there
+// (the transform test hook of src/ptf_rk3.f90:629-734).  Splitting costs 2 x 3S
+// complex words of traffic but lets both halves stream at full occupancy.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void rk_coeffs(int stage, double& beta, double& gamma) {
     if (stage == 1) { beta = 0.0; gamma = 1.0 / 3.0; }
@@ -286,73 +313,70 @@ __device__ __forceinline__ void rk_coeffs(int stage, double& beta, double& gamma
     else { beta = -(153.0 / 128.0); gamma = 8.0 / 15.0; }
 }
 
+// K5a: CTA = (i tile, j); the three NL fields in turn: tile load, barrier, warp
+// w transforms line i = i0 + w and stores its truncated, normalised values as a
+// contiguous k row of NL-hat [c][i][j][k] (coalesced per warp).
+struct Out3 { double2* p[3]; };
+
 template <int NZ>
-__global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int stage, int mode) {
-    constexpr int L5 = Cfg<NZ>::L5, LP5 = Cfg<NZ>::LP5, NT5 = 32 * L5;
-    extern __shared__ double2 smem[];
-    double2* s = smem;                                      // tile [rows(NZ)][LP5]
-    double2* T = smem + tile_rows<NZ, PS>() * LP5;          // fields 0, 1: [2][NKK][LP5]
+__global__ void __launch_bounds__(NT, Cfg<NZ>::MINB) k_zpass_fwd(Fields F, Geo g, Out3 nlh) {
+    extern __shared__ double2 s[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i0 = blockIdx.x * L5, j = blockIdx.y;
+    const int i0 = blockIdx.x * L, j = blockIdx.y;
+    const int i = i0 + w;
     const int KK = g.kk, NKK = g.nkk;
+    const long long zs = (long long)g.nkj * g.nkip;
+    const double2* tw = stage_twiddles<NZ>(s + tile_rows<NZ, PS>() * LP, F.tw_z);
     for (int f = 0; f < 3; f++) {
         if (f > 0) __syncthreads();                         // warps are done with the previous tile
         const double2* src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
-        const long long zs = (long long)g.nkj * g.nkip;
-        for (int q = tid; q < NZ * L5; q += NT5) {
-            const int l = q % L5, z = q / L5;
-            s[prow<PS>(z) * LP5 + l] = src[z * zs + l];
+        for (int q = tid; q < NZ * L; q += NT) {
+            const int l = q % L, z = q / L;
+            s[prow<PS>(z) * LP + l] = src[z * zs + l];
         }
         __syncthreads();
-        fft_warp<NZ, -1, LP5, PS>(s + w, F.tw_z, lane);
-        if (f < 2) {
+        fft_warp<NZ, -1, LP, PS>(s + w, tw, lane);
+        if (i < g.nki) {
+            double2* dst = nlh.p[f] + ((long long)i * g.nkj + j) * NKK;
             for (int k = lane; k < NKK; k += 32) {
                 const int z = (k <= KK) ? k : NZ - NKK + k;
-                T[(f * NKK + k) * LP5 + w] = s[prow<PS>(z) * LP5 + w];
+                const double2 v = s[prow<PS>(z) * LP + w];
+                dst[k] = mk(v.x * g.norm, v.y * g.norm);
             }
         }
     }
-    __syncwarp();
-    const int i = i0 + w;
-    if (i >= g.nki) return;                                 // no block barrier follows
-    const double dt = F.clock->dt;
+}
+
+// K5b: per mode f_RK3FormFIsotropic / f_RK3FormFBFRot + f_RK3RungeKutta +
+// f_RK3ContinuityFixIsotropic (src/pf_rk3.f90:2323-2673, 3457-3531), one thread
+// per mode, streaming NL-hat, u and rk.
+__global__ void __launch_bounds__(256) k_rk_update(Fields F, Geo g, const double2* __restrict__ nlh, int stage) {
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= g.S) return;
+    const int NKK = g.nkk;
+    const int k = (int)(m % NKK);
+    const long long ij = m / NKK;
+    const int j = (int)(ij % g.nkj), i = (int)(ij / g.nkj);
+    const double k1 = (double)i, k2 = wvn(j, g.kj), k3 = wvn(k, g.kk);
+    const double kmag2 = (k1 * k1) + (k2 * k2) + (k3 * k3);
+    if (!(kmag2 > 0.0)) return;
     double beta, gamma;
     rk_coeffs(stage, beta, gamma);
-    const double k1 = (double)i, k2 = wvn(j, g.kj);
-    const int NK = g.fnk, FW = 2 * NK + 1;
-    const long long row = ((long long)i * g.nkj + j) * NKK;
-    BF bf;
-    if (g.shear) bf = make_bf(g, F.clock);
-    for (int k = lane; k < NKK; k += 32) {
-        const long long m = row + k;
-        const int z = (k <= KK) ? k : NZ - NKK + k;
-        double2 nl[3];
+    const double dt = F.clock->dt;
+    const double kv[3] = {k1, k2, k3};
+    double2 nl[3], uu[3], tot[3];
 #pragma unroll
-        for (int c = 0; c < 2; c++) nl[c] = T[(c * NKK + k) * LP5 + w];
-        nl[2] = s[prow<PS>(z) * LP5 + w];
-#pragma unroll
-        for (int c = 0; c < 3; c++) nl[c] = mk(nl[c].x * g.norm, nl[c].y * g.norm);
-        if (mode == 1) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) F.rk[c][m] = nl[c];
-            continue;
-        }
-        const double k3 = wvn(k, KK);
-        const double kmag2 = (k1 * k1) + (k2 * k2) + (k3 * k3);
-        if (!(kmag2 > 0.0)) continue;
-        const double kv[3] = {k1, k2, k3};
-        double2 uu[3];
-        double2 tot[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) uu[c] = F.u[c][m];
-        if (g.shear) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
-            rhs_bf(bf, g.nu, kv, uu, nl, tot);
-        } else {
+    for (int c = 0; c < 3; c++) { nl[c] = nlh[c * g.S + m]; uu[c] = F.u[c][m]; }
+    if (g.shear) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
+        const BF bf = make_bf(g, F.clock);
+        rhs_bf(bf, g.nu, kv, uu, nl, tot);
+    } else {
         const double2 kdn = mk(k1 * nl[0].x + k2 * nl[1].x + k3 * nl[2].x,
                                k1 * nl[0].y + k2 * nl[1].y + k3 * nl[2].y);
         double2 force[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
         const double kmag = sqrt(kmag2);
         if (kmag <= g.force_kf && kmag > 0.0) {
+            const int NK = g.fnk, FW = 2 * NK + 1;
             const int jw = (int)k2, kw = (int)k3;
             if (i <= NK && jw >= -NK && jw <= NK && kw >= -NK && kw <= NK) {
                 double2 fv[3];
@@ -371,38 +395,39 @@ __global__ void __launch_bounds__(NT, 1) k_zpass_fwd_update(Fields F, Geo g, int
         for (int c = 0; c < 3; c++)
             tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
                         -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
-        }
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            double2 r;
-            if (stage == 1) r = tot[c];   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
-            else {
-                const double2 r0 = F.rk[c][m];
-                r = mk((beta * r0.x) + tot[c].x, (beta * r0.y) + tot[c].y);
-            }
-            F.rk[c][m] = r;
-            uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
-        }
-        const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x,
-                               k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-            F.u[c][m] = mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2));
     }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double2 r;
+        if (stage == 1) r = tot[c];   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
+        else {
+            const double2 r0 = F.rk[c][m];
+            r = mk((beta * r0.x) + tot[c].x, (beta * r0.y) + tot[c].y);
+        }
+        F.rk[c][m] = r;
+        uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
+    }
+    const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x, k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        F.u[c][m] = mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2));
 }
 
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+template <int N> static size_t tw_words() { return tw_smem<N>() ? (size_t)N : 0; }
 template <int N> static size_t smem_k1() {
-    return sizeof(double2) * (size_t)Cfg<N>::NB1 * tile_rows<N, PS>() * LP;
+    return sizeof(double2) * ((size_t)Cfg<N>::NB1 * tile_rows<N, PS>() * LP + tw_words<N>());
 }
-template <int N> static size_t smem_ky() { return sizeof(double2) * (size_t)tile_rows<N, PS>() * LP; }
+template <int N> static size_t smem_ky() {
+    return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
+}
 template <int N> static size_t smem_kx() {
-    return sizeof(double2) * (size_t)Cfg<N>::NWX * tile_rows<N, PS>() * 3;
+    return sizeof(double2) * ((size_t)Cfg<N>::NWX * tile_rows<N, PS>() * 3 + tw_words<N>());
 }
-template <int N> static size_t smem_k5(const Geo& g) {
-    return sizeof(double2) * ((size_t)tile_rows<N, PS>() + 2 * (size_t)g.nkk) * Cfg<N>::LP5;
+template <int N> static size_t smem_k5() {
+    return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
 }
 
 template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
@@ -414,7 +439,7 @@ cudaError_t configure_kernels(const Geo& g) {
 #define PD_CFG(N)                                                                     \
     if (g.nz == N) {                                                                  \
         if ((e = set_smem(k_zpass_inv<N>, smem_k1<N>()))) return e;                   \
-        if ((e = set_smem(k_zpass_fwd_update<N>, smem_k5<N>(g)))) return e;           \
+        if ((e = set_smem(k_zpass_fwd<N>, smem_k5<N>()))) return e;                   \
     }                                                                                 \
     if (g.ny == N) {                                                                  \
         if ((e = set_smem(k_ypass_inv<N>, smem_ky<N>()))) return e;                   \
@@ -484,17 +509,20 @@ cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
 }
 
 cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, int mode, cudaStream_t st) {
+    Out3 nlh;
+    for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? f.rk[c] : f.yb + c * g.S;
     switch (g.nz) {
 #define PD_L(N)                                                                             \
-    case N: {                                                                               \
-        dim3 grid((g.nki + Cfg<N>::L5 - 1) / Cfg<N>::L5, g.nkj);                            \
-        k_zpass_fwd_update<N><<<grid, 32 * Cfg<N>::L5, smem_k5<N>(g), st>>>(f, g, stage, mode); \
-        break;                                                                              \
-    }
+    case N:                                                                                 \
+        k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k5<N>(), st>>>(f, g, nlh);       \
+        break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
+    cudaError_t e = cudaGetLastError();
+    if (e || mode == 1) return e;
+    k_rk_update<<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
     return cudaGetLastError();
 }
 

@@ -504,7 +504,7 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     PD_CK(launch_stage_scalars(g, h->F, h->sp, h->fp, stage, h->st)); n++;
     if (part) { PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->st)); n++; }
     PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
-    PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n++;
+    PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
     PD_CK(launch_advance_time(g, h->F, stage, h->st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;
@@ -706,7 +706,7 @@ extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
     if (!h->launches_per_step) {
         // count without launching: same sequence as enqueue_step
         const bool part = h->particles_on && h->P.np > 0;
-        h->launches_per_step = 1 + 3 * (7 + (part ? 1 : 0)) + (part ? 5 : 0) + (h->g.shear ? (part ? 2 : 1) : 0);
+        h->launches_per_step = 1 + 3 * (8 + (part ? 1 : 0)) + (part ? 5 : 0) + (h->g.shear ? (part ? 2 : 1) : 0);
     }
     *n = h->launches_per_step;
     return PANDORA_OK;
@@ -750,7 +750,7 @@ extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes
     case 2: *bytes = c16 * (6 * Z + 6 * Y); break;
     case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? 8.0 * 3 * R : 0.0); break;
     case 4: *bytes = c16 * (3 * Y + 3 * Z); break;
-    case 5: *bytes = c16 * (3 * Z + 6 * S + 6 * S); break;
+    case 5: *bytes = c16 * (3 * Z + 3 * S) + c16 * (3 * S + 6 * S + 6 * S); break;   // K5a + K5b
     case 6: *bytes = part ? 8.0 * (3 * R + 24.0 * (double)h->P.np) : 0.0; break;
     case 7: *bytes = c16 * 3 * S; break;
     default: return PANDORA_ERR_INVALID_ARG;
