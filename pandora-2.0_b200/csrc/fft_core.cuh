@@ -188,12 +188,18 @@ template <int N, int PS> constexpr int tile_rows() { return PS > 0 ? N + (N >> P
 // One pass, split into a load/compute half and a store half so that a CPU
 // emulator can run all items' first halves before any second half (that is
 // what the __syncthreads() between them does on the GPU).
-template <int N, int R, int NS, int S, int L, int LP, int PS = 0>
+// Element n of line l: interleaved columns (AS = 0, s[prow(n)*LP + l]) or separate
+// arrays AS elements apart (s[l*AS + prow(n)]).
+template <int LP, int PS, int AS> PD_HD int tidx(int n, int l) {
+    return AS ? l * AS + prow<PS>(n) : prow<PS>(n) * LP + l;
+}
+
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0>
 PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
     constexpr int NR = N / R;
     const int l = w % L, j = w / L;
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = s[prow<PS>(j + r * NR) * LP + l];
+    for (int r = 0; r < R; r++) v[r] = s[tidx<LP, PS, AS>(j + r * NR, l)];
     if constexpr (NS > 1) {
         const int k = j % NS;
         constexpr int step = N / (NS * R);
@@ -202,13 +208,65 @@ PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
     }
     dft<R, S>(v);
 }
-template <int N, int R, int NS, int L, int LP, int PS = 0>
+template <int N, int R, int NS, int L, int LP, int PS = 0, int AS = 0>
 PD_HD void pass_store(double2* s, int w, const double2* v) {
     const int l = w % L, j = w / L;
     const int k = j % NS;
     const int d = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) s[prow<PS>(d + r * NS) * LP + l] = v[r];
+    for (int r = 0; r < R; r++) s[tidx<LP, PS, AS>(d + r * NS, l)] = v[r];
+}
+
+// Transforms whose first pass reads global memory and whose last pass writes it
+// ("direct" tile transforms).  The L lines of a tile are interleaved in shared
+// memory, element n of line l at s[n*L + l] with L = 8: the 8 threads of a
+// quarter-warp always own the 8 lines of one butterfly, so every shared access of
+// every pass is one contiguous 128-byte row (no bank conflicts, no pad rows), and
+// the same 8 threads touch 8 lines x 16 bytes of global memory per element.
+// The first pass takes element n of line l from ld(n, l); the last pass hands
+// output n of line l to st(n, l, value).  A two-pass length costs one shared-memory
+// round trip per element instead of four.
+template <int N, int R, int S, int L, class Ld>
+PD_HD void pass_first(double2* s, int w, Ld& ld) {
+    constexpr int NR = N / R;
+    const int l = w % L, j = w / L;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = ld(j + r * NR, l);
+    dft<R, S>(v);
+#pragma unroll
+    for (int r = 0; r < R; r++) s[(j * R + r) * L + l] = v[r];
+}
+template <int N, int R, int S, int L, class St>
+PD_HD void pass_last(const double2* s, const double2* tw, int w, St& st) {
+    constexpr int NS = N / R;
+    double2 v[R];
+    pass_load<N, R, NS, S, L, L, 0>(s, tw, w, v);
+    const int l = w % L, j = w / L;
+#pragma unroll
+    for (int r = 0; r < R; r++) st(j + r * NS, l, v[r]);
+}
+// Single-pass lengths: global to global, no shared memory.
+template <int N, int S, int L, class Ld, class St>
+PD_HD void pass_only(int l, Ld& ld, St& st) {
+    double2 v[N];
+#pragma unroll
+    for (int r = 0; r < N; r++) v[r] = ld(r, l);
+    dft<N, S>(v);
+#pragma unroll
+    for (int r = 0; r < N; r++) st(r, l, v[r]);
+}
+
+// Threads per CTA of a direct tile transform of L = 8 lines: one item per thread
+// in the widest pass, at most 512.
+template <int N> constexpr int tile_items_max() {
+    constexpr int a = N / Plan<N>::r0;
+    constexpr int b = Plan<N>::r1 ? N / Plan<N>::r1 : 0;
+    constexpr int c = Plan<N>::r2 ? N / Plan<N>::r2 : 0;
+    return 8 * (a > b ? (a > c ? a : c) : (b > c ? b : c));
+}
+template <int N> constexpr int tile_threads() {
+    return tile_items_max<N>() < 64 ? 64 : (tile_items_max<N>() > 512 ? 512 : tile_items_max<N>());
 }
 
 // Radix schedule of the warp-level transforms (one line per warp): radix 8 where
@@ -235,6 +293,17 @@ template <int N> constexpr bool wplan_ok() {
     return WPlan<N>::r0 * (WPlan<N>::r1 ? WPlan<N>::r1 : 1) * (WPlan<N>::r2 ? WPlan<N>::r2 : 1) == N;
 }
 
+// Fewer, larger passes (radix 16) for kernels limited by shared-memory bandwidth
+// rather than by registers: each pass costs a full read and write of the line.
+template <int N> struct WPlanL : WPlan<N> {};
+template <> struct WPlanL<128> { static constexpr int r0 = 16, r1 = 8, r2 = 0; };
+template <> struct WPlanL<256> { static constexpr int r0 = 16, r1 = 16, r2 = 0; };
+template <> struct WPlanL<48> { static constexpr int r0 = 3, r1 = 16, r2 = 0; };
+
+template <int N> constexpr bool wplanl_ok() {
+    return WPlanL<N>::r0 * (WPlanL<N>::r1 ? WPlanL<N>::r1 : 1) * (WPlanL<N>::r2 ? WPlanL<N>::r2 : 1) == N;
+}
+
 #if defined(__CUDACC__)
 // One pass of a single line owned by one warp: the line is column 0 of `s`
 // (element n at s[prow<PS>(n)*LP]); only __syncwarp() separates the halves.
@@ -257,9 +326,11 @@ __device__ __forceinline__ void wpass(double2* s, const double2* __restrict__ tw
     __syncwarp();
 }
 
-// NA lines at columns 0..NA-1 of `s` transformed in lockstep by one warp: each
-// pass has NA times the independent work of a single line.
-template <int N, int R, int NS, int S, int LP, int PS, int NA>
+// NA lines transformed in lockstep by one warp (interleaved columns 0..NA-1 for
+// AS = 0, else separate arrays AS elements apart): each pass has NA times the
+// independent work of a single line, which fills the lanes a radix-16 pass of
+// one line leaves idle.
+template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0>
 __device__ __forceinline__ void wpass_n(double2* s, const double2* __restrict__ tw, int lane) {
     constexpr int WORK = (N / R) * NA;
     constexpr int IT = (WORK + 31) / 32;
@@ -267,32 +338,36 @@ __device__ __forceinline__ void wpass_n(double2* s, const double2* __restrict__ 
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS>(s, tw, w, v[it]);
+        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS, AS>(s, tw, w, v[it]);
     }
     __syncwarp();
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS>(s, w, v[it]);
+        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS, AS>(s, w, v[it]);
     }
     __syncwarp();
 }
 
-template <int N, int S, int LP, int PS, int NA>
+template <int N, int S, int LP, int PS, int NA, bool LOWPASS = false, int AS = 0>
 __device__ __forceinline__ void fft_warp_n(double2* s, const double2* __restrict__ tw, int lane) {
-    static_assert(wplan_ok<N>(), "no warp radix plan for this length");
-    constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
-    wpass_n<N, R0, 1, S, LP, PS, NA>(s, tw, lane);
-    if constexpr (R1 != 0) wpass_n<N, R1, R0, S, LP, PS, NA>(s, tw, lane);
-    if constexpr (R2 != 0) wpass_n<N, R2, R0 * R1, S, LP, PS, NA>(s, tw, lane);
+    static_assert(wplan_ok<N>() && wplanl_ok<N>(), "no warp radix plan for this length");
+    constexpr int R0 = LOWPASS ? WPlanL<N>::r0 : WPlan<N>::r0;
+    constexpr int R1 = LOWPASS ? WPlanL<N>::r1 : WPlan<N>::r1;
+    constexpr int R2 = LOWPASS ? WPlanL<N>::r2 : WPlan<N>::r2;
+    wpass_n<N, R0, 1, S, LP, PS, NA, AS>(s, tw, lane);
+    if constexpr (R1 != 0) wpass_n<N, R1, R0, S, LP, PS, NA, AS>(s, tw, lane);
+    if constexpr (R2 != 0) wpass_n<N, R2, R0 * R1, S, LP, PS, NA, AS>(s, tw, lane);
 }
 
 // Full length-N transform of the line at column 0 of `s` by the calling warp
 // (the caller makes the line's data visible to the warp before the call).
-template <int N, int S, int LP, int PS>
+template <int N, int S, int LP, int PS, bool LOWPASS = false>
 __device__ __forceinline__ void fft_warp(double2* s, const double2* __restrict__ tw, int lane) {
-    static_assert(wplan_ok<N>(), "no warp radix plan for this length");
-    constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
+    static_assert(wplan_ok<N>() && wplanl_ok<N>(), "no warp radix plan for this length");
+    constexpr int R0 = LOWPASS ? WPlanL<N>::r0 : WPlan<N>::r0;
+    constexpr int R1 = LOWPASS ? WPlanL<N>::r1 : WPlan<N>::r1;
+    constexpr int R2 = LOWPASS ? WPlanL<N>::r2 : WPlan<N>::r2;
     wpass<N, R0, 1, S, LP, PS>(s, tw, lane);
     if constexpr (R1 != 0) wpass<N, R1, R0, S, LP, PS>(s, tw, lane);
     if constexpr (R2 != 0) wpass<N, R2, R0 * R1, S, LP, PS>(s, tw, lane);
@@ -326,6 +401,28 @@ __device__ __forceinline__ void fft_tile(double2* s, const double2* __restrict__
     pass<N, R0, 1, S, L, LP, NT>(s, tw, tid);
     if constexpr (R1 != 0) pass<N, R1, R0, S, L, LP, NT>(s, tw, tid);
     if constexpr (R2 != 0) pass<N, R2, R0 * R1, S, L, LP, NT>(s, tw, tid);
+}
+
+// Direct tile transform of L interleaved lines by NT threads (see pass_first).
+// The caller makes `s` free before the call (a barrier after any earlier use);
+// on return other threads may still read `s`.
+template <int N, int S, int L, int NT, class Ld, class St>
+__device__ __forceinline__ void fft_tile_io(double2* s, const double2* __restrict__ tw, int tid, Ld& ld, St& st) {
+    static_assert(plan_ok<N>(), "no radix plan for this length");
+    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+    if constexpr (R1 == 0) {
+        for (int l = tid; l < L; l += NT) pass_only<N, S, L>(l, ld, st);
+    } else {
+        constexpr int W0 = (N / R0) * L;
+#pragma unroll
+        for (int w = tid; w < W0; w += NT) pass_first<N, R0, S, L>(s, w, ld);
+        __syncthreads();
+        if constexpr (R2 != 0) pass<N, R1, R0, S, L, L, NT>(s, tw, tid);   // in place, ends with a barrier
+        constexpr int RL = R2 ? R2 : R1;
+        constexpr int WL = (N / RL) * L;
+#pragma unroll
+        for (int w = tid; w < WL; w += NT) pass_last<N, RL, S, L>(s, tw, w, st);
+    }
 }
 #endif
 

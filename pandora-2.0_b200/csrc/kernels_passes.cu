@@ -18,6 +18,7 @@
 // whole lines per warp and needs no block barrier at all.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
@@ -37,19 +38,18 @@ constexpr int L = NW;             // lines per tile, one per warp
 constexpr int LP = L + 1;         // padded row of the tile (odd: conflict-free transposes)
 
 // K1 double-buffers its tile where shared memory allows; K3 holds three
-// complex lines per warp, so long lines get fewer warps per CTA.
+// complex arrays per warp, so long lines get fewer warps per CTA.
 template <int N> struct Cfg {
     // resident CTAs per SM asked of the register allocator (64 registers at 4)
     static constexpr int MINB = (N <= 256) ? 4 : ((N <= 512) ? 2 : 1);
     static constexpr int NB1 = (N <= 256) ? 1 : ((N <= 512) ? 2 : 1);
     static constexpr int NWX = (N <= 512) ? 8 : 4;
     static constexpr int MINBX = (N <= 256) ? 2 : 1;   // K3 CTAs per SM (shared memory allows 2 up to 256)
-    static constexpr int NAX = 1;                      // K3 arrays transformed in lockstep per warp
 };
 
 // Twiddle table staged in shared memory (after the tiles) where it fits; the
 // per-item twiddle reads of a pass then hit shared memory instead of L1.
-template <int N> constexpr bool tw_smem() { return N <= 512; }
+template <int N> constexpr bool tw_smem() { return false; }   // measured slower: shared memory is the busier unit
 template <int N>
 __device__ __forceinline__ const double2* stage_twiddles(double2* dst, const double2* __restrict__ src) {
     if constexpr (!tw_smem<N>()) {
@@ -212,18 +212,28 @@ __global__ void __launch_bounds__(NT, Cfg<NY>::MINB) k_ypass_fwd(Fields F, Geo g
 // truncated to i = 0..KI (src/pf_fftw.f90:780).  NL overwrites yb fields 0..2 of
 // the same line.  Optionally writes the physical velocity (arr_u*_3r,
 // src/pf_rk3.f90:1108-1115) and the CFL maximum (src/pf_fluidstats.f90:913-917).
-// Warp shared region: element n of array p at s[prow(n)*3 + p].
+// Warp shared region: three arrays XAS elements apart (XAS = 4 mod 8 in 16-byte
+// units), element n of array p at s[p*XAS + prow<XPS>(n)].  Up to N = 256 the
+// warp transforms arrays 0 and 1 in lockstep (a radix-16 pass of one array
+// leaves half the lanes idle); with the offset of 4 bank groups between the two
+// arrays and XPS chosen per length, those passes are free of bank conflicts.
 // ---------------------------------------------------------------------------
+template <int N> constexpr int xps() {
+    return (N == 16 || N == 32) ? 2 : ((N == 24 || N == 64 || N == 192 || N == 384 || N == 512) ? 3 : 4);
+}
+template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
+template <int N> constexpr int xna() { return N <= 256 ? 2 : 1; }
+
 template <int NX>
 __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, int want_phys, int want_cfl) {
-    constexpr int LPX = 3;
+    constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
     extern __shared__ double2 smem[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const long long lines = (long long)g.ny * g.nz;
-    const double2* tw = stage_twiddles<NX>(smem + (size_t)Cfg<NX>::NWX * tile_rows<NX, PS>() * LPX, F.tw_x);
+    const double2* tw = F.tw_x;
     const long long q = (long long)blockIdx.x * Cfg<NX>::NWX + w;
     if (q >= lines) return;                       // whole warp; no block barrier follows
-    double2* s = smem + (size_t)w * tile_rows<NX, PS>() * LPX;
+    double2* s = smem + (size_t)w * 3 * XAS;
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int KI = g.ki, NKI = g.nki;
     double2* b = F.yb + q * g.nkip;
@@ -234,26 +244,26 @@ __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, i
         for (int p = 0; p < 3; p++) {
             double2 X = b[(2 * p) * fstride + m], Y = b[(2 * p + 1) * fstride + m];
             if (m == 0) { X.y = 0.0; Y.y = 0.0; }
-            s[prow<PS>(m) * LPX + p] = mk(X.x - Y.y, X.y + Y.x);
-            if (m > 0) s[prow<PS>(NX - m) * LPX + p] = mk(X.x + Y.y, -X.y + Y.x);
+            s[p * XAS + prow<XPS>(m)] = mk(X.x - Y.y, X.y + Y.x);
+            if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
         }
     }
     for (int n = KI + 1 + lane; n < NX - KI; n += 32) {
 #pragma unroll
-        for (int p = 0; p < 3; p++) s[prow<PS>(n) * LPX + p] = mk(0.0, 0.0);
+        for (int p = 0; p < 3; p++) s[p * XAS + prow<XPS>(n)] = mk(0.0, 0.0);
     }
     __syncwarp();
-    if constexpr (Cfg<NX>::NAX == 3) {
-        pdfft::fft_warp_n<NX, +1, LPX, PS, 3>(s, tw, lane);
+    if constexpr (NA == 2) {
+        pdfft::fft_warp_n<NX, +1, 1, XPS, 2, true, XAS>(s, tw, lane);
     } else {
-        fft_warp<NX, +1, LPX, PS>(s + 0, tw, lane);
-        fft_warp<NX, +1, LPX, PS>(s + 1, tw, lane);
-        fft_warp<NX, +1, LPX, PS>(s + 2, tw, lane);
+        fft_warp<NX, +1, 1, XPS, true>(s, tw, lane);
+        fft_warp<NX, +1, 1, XPS, true>(s + XAS, tw, lane);
     }
+    fft_warp<NX, +1, 1, XPS, true>(s + 2 * XAS, tw, lane);
     double umax = 0.0;
     for (int n = lane; n < NX; n += 32) {
-        double2* e = s + prow<PS>(n) * LPX;
-        const double2 a = e[0], bb = e[1], c = e[2];
+        double2* e = s + prow<XPS>(n);
+        const double2 a = e[0], bb = e[XAS], c = e[2 * XAS];
         const double u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
         if (want_phys) {
             F.phys[q * NX + n] = u1;
@@ -266,10 +276,10 @@ __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, i
             double nl[3];
             nl_bf(bf, uu, om, nl);
             e[0] = mk(nl[0], nl[1]);
-            e[1] = mk(nl[2], 0.0);
+            e[XAS] = mk(nl[2], 0.0);
         } else {
             e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
-            e[1] = mk(u2 * w1 - u1 * w2, 0.0);
+            e[XAS] = mk(u2 * w1 - u1 * w2, 0.0);
         }
     }
     if (want_cfl) {
@@ -277,20 +287,20 @@ __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, i
         if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong(umax));
     }
     __syncwarp();
-    if constexpr (Cfg<NX>::NAX == 3) {
-        pdfft::fft_warp_n<NX, -1, LPX, PS, 2>(s, tw, lane);
+    if constexpr (NA == 2) {
+        pdfft::fft_warp_n<NX, -1, 1, XPS, 2, true, XAS>(s, tw, lane);
     } else {
-        fft_warp<NX, -1, LPX, PS>(s + 0, tw, lane);
-        fft_warp<NX, -1, LPX, PS>(s + 1, tw, lane);
+        fft_warp<NX, -1, 1, XPS, true>(s, tw, lane);
+        fft_warp<NX, -1, 1, XPS, true>(s + XAS, tw, lane);
     }
     for (int m = lane; m < g.nkip; m += 32) {
         double2 n1 = mk(0.0, 0.0), n2 = n1, n3 = n1;
         if (m < NKI) {
             const int mc = (NX - m) % NX;
-            const double2 Z = s[prow<PS>(m) * LPX], Zc = s[prow<PS>(mc) * LPX];
+            const double2 Z = s[prow<XPS>(m)], Zc = s[prow<XPS>(mc)];
             n1 = mk(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
             n2 = mk(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-            const double2 W = s[prow<PS>(m) * LPX + 1], Wc = s[prow<PS>(mc) * LPX + 1];
+            const double2 W = s[XAS + prow<XPS>(m)], Wc = s[XAS + prow<XPS>(mc)];
             n3 = mk(0.5 * (W.x + Wc.x), 0.5 * (W.y - Wc.y));
         }
         b[m] = n1;
@@ -414,6 +424,133 @@ __global__ void __launch_bounds__(256) k_rk_update(Fields F, Geo g, const double
 }
 
 // ---------------------------------------------------------------------------
+// Direct-I/O tile kernels for the z and y passes (pdfft::fft_tile_io): one field
+// per CTA, 8 interleaved lines, the first radix pass reading its butterfly
+// inputs straight from HBM and the last pass writing its outputs straight to
+// HBM, so a 256-point line crosses shared memory once (one block barrier).
+// ---------------------------------------------------------------------------
+template <int N> struct TCfg {
+    static constexpr int NT = pdfft::tile_threads<N>();
+    static constexpr int MINB = NT <= 128 ? 4 : (NT <= 256 ? 2 : 1);
+    static constexpr size_t SMEM = sizeof(double2) * (size_t)N * L;
+};
+
+// K1: field f = blockIdx.x (0..2 velocity, 3..5 vorticity), lines i0..i0+7 at one j.
+// The six CTAs of a tile are adjacent in launch order, so the three that read a
+// velocity component run together and two of the three reads hit L2.
+template <int NZ>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zinv_io(Fields F, Geo g, int stage) {
+    extern __shared__ double2 s[];
+    const int f = blockIdx.x, i0 = blockIdx.y * L, j = blockIdx.z;
+    if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
+    const int KK = g.kk, NKK = g.nkk, nki = g.nki;
+    const double k2 = wvn(j, g.kj);
+    const long long istride = (long long)g.nkj * NKK;
+    const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
+    // velocity: u_f; vorticity f: i (ka a - kb b) with a, b, ka, kb as in field_value
+    const double2* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
+    const double2* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
+    BF bf;
+    if (g.shear && f >= 3) bf = make_bf(g, F.clock);
+    auto ld = [&](int z, int l) -> double2 {
+        const int i = i0 + l;
+        int k;
+        if (z <= KK) k = z;
+        else if (z >= NZ - KK) k = z - NZ + NKK;
+        else return mk(0.0, 0.0);
+        if (i >= nki) return mk(0.0, 0.0);
+        const long long m = row0 + l * istride + k;
+        if (f < 3) return pa[m];
+        const double k1 = (double)i, k3 = wvn(k, KK);
+        if (g.shear) {   // BF-rot vorticity (f_RK3VorticityBFRot)
+            const double kv[3] = {k1, k2, k3};
+            const double2 uv[3] = {F.u[0][m], F.u[1][m], F.u[2][m]};
+            double2 w3[3];
+            vort_bf(bf, uv, kv, w3);
+            return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
+        }
+        const double ka = (f == 3) ? k2 : ((f == 4) ? k3 : k1);
+        const double kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2);
+        const double2 a = pa[m], b = pb[m];
+        return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
+    };
+    double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+    const long long zs = (long long)g.nkj * g.nkip;
+    auto st = [&](int z, int l, double2 v) { dst[z * zs + l] = v; };
+    pdfft::fft_tile_io<NZ, +1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+}
+
+// K2: backward y transforms of field f = blockIdx.z, j zero-padded into [KJ+1, NY-KJ-1].
+template <int NY>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yinv_io(Fields F, Geo g) {
+    extern __shared__ double2 s[];
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const int KJ = g.kj, NKJ = g.nkj;
+    const long long rs = g.nkip;
+    const double2* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
+    double2* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
+    auto ld = [&](int y, int l) -> double2 {
+        if (y <= KJ) return src[y * rs + l];
+        if (y >= NY - KJ) return src[(y - NY + NKJ) * rs + l];
+        return mk(0.0, 0.0);
+    };
+    auto st = [&](int y, int l, double2 v) { dst[y * rs + l] = v; };
+    pdfft::fft_tile_io<NY, +1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+}
+
+// K4: forward y transforms of NL field f = blockIdx.z, truncated to j.
+template <int NY>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yfwd_io(Fields F, Geo g) {
+    extern __shared__ double2 s[];
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const int KJ = g.kj, NKJ = g.nkj;
+    const long long rs = g.nkip;
+    const double2* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
+    double2* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
+    auto ld = [&](int y, int l) -> double2 { return src[y * rs + l]; };
+    auto st = [&](int y, int l, double2 v) {
+        if (y <= KJ) dst[y * rs + l] = v;
+        else if (y >= NY - KJ) dst[(y - NY + NKJ) * rs + l] = v;
+    };
+    pdfft::fft_tile_io<NY, -1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+}
+
+// K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
+// to k, stored as rows of NL-hat [c][i][j][k].
+template <int NZ>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zfwd_io(Fields F, Geo g, Out3 nlh) {
+    extern __shared__ double2 s[];
+    const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z;
+    const int KK = g.kk, NKK = g.nkk, nki = g.nki;
+    const long long zs = (long long)g.nkj * g.nkip;
+    const double2* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+    double2* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
+    const long long istride = (long long)g.nkj * NKK;
+    const double norm = g.norm;
+    auto ld = [&](int z, int l) -> double2 { return src[z * zs + l]; };
+    auto st = [&](int z, int l, double2 v) {
+        if (i0 + l >= nki) return;
+        int k;
+        if (z <= KK) k = z;
+        else if (z >= NZ - KK) k = z - NZ + NKK;
+        else return;
+        dst[l * istride + k] = mk(v.x * norm, v.y * norm);
+    };
+    pdfft::fft_tile_io<NZ, -1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+}
+
+// The direct-I/O kernels are the default; PANDORA_TILE_IO=0 selects the
+// warp-per-line tile kernels above.
+static bool tile_io() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("PANDORA_TILE_IO");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
 template <int N> static size_t tw_words() { return tw_smem<N>() ? (size_t)N : 0; }
@@ -424,7 +561,7 @@ template <int N> static size_t smem_ky() {
     return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
 }
 template <int N> static size_t smem_kx() {
-    return sizeof(double2) * ((size_t)Cfg<N>::NWX * tile_rows<N, PS>() * 3 + tw_words<N>());
+    return sizeof(double2) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
 }
 template <int N> static size_t smem_k5() {
     return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
@@ -440,10 +577,14 @@ cudaError_t configure_kernels(const Geo& g) {
     if (g.nz == N) {                                                                  \
         if ((e = set_smem(k_zpass_inv<N>, smem_k1<N>()))) return e;                   \
         if ((e = set_smem(k_zpass_fwd<N>, smem_k5<N>()))) return e;                   \
+        if ((e = set_smem(k_zinv_io<N>, TCfg<N>::SMEM))) return e;                    \
+        if ((e = set_smem(k_zfwd_io<N>, TCfg<N>::SMEM))) return e;                    \
     }                                                                                 \
     if (g.ny == N) {                                                                  \
         if ((e = set_smem(k_ypass_inv<N>, smem_ky<N>()))) return e;                   \
         if ((e = set_smem(k_ypass_fwd<N>, smem_ky<N>()))) return e;                   \
+        if ((e = set_smem(k_yinv_io<N>, TCfg<N>::SMEM))) return e;                    \
+        if ((e = set_smem(k_yfwd_io<N>, TCfg<N>::SMEM))) return e;                    \
     }                                                                                 \
     if (g.nx == N) {                                                                  \
         if ((e = set_smem(k_xpass<N>, smem_kx<N>()))) return e;                       \
@@ -457,7 +598,10 @@ cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStrea
     switch (g.nz) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        k_zpass_inv<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k1<N>(), st>>>(f, g, stage); \
+        if (tile_io())                                                                \
+            k_zinv_io<N><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
+        else                                                                          \
+            k_zpass_inv<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k1<N>(), st>>>(f, g, stage); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -470,7 +614,10 @@ cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), NT, smem_ky<N>(), st>>>(f, g);    \
+        if (tile_io())                                                                \
+            k_yinv_io<N><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
+        else                                                                          \
+            k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), NT, smem_ky<N>(), st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -499,7 +646,10 @@ cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), NT, smem_ky<N>(), st>>>(f, g);    \
+        if (tile_io())                                                                \
+            k_yfwd_io<N><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
+        else                                                                          \
+            k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), NT, smem_ky<N>(), st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -514,7 +664,10 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, in
     switch (g.nz) {
 #define PD_L(N)                                                                             \
     case N:                                                                                 \
-        k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k5<N>(), st>>>(f, g, nlh);       \
+        if (tile_io())                                                                      \
+            k_zfwd_io<N><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, nlh); \
+        else                                                                                \
+            k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k5<N>(), st>>>(f, g, nlh);   \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L

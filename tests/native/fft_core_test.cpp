@@ -10,15 +10,54 @@
 
 using namespace pdfft;
 
-template <int N, int R, int NS, int S, int L, int LP, int PS = 0>
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0>
 static void emu_pass(std::vector<double2>& s, const std::vector<double2>& tw) {
     constexpr int WORK = (N / R) * L;
     std::vector<double2> v((size_t)WORK * R);
-    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP, PS>(s.data(), tw.data(), w, &v[(size_t)w * R]);
-    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP, PS>(s.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP, PS, AS>(s.data(), tw.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP, PS, AS>(s.data(), w, &v[(size_t)w * R]);
 }
 
-template <int N, int S, int L, int LP, bool WARP>
+// Two lines in separate arrays AS elements apart, transformed in lockstep with the
+// low-pass warp plan and pad interval PS (the x-pass layout).
+template <int N, int S, int PS>
+static double check_pair() {
+    constexpr int AS = (N + (N >> PS) + 7) / 8 * 8 + 4;
+    constexpr int R0 = WPlanL<N>::r0, R1 = WPlanL<N>::r1, R2 = WPlanL<N>::r2;
+    std::vector<double2> tw(N);
+    for (int e = 0; e < N; e++) {
+        long double a = 6.283185307179586476925286766559005768L * e / N;
+        tw[e] = mk((double)cosl(a), -(double)sinl(a));
+    }
+    std::vector<double2> s((size_t)2 * AS), x((size_t)2 * N);
+    srand(N * 11 + S + 5);
+    for (int l = 0; l < 2; l++)
+        for (int n = 0; n < N; n++) {
+            double2 v = mk(rand() / (double)RAND_MAX - 0.5, rand() / (double)RAND_MAX - 0.5);
+            x[(size_t)l * N + n] = v;
+            s[(size_t)l * AS + prow<PS>(n)] = v;
+        }
+    emu_pass<N, R0, 1, S, 2, 1, PS, AS>(s, tw);
+    if constexpr (R1 != 0) emu_pass<N, R1, R0, S, 2, 1, PS, AS>(s, tw);
+    if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, 2, 1, PS, AS>(s, tw);
+    double err = 0, mag = 0;
+    for (int l = 0; l < 2; l++)
+        for (int k = 0; k < N; k++) {
+            long double re = 0, im = 0;
+            for (int n = 0; n < N; n++) {
+                long double a = S * 6.283185307179586476925286766559005768L * (long double)((long)k * n % N) / N;
+                double2 v = x[(size_t)l * N + n];
+                re += v.x * cosl(a) - v.y * sinl(a);
+                im += v.x * sinl(a) + v.y * cosl(a);
+            }
+            double2 g = s[(size_t)l * AS + prow<PS>(k)];
+            err = fmax(err, fabs((double)(g.x - re)) + fabs((double)(g.y - im)));
+            mag = fmax(mag, fabs((double)re) + fabs((double)im));
+        }
+    return err / mag;
+}
+
+template <int N, int S, int L, int LP, bool WARP, bool LOWPASS = false, bool DIRECT = false>
 static double check() {
     static_assert(plan_ok<N>(), "plan");
     std::vector<double2> tw(N);
@@ -36,7 +75,9 @@ static double check() {
         }
     if constexpr (WARP) {
         // warp plan, one line per warp: every line is column l of the tile (offset l, L = 1)
-        constexpr int R0 = WPlan<N>::r0, R1 = WPlan<N>::r1, R2 = WPlan<N>::r2;
+        constexpr int R0 = LOWPASS ? WPlanL<N>::r0 : WPlan<N>::r0;
+        constexpr int R1 = LOWPASS ? WPlanL<N>::r1 : WPlan<N>::r1;
+        constexpr int R2 = LOWPASS ? WPlanL<N>::r2 : WPlan<N>::r2;
         // padded rows (PS = 3) as the kernels use them
         for (int l = 0; l < L; l++) {
             std::vector<double2> col((size_t)tile_rows<N, 3>() * LP);
@@ -45,6 +86,21 @@ static double check() {
             if constexpr (R1 != 0) emu_pass<N, R1, R0, S, 1, LP, 3>(col, tw);
             if constexpr (R2 != 0) emu_pass<N, R2, R0 * R1, S, 1, LP, 3>(col, tw);
             for (int n = 0; n < N; n++) s[(size_t)n * LP + l] = col[(size_t)prow<3>(n) * LP];
+        }
+    } else if constexpr (DIRECT) {
+        // direct tile transform: first pass from x, last pass into the tile s, lines
+        // interleaved in a scratch tile of pitch L (one CTA emulated pass by pass)
+        constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+        std::vector<double2> t((size_t)N * L);
+        auto ld = [&](int n, int l) { return x[(size_t)l * N + n]; };
+        auto st = [&](int n, int l, double2 v) { s[(size_t)n * LP + l] = v; };
+        if constexpr (R1 == 0) {
+            for (int l = 0; l < L; l++) pass_only<N, S, L>(l, ld, st);
+        } else {
+            for (int w = 0; w < (N / R0) * L; w++) pass_first<N, R0, S, L>(t.data(), w, ld);
+            if constexpr (R2 != 0) emu_pass<N, R1, R0, S, L, L>(t, tw);
+            constexpr int RL = R2 ? R2 : R1;
+            for (int w = 0; w < (N / RL) * L; w++) pass_last<N, RL, S, L>(t.data(), tw.data(), w, st);
         }
     } else {
         constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
@@ -90,6 +146,29 @@ int main() {
     RUN(448); RUN(512); RUN(640); RUN(768); RUN(896); RUN(1024);
     RUNW(16); RUNW(24); RUNW(32); RUNW(48); RUNW(64); RUNW(96); RUNW(128); RUNW(192); RUNW(256);
     RUNW(384); RUNW(512); RUNW(768); RUNW(1024);
+#define RUNL(N)                                                                             \
+    do {                                                                                    \
+        double e1 = check<N, -1, 2, 3, true, true>(), e2 = check<N, +1, 2, 3, true, true>();   \
+        printf("warp low-pass N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                       \
+        if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                             \
+    } while (0)
+    RUNL(48); RUNL(128); RUNL(256); RUNL(512);
+#define RUND(N)                                                                                      \
+    do {                                                                                             \
+        double e1 = check<N, -1, 8, 9, false, false, true>(), e2 = check<N, +1, 8, 9, false, false, true>(); \
+        printf("direct tile N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                                 \
+        if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                                      \
+    } while (0)
+    RUND(16); RUND(24); RUND(32); RUND(48); RUND(64); RUND(96); RUND(128); RUND(192); RUND(256);
+    RUND(384); RUND(512); RUND(768); RUND(1024);
+#define RUNP(N, PS)                                                          \
+    do {                                                                     \
+        double e1 = check_pair<N, -1, PS>(), e2 = check_pair<N, +1, PS>();   \
+        printf("pair N=%4d PS=%d fwd %.2e bwd %.2e\n", N, PS, e1, e2);      \
+        if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                              \
+    } while (0)
+    RUNP(16, 2); RUNP(24, 3); RUNP(32, 2); RUNP(48, 4); RUNP(64, 3); RUNP(96, 4); RUNP(128, 4);
+    RUNP(192, 3); RUNP(256, 4);
     printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }
