@@ -393,16 +393,6 @@ __device__ __forceinline__ void pass(double2* s, const double2* __restrict__ tw,
     __syncthreads();
 }
 
-// Full length-N transform of L lines of the tile (caller syncs before).
-template <int N, int S, int L, int LP, int NT>
-__device__ __forceinline__ void fft_tile(double2* s, const double2* __restrict__ tw, int tid) {
-    static_assert(plan_ok<N>(), "no radix plan for this length");
-    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
-    pass<N, R0, 1, S, L, LP, NT>(s, tw, tid);
-    if constexpr (R1 != 0) pass<N, R1, R0, S, L, LP, NT>(s, tw, tid);
-    if constexpr (R2 != 0) pass<N, R2, R0 * R1, S, L, LP, NT>(s, tw, tid);
-}
-
 // Direct tile transform of L interleaved lines by NT threads (see pass_first).
 // The caller makes `s` free before the call (a barrier after any earlier use);
 // on return other threads may still read `s`.

@@ -114,7 +114,7 @@ __device__ int normal_pair(uint64_t key, uint64_t call, double& r1, double& r2) 
 
 __global__ void __launch_bounds__(256) k_stage_scalars(Fields F, Geo g, StepParams sp, ForceParams fp,
                                                        int stage) {
-    extern __shared__ double nrm[];   // [2 * calls]
+    extern __shared__ double nrm[];   // [2 * calls] normal pairs, then the i = 0 plane [3][FW][FW]
     Clock* ck = F.clock;
     const int tid = threadIdx.x;
     if (stage == 1 && tid == 0) {
@@ -157,41 +157,58 @@ __global__ void __launch_bounds__(256) k_stage_scalars(Fields F, Geo g, StepPara
     }
     if (bad) atomicOr(&ck->status, PD_ST_POLAR);
     __syncthreads();
-    if (tid != 0) return;
     const double dt_over_TF = ck->dt / fp.tf;
     const double amp = sqrt(2.0 * (fp.sigma * fp.sigma) * dt_over_TF);
     const double decay = 1.0 - dt_over_TF;
-    long long c = 0;
     double2* ff = F.forcing;
-    auto at = [&](int comp, int i, int jw, int kw) -> double2& {
-        return ff[comp * fstride + ((long long)i * FW + (jw + NK)) * FW + (kw + NK)];
-    };
-    auto ou = [&](int i, int jw, int kw) {
+    const int plane = FW * FW;
+    // Modes i >= 1 take normal pairs c0 + 3q.. in the order i, jw, kw (all from -NK):
+    // independent of each other, updated in parallel.
+    const long long c0 = 3LL * (NK + 1) * (2 * NK + 1);
+    for (int q = tid; q < NK * plane; q += blockDim.x) {
+        const long long m = (long long)plane + q;   // (i*FW + jw+NK)*FW + kw+NK with i >= 1
+        const long long c = c0 + 3LL * q;
+#pragma unroll
         for (int comp = 0; comp < 3; comp++) {
-            double2& v = at(comp, i, jw, kw);
-            const double re = nrm[2 * (c + comp)], im = nrm[2 * (c + comp) + 1];
-            v = mk(v.x * decay + re * amp, v.y * decay + im * amp);
+            double2& v = ff[comp * fstride + m];
+            v = mk(v.x * decay + nrm[2 * (c + comp)] * amp, v.y * decay + nrm[2 * (c + comp) + 1] * amp);
         }
-        c += 3;
-    };
-    auto conj_copy = [&](int jd, int kd, int js, int ks) {
-        for (int comp = 0; comp < 3; comp++) {
-            const double2 sv = at(comp, 0, js, ks);
-            at(comp, 0, jd, kd) = mk(sv.x, -sv.y);
-        }
-    };
-    for (int jw = 0; jw <= NK; jw++)
-        for (int kw = 0; kw <= NK; kw++) {
-            ou(0, jw, kw);
-            conj_copy(-jw, -kw, jw, kw);
-            if (jw > 0) {
-                ou(0, -jw, kw);
-                conj_copy(jw, -kw, -jw, kw);
+    }
+    // The i = 0 plane: the OU update of the half jw >= 0 (and jw < 0 for kw >= 0)
+    // interleaved with conjugate copies that later steps overwrite again, so it
+    // runs in its original order, on a shared-memory copy of the plane.
+    double2* pl = (double2*)(nrm + 2 * calls);   // [3][FW][FW]
+    for (int q = tid; q < 3 * plane; q += blockDim.x) pl[q] = ff[(q / plane) * fstride + q % plane];
+    __syncthreads();
+    if (tid == 0) {
+        long long c = 0;
+        auto at = [&](int comp, int jw, int kw) -> double2& { return pl[comp * plane + (jw + NK) * FW + (kw + NK)]; };
+        auto ou = [&](int jw, int kw) {
+            for (int comp = 0; comp < 3; comp++) {
+                double2& v = at(comp, jw, kw);
+                const double re = nrm[2 * (c + comp)], im = nrm[2 * (c + comp) + 1];
+                v = mk(v.x * decay + re * amp, v.y * decay + im * amp);
             }
-        }
-    for (int i = 1; i <= NK; i++)
-        for (int jw = -NK; jw <= NK; jw++)
-            for (int kw = -NK; kw <= NK; kw++) ou(i, jw, kw);
+            c += 3;
+        };
+        auto conj_copy = [&](int jd, int kd, int js, int ks) {
+            for (int comp = 0; comp < 3; comp++) {
+                const double2 sv = at(comp, js, ks);
+                at(comp, jd, kd) = mk(sv.x, -sv.y);
+            }
+        };
+        for (int jw = 0; jw <= NK; jw++)
+            for (int kw = 0; kw <= NK; kw++) {
+                ou(jw, kw);
+                conj_copy(-jw, -kw, jw, kw);
+                if (jw > 0) {
+                    ou(-jw, kw);
+                    conj_copy(jw, -kw, -jw, kw);
+                }
+            }
+    }
+    __syncthreads();
+    for (int q = tid; q < 3 * plane; q += blockDim.x) ff[(q / plane) * fstride + q % plane] = pl[q];
 }
 
 // simtime after stage s: t0 + {1/3, 3/4, 1} dt (src/pg_rk3.f90:109-127); the step
@@ -414,10 +431,21 @@ cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// Shared memory of k_stage_scalars: the normal pairs of one stage, then the i = 0
+// forcing plane (about 132 KB at the largest forcing radius, FORCE_KF = 8).
+static size_t stage_scalars_smem(const Geo& g, const ForceParams& fp) {
+    const int fw = 2 * g.fnk + 1;
+    return sizeof(double) * 2 * (size_t)fp.calls_per_stage + sizeof(double2) * 3 * (size_t)fw * fw;
+}
+
+cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp) {
+    return cudaFuncSetAttribute(k_stage_scalars, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)stage_scalars_smem(g, fp));
+}
+
 cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams& sp, const ForceParams& fp,
                                  int stage, cudaStream_t st) {
-    const size_t sm = sizeof(double) * 2 * (size_t)fp.calls_per_stage;
-    k_stage_scalars<<<1, 256, sm, st>>>(f, g, sp, fp, stage);
+    k_stage_scalars<<<1, 256, stage_scalars_smem(g, fp), st>>>(f, g, sp, fp, stage);
     return cudaGetLastError();
 }
 

@@ -21,24 +21,42 @@ namespace pd {
 
 constexpr int kMaxOrder = 6;
 
+// Lagrange basis weight m at x over the ORD nodes: prod_{n != m} (x - x_n) / (x_m - x_n),
+// formed as one quotient of the two products (one FP64 division per weight).
 template <int ORD>
-__device__ __forceinline__ void lagrange_weights(double x, const double* nodes, double* w) {
+__device__ __forceinline__ double lagrange_weight(double x, const double* nodes, int m) {
+    double xm = nodes[0];
 #pragma unroll
-    for (int m = 0; m < ORD; m++) {
-        double v = 1.0;
+    for (int n = 1; n < ORD; n++)
+        if (n == m) xm = nodes[n];   // m may be a run-time value: select, do not index
+    double num = 1.0, den = 1.0;
 #pragma unroll
-        for (int n = 0; n < ORD; n++)
-            if (n != m) v *= (x - nodes[n]) / (nodes[m] - nodes[n]);
-        w[m] = v;
-    }
+    for (int n = 0; n < ORD; n++)
+        if (n != m) { num *= x - nodes[n]; den *= xm - nodes[n]; }
+    return num / den;
 }
+
+// G threads per particle (G = the power of two at or above ORD): thread `sub` of a
+// group gathers the stencil column x = i0 + sub (threads sub >= ORD add nothing),
+// so one warp load touches 32/G particles' rows of consecutive values instead of
+// 32 scattered rows; the group sums its partial results with shuffles and its
+// first thread does the update.
+template <int ORD> constexpr int part_group() { return ORD <= 1 ? 1 : (ORD <= 2 ? 2 : (ORD <= 4 ? 4 : 8)); }
 
 template <int ORD>
 __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const double* __restrict__ phys,
                                                    Clock* ck, PartParams pp, int stage) {
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int G = part_group<ORD>();
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = t / G;
+    const int sub = (int)(t % G);
     const int tstep = ck->tstep;
-    if (n >= P.np || tstep < pp.release) return;
+    if (tstep < pp.release) return;                     // uniform over the launch
+    if (G == 1 && n >= P.np) return;
+    // With G > 1 every lane of a warp reaches the shuffles: lanes past the last
+    // particle (whole groups at the tail) gather for the last particle and store nothing.
+    const bool valid = n < P.np;
+    const long long nn = valid ? n : P.np - 1;
     const double dt = ck->dt;
     double beta, gamma;
     if (stage == 1) { beta = 0.0; gamma = 1.0 / 3.0; }
@@ -50,7 +68,7 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
     double xp[3], up[3], ur[3], pr[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        xp[c] = P.xp[c][n]; up[c] = P.up[c][n]; ur[c] = P.uprk[c][n]; pr[c] = P.prk[c][n];
+        xp[c] = P.xp[c][nn]; up[c] = P.up[c][nn]; ur[c] = P.uprk[c][nn]; pr[c] = P.prk[c][nn];
     }
     // p_InterpFindMolecule: stencil start from the same rounded arithmetic
     double w[3][ORD];
@@ -73,32 +91,69 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
             int q = (i0 + m) % NN[c];
             idx[c][m] = q < 0 ? q + NN[c] : q;
         }
-        lagrange_weights<ORD>(xp[c], nodes, w[c]);
-    }
-    long long rowoff[ORD][ORD];
+        if constexpr (G == 1) {
 #pragma unroll
-    for (int zi = 0; zi < ORD; zi++)
+            for (int m = 0; m < ORD; m++) w[c][m] = lagrange_weight<ORD>(xp[c], nodes, m);
+        } else {
+            // each thread of the group forms the weight of its own offset; the
+            // group exchanges them (lanes of a group are consecutive)
+            const double mine = lagrange_weight<ORD>(xp[c], nodes, sub < ORD ? sub : ORD - 1);
+            const int base = (threadIdx.x & 31) & ~(G - 1);
 #pragma unroll
-        for (int yi = 0; yi < ORD; yi++) rowoff[zi][yi] = ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx;
-    double uf[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const double* f = phys + (long long)c * g.R;
-        double acc_z = 0.0;
-#pragma unroll
-        for (int zi = 0; zi < ORD; zi++) {
-            double acc_y = 0.0;
-#pragma unroll
-            for (int yi = 0; yi < ORD; yi++) {
-                const double* row = f + rowoff[zi][yi];
-                double acc_x = 0.0;
-#pragma unroll
-                for (int xi = 0; xi < ORD; xi++) acc_x += w[0][xi] * __ldg(row + idx[0][xi]);
-                acc_y += w[1][yi] * acc_x;
-            }
-            acc_z += w[2][zi] * acc_y;
+            for (int m = 0; m < ORD; m++) w[c][m] = __shfl_sync(0xffffffffu, mine, base + m);
         }
-        uf[c] = acc_z;
+    }
+    double uf[3];
+    if constexpr (G == 1) {
+        long long rowoff[ORD][ORD];
+#pragma unroll
+        for (int zi = 0; zi < ORD; zi++)
+#pragma unroll
+            for (int yi = 0; yi < ORD; yi++) rowoff[zi][yi] = ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double* f = phys + (long long)c * g.R;
+            double acc_z = 0.0;
+#pragma unroll
+            for (int zi = 0; zi < ORD; zi++) {
+                double acc_y = 0.0;
+#pragma unroll
+                for (int yi = 0; yi < ORD; yi++) {
+                    const double* row = f + rowoff[zi][yi];
+                    double acc_x = 0.0;
+#pragma unroll
+                    for (int xi = 0; xi < ORD; xi++) acc_x += w[0][xi] * __ldg(row + idx[0][xi]);
+                    acc_y += w[1][yi] * acc_x;
+                }
+                acc_z += w[2][zi] * acc_y;
+            }
+            uf[c] = acc_z;
+        }
+    } else {
+        // column x = idx[0][sub]; the x weights are applied before the group sum
+        int xs = idx[0][0];
+        double wx = (sub == 0) ? w[0][0] : 0.0;
+#pragma unroll
+        for (int xi = 1; xi < ORD; xi++)
+            if (sub == xi) { xs = idx[0][xi]; wx = w[0][xi]; }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const double* f = phys + (long long)c * g.R + xs;
+            double acc_z = 0.0;
+#pragma unroll
+            for (int zi = 0; zi < ORD; zi++) {
+                double acc_y = 0.0;
+#pragma unroll
+                for (int yi = 0; yi < ORD; yi++)
+                    acc_y += w[1][yi] * __ldg(f + ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx);
+                acc_z += w[2][zi] * acc_y;
+            }
+            double v = wx * acc_z;
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            uf[c] = v;
+        }
+        if (sub != 0 || !valid) return;
     }
     double xw[3] = {xp[0], xp[1], xp[2]};   // frame in which the RK3 update runs
     if (g.shear) {
@@ -276,9 +331,12 @@ __global__ void k_part_scatter(Particles src, PartSort s) {
 cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp, int stage,
                              cudaStream_t st) {
     if (p.np == 0) return cudaSuccess;
-    const unsigned nb = (unsigned)((p.np + 255) / 256);
     switch (pp.order) {
-#define PD_ORD(O) case O: k_particles<O><<<nb, 256, 0, st>>>(p, g, f.phys, f.clock, pp, stage); break;
+#define PD_ORD(O)                                                                                  \
+    case O:                                                                                        \
+        k_particles<O><<<(unsigned)((p.np * part_group<O>() + 255) / 256), 256, 0, st>>>(p, g, f.phys, \
+                                                                                       f.clock, pp, stage); \
+        break;
         PD_ORD(1) PD_ORD(2) PD_ORD(3) PD_ORD(4) PD_ORD(5) PD_ORD(6)
 #undef PD_ORD
     default: return cudaErrorInvalidValue;

@@ -10,15 +10,14 @@
 //   K4 ypass_fwd   yb fields 0..2      -> 3 forward y FFTs, truncate j       -> zb fields 0..2
 //   K5 zpass_fwd   zb fields 0..2      -> 3 forward z FFTs, x 1/(NX NY NZ), truncate k, then the
 //                                         per-mode RHS + low-storage RK3 + continuity fix on u, rk
-// Every pass reads and writes HBM once, in coalesced rows.  A CTA of 8 warps
-// works on a tile of 8 lines: the tile moves between HBM and shared memory with
-// all 256 threads (rows of 8 consecutive i = 128 bytes), and in between each
-// warp transforms its own line with warp-synchronous Stockham passes, so a tile
-// costs two block barriers whatever the transform length.  The x pass owns
-// whole lines per warp and needs no block barrier at all.
+// Every pass reads and writes HBM once.  The z and y passes (K1, K2, K4, K5a)
+// are tile transforms of 8 lines interleaved in shared memory (pdfft::fft_tile_io):
+// the first radix pass loads its butterfly inputs straight from HBM (rows of 8
+// consecutive i = 128 bytes) and the last pass stores straight to HBM, so a
+// two-pass length crosses shared memory once, behind one block barrier.  The x
+// pass owns whole lines per warp and needs no block barrier at all.
 #include <cuda_runtime.h>
 #include <math.h>
-#include <stdlib.h>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
@@ -30,36 +29,14 @@ using pdfft::mk;
 using pdfft::prow;
 using pdfft::tile_rows;
 
-constexpr int PS = 3;             // one pad row per 8 rows of a tile (pdfft::prow)
+constexpr int L = 8;              // lines per tile of the z and y passes (one 128-byte row)
+constexpr int NT = 256;           // threads per CTA of the x pass (8 warps, one line each)
 
-constexpr int NW = 8;             // warps per CTA
-constexpr int NT = 32 * NW;       // threads per CTA
-constexpr int L = NW;             // lines per tile, one per warp
-constexpr int LP = L + 1;         // padded row of the tile (odd: conflict-free transposes)
-
-// K1 double-buffers its tile where shared memory allows; K3 holds three
-// complex arrays per warp, so long lines get fewer warps per CTA.
+// K3 holds three complex arrays per warp, so long lines get fewer warps per CTA.
 template <int N> struct Cfg {
-    // resident CTAs per SM asked of the register allocator (64 registers at 4)
-    static constexpr int MINB = (N <= 256) ? 4 : ((N <= 512) ? 2 : 1);
-    static constexpr int NB1 = (N <= 256) ? 1 : ((N <= 512) ? 2 : 1);
     static constexpr int NWX = (N <= 512) ? 8 : 4;
     static constexpr int MINBX = (N <= 256) ? 2 : 1;   // K3 CTAs per SM (shared memory allows 2 up to 256)
 };
-
-// Twiddle table staged in shared memory (after the tiles) where it fits; the
-// per-item twiddle reads of a pass then hit shared memory instead of L1.
-template <int N> constexpr bool tw_smem() { return false; }   // measured slower: shared memory is the busier unit
-template <int N>
-__device__ __forceinline__ const double2* stage_twiddles(double2* dst, const double2* __restrict__ src) {
-    if constexpr (!tw_smem<N>()) {
-        return src;
-    } else {
-        for (int q = threadIdx.x; q < N; q += blockDim.x) dst[q] = src[q];
-        __syncthreads();
-        return dst;
-    }
-}
 
 #define PD_FOR_EACH_N(X) \
     X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
@@ -72,133 +49,6 @@ bool supported_length(int n) {
         return true;
     default:
         return false;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// K1: spectral velocity and vorticity, backward z transforms.
-// CTA = (i tile of 8 lines, one j); warp w owns line i = i0 + w.  Field f:
-// 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
-// f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
-// f_RK3Derivative 3735-3743).  k is zero-padded into [KK+1, NZ-KK-1] as
-// src/pf_rk3.f90:437-443.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 field_value(const double2* const* u, long long m, int f, double k1,
-                                               double k2, double k3) {
-    if (f < 3) return u[f][m];
-    double2 a, b;
-    double ka, kb;
-    // omega1 = (0 - dv/dz) + dw/dy ; omega2 = du/dz - dw/dx ; omega3 = (-du/dy) + dv/dx
-    if (f == 3) { a = u[2][m]; ka = k2; b = u[1][m]; kb = k3; }
-    else if (f == 4) { a = u[0][m]; ka = k3; b = u[2][m]; kb = k1; }
-    else { a = u[1][m]; ka = k1; b = u[0][m]; kb = k2; }
-    // i*ka*a - i*kb*b, with i*k*v = (-k v.y, k v.x)
-    return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
-}
-
-template <int NZ>
-__global__ void __launch_bounds__(NT, Cfg<NZ>::MINB) k_zpass_inv(Fields F, Geo g, int stage) {
-    constexpr int NB = Cfg<NZ>::NB1;
-    extern __shared__ double2 smem[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i0 = blockIdx.x * L, j = blockIdx.y;
-    const int i = i0 + w;
-    if (stage == 1 && blockIdx.x == 0 && j == 0 && tid == 0) F.clock->ucfl_bits = 0ull;
-    const double2* tw = stage_twiddles<NZ>(smem + NB * (tile_rows<NZ, PS>() * LP), F.tw_z);
-    const double k2 = wvn(j, g.kj);
-    const int KK = g.kk, NKK = g.nkk;
-    const double2* u[3] = {F.u[0], F.u[1], F.u[2]};
-    const long long row = ((long long)i * g.nkj + j) * NKK;
-    BF bf;
-    if (g.shear) bf = make_bf(g, F.clock);
-    for (int f = 0; f < 6; f++) {
-        double2* s = smem + (f % NB) * (tile_rows<NZ, PS>() * LP);
-        if (NB == 1 && f > 0) __syncthreads();           // previous store has read the tile
-        double2* col = s + w;
-        for (int k = lane; k < NKK; k += 32) {
-            const int z = (k <= KK) ? k : NZ - NKK + k;
-            double2 v = mk(0.0, 0.0);
-            if (i < g.nki) {
-                if (g.shear && f >= 3) {   // BF-rot vorticity (f_RK3VorticityBFRot)
-                    const double kv[3] = {(double)i, k2, wvn(k, KK)};
-                    const double2 uv[3] = {u[0][row + k], u[1][row + k], u[2][row + k]};
-                    double2 w3[3];
-                    vort_bf(bf, uv, kv, w3);
-                    v = w3[f - 3];
-                } else {
-                    v = field_value(u, row + k, f, (double)i, k2, wvn(k, KK));
-                }
-            }
-            col[prow<PS>(z) * LP] = v;
-        }
-        for (int z = KK + 1 + lane; z < NZ - KK; z += 32) col[prow<PS>(z) * LP] = mk(0.0, 0.0);
-        __syncwarp();
-        fft_warp<NZ, +1, LP, PS>(col, tw, lane);
-        __syncthreads();
-        double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
-        const long long zs = (long long)g.nkj * g.nkip;
-        for (int q = tid; q < NZ * L; q += NT) {
-            const int l = q % L, z = q / L;
-            dst[z * zs + l] = s[prow<PS>(z) * LP + l];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// K2: backward y transforms, j padded into [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs,
-// src/pf_rk3.f90:1458-1473).  CTA = (i tile, z, field).
-// ---------------------------------------------------------------------------
-template <int NY>
-__global__ void __launch_bounds__(NT, Cfg<NY>::MINB) k_ypass_inv(Fields F, Geo g) {
-    extern __shared__ double2 s[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
-    const int KJ = g.kj, NKJ = g.nkj, npad = NY - NKJ;
-    const double2* tw = stage_twiddles<NY>(s + tile_rows<NY, PS>() * LP, F.tw_y);
-    const double2* src = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
-    for (int q = tid; q < NKJ * L; q += NT) {
-        const int l = q % L, jj = q / L;
-        const int y = (jj <= KJ) ? jj : NY - NKJ + jj;
-        s[prow<PS>(y) * LP + l] = src[(long long)jj * g.nkip + l];
-    }
-    for (int q = tid; q < npad * L; q += NT) {
-        const int l = q % L, y = KJ + 1 + q / L;
-        s[prow<PS>(y) * LP + l] = mk(0.0, 0.0);
-    }
-    __syncthreads();
-    fft_warp<NY, +1, LP, PS>(s + w, tw, lane);
-    __syncthreads();
-    double2* dst = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
-    for (int q = tid; q < NY * L; q += NT) {
-        const int l = q % L, y = q / L;
-        dst[(long long)y * g.nkip + l] = s[prow<PS>(y) * LP + l];
-    }
-}
-
-// ---------------------------------------------------------------------------
-// K4: forward y transforms of the three NL fields, truncate j
-// (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
-// ---------------------------------------------------------------------------
-template <int NY>
-__global__ void __launch_bounds__(NT, Cfg<NY>::MINB) k_ypass_fwd(Fields F, Geo g) {
-    extern __shared__ double2 s[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
-    const double2* tw = stage_twiddles<NY>(s + tile_rows<NY, PS>() * LP, F.tw_y);
-    const double2* src = F.yb + (((long long)f * g.nz + z) * NY) * g.nkip + i0;
-    for (int q = tid; q < NY * L; q += NT) {
-        const int l = q % L, y = q / L;
-        s[prow<PS>(y) * LP + l] = src[(long long)y * g.nkip + l];
-    }
-    __syncthreads();
-    fft_warp<NY, -1, LP, PS>(s + w, tw, lane);
-    __syncthreads();
-    const int KJ = g.kj, NKJ = g.nkj;
-    double2* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * g.nkip + i0;
-    for (int q = tid; q < NKJ * L; q += NT) {
-        const int l = q % L, jj = q / L;
-        const int y = (jj <= KJ) ? jj : NY - NKJ + jj;
-        dst[(long long)jj * g.nkip + l] = s[prow<PS>(y) * LP + l];
     }
 }
 
@@ -323,44 +173,15 @@ __device__ __forceinline__ void rk_coeffs(int stage, double& beta, double& gamma
     else { beta = -(153.0 / 128.0); gamma = 8.0 / 15.0; }
 }
 
-// K5a: CTA = (i tile, j); the three NL fields in turn: tile load, barrier, warp
-// w transforms line i = i0 + w and stores its truncated, normalised values as a
-// contiguous k row of NL-hat [c][i][j][k] (coalesced per warp).
 struct Out3 { double2* p[3]; };
-
-template <int NZ>
-__global__ void __launch_bounds__(NT, Cfg<NZ>::MINB) k_zpass_fwd(Fields F, Geo g, Out3 nlh) {
-    extern __shared__ double2 s[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int i0 = blockIdx.x * L, j = blockIdx.y;
-    const int i = i0 + w;
-    const int KK = g.kk, NKK = g.nkk;
-    const long long zs = (long long)g.nkj * g.nkip;
-    const double2* tw = stage_twiddles<NZ>(s + tile_rows<NZ, PS>() * LP, F.tw_z);
-    for (int f = 0; f < 3; f++) {
-        if (f > 0) __syncthreads();                         // warps are done with the previous tile
-        const double2* src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
-        for (int q = tid; q < NZ * L; q += NT) {
-            const int l = q % L, z = q / L;
-            s[prow<PS>(z) * LP + l] = src[z * zs + l];
-        }
-        __syncthreads();
-        fft_warp<NZ, -1, LP, PS>(s + w, tw, lane);
-        if (i < g.nki) {
-            double2* dst = nlh.p[f] + ((long long)i * g.nkj + j) * NKK;
-            for (int k = lane; k < NKK; k += 32) {
-                const int z = (k <= KK) ? k : NZ - NKK + k;
-                const double2 v = s[prow<PS>(z) * LP + w];
-                dst[k] = mk(v.x * g.norm, v.y * g.norm);
-            }
-        }
-    }
-}
 
 // K5b: per mode f_RK3FormFIsotropic / f_RK3FormFBFRot + f_RK3RungeKutta +
 // f_RK3ContinuityFixIsotropic (src/pf_rk3.f90:2323-2673, 3457-3531), one thread
 // per mode, streaming NL-hat, u and rk.
-__global__ void __launch_bounds__(256) k_rk_update(Fields F, Geo g, const double2* __restrict__ nlh, int stage) {
+// Separate instantiations for the isotropic (with forcing) and the BF-rot right-hand
+// side: 3 and 4 CTAs of 256 threads per SM, without spills.
+template <bool SHEAR>
+__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(Fields F, Geo g, const double2* __restrict__ nlh, int stage) {
     const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= g.S) return;
     const int NKK = g.nkk;
@@ -377,7 +198,7 @@ __global__ void __launch_bounds__(256) k_rk_update(Fields F, Geo g, const double
     double2 nl[3], uu[3], tot[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) { nl[c] = nlh[c * g.S + m]; uu[c] = F.u[c][m]; }
-    if (g.shear) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
+    if constexpr (SHEAR) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
         const BF bf = make_bf(g, F.clock);
         rhs_bf(bf, g.nu, kv, uu, nl, tot);
     } else {
@@ -424,22 +245,26 @@ __global__ void __launch_bounds__(256) k_rk_update(Fields F, Geo g, const double
 }
 
 // ---------------------------------------------------------------------------
-// Direct-I/O tile kernels for the z and y passes (pdfft::fft_tile_io): one field
+// z and y passes: direct-I/O tile transforms (pdfft::fft_tile_io), one field
 // per CTA, 8 interleaved lines, the first radix pass reading its butterfly
 // inputs straight from HBM and the last pass writing its outputs straight to
 // HBM, so a 256-point line crosses shared memory once (one block barrier).
 // ---------------------------------------------------------------------------
 template <int N> struct TCfg {
     static constexpr int NT = pdfft::tile_threads<N>();
-    static constexpr int MINB = NT <= 128 ? 4 : (NT <= 256 ? 2 : 1);
+    static constexpr int MINB = NT <= 128 ? 5 : (NT <= 256 ? 2 : 1);
     static constexpr size_t SMEM = sizeof(double2) * (size_t)N * L;
 };
 
-// K1: field f = blockIdx.x (0..2 velocity, 3..5 vorticity), lines i0..i0+7 at one j.
-// The six CTAs of a tile are adjacent in launch order, so the three that read a
-// velocity component run together and two of the three reads hit L2.
-template <int NZ>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zinv_io(Fields F, Geo g, int stage) {
+// K1: spectral velocity and vorticity, backward z transforms.  Field f =
+// blockIdx.x: 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
+// f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
+// f_RK3Derivative 3735-3743), or the BF-rot vorticity; lines i0..i0+7 at one j;
+// k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
+// of a tile are adjacent in launch order, so the three that read a velocity
+// component run together and two of the three reads hit L2.
+template <int NZ, bool SHEAR>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zpass_inv(Fields F, Geo g, int stage) {
     extern __shared__ double2 s[];
     const int f = blockIdx.x, i0 = blockIdx.y * L, j = blockIdx.z;
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
@@ -447,11 +272,14 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zinv_io(Fields
     const double k2 = wvn(j, g.kj);
     const long long istride = (long long)g.nkj * NKK;
     const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
-    // velocity: u_f; vorticity f: i (ka a - kb b) with a, b, ka, kb as in field_value
+    // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
+    // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1)
     const double2* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
     const double2* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
     BF bf;
-    if (g.shear && f >= 3) bf = make_bf(g, F.clock);
+    if constexpr (SHEAR) {
+        if (f >= 3) bf = make_bf(g, F.clock);
+    }
     auto ld = [&](int z, int l) -> double2 {
         const int i = i0 + l;
         int k;
@@ -462,17 +290,18 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zinv_io(Fields
         const long long m = row0 + l * istride + k;
         if (f < 3) return pa[m];
         const double k1 = (double)i, k3 = wvn(k, KK);
-        if (g.shear) {   // BF-rot vorticity (f_RK3VorticityBFRot)
+        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot)
             const double kv[3] = {k1, k2, k3};
             const double2 uv[3] = {F.u[0][m], F.u[1][m], F.u[2][m]};
             double2 w3[3];
             vort_bf(bf, uv, kv, w3);
             return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
+        } else {
+            const double ka = (f == 3) ? k2 : ((f == 4) ? k3 : k1);
+            const double kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2);
+            const double2 a = pa[m], b = pb[m];
+            return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
         }
-        const double ka = (f == 3) ? k2 : ((f == 4) ? k3 : k1);
-        const double kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2);
-        const double2 a = pa[m], b = pb[m];
-        return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
     };
     double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
     const long long zs = (long long)g.nkj * g.nkip;
@@ -480,9 +309,10 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zinv_io(Fields
     pdfft::fft_tile_io<NZ, +1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
 }
 
-// K2: backward y transforms of field f = blockIdx.z, j zero-padded into [KJ+1, NY-KJ-1].
+// K2: backward y transforms of field f = blockIdx.z, j zero-padded into
+// [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).
 template <int NY>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yinv_io(Fields F, Geo g) {
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_ypass_inv(Fields F, Geo g) {
     extern __shared__ double2 s[];
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
     const int KJ = g.kj, NKJ = g.nkj;
@@ -498,9 +328,10 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yinv_io(Fields
     pdfft::fft_tile_io<NY, +1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
 }
 
-// K4: forward y transforms of NL field f = blockIdx.z, truncated to j.
+// K4: forward y transforms of NL field f = blockIdx.z, truncated to j
+// (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
 template <int NY>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yfwd_io(Fields F, Geo g) {
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_ypass_fwd(Fields F, Geo g) {
     extern __shared__ double2 s[];
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
     const int KJ = g.kj, NKJ = g.nkj;
@@ -518,7 +349,7 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_yfwd_io(Fields
 // K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
 // to k, stored as rows of NL-hat [c][i][j][k].
 template <int NZ>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zfwd_io(Fields F, Geo g, Out3 nlh) {
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zpass_fwd(Fields F, Geo g, Out3 nlh) {
     extern __shared__ double2 s[];
     const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
@@ -539,32 +370,11 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zfwd_io(Fields
     pdfft::fft_tile_io<NZ, -1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
 }
 
-// The direct-I/O kernels are the default; PANDORA_TILE_IO=0 selects the
-// warp-per-line tile kernels above.
-static bool tile_io() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("PANDORA_TILE_IO");
-        v = (e && e[0] == '0') ? 0 : 1;
-    }
-    return v == 1;
-}
-
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-template <int N> static size_t tw_words() { return tw_smem<N>() ? (size_t)N : 0; }
-template <int N> static size_t smem_k1() {
-    return sizeof(double2) * ((size_t)Cfg<N>::NB1 * tile_rows<N, PS>() * LP + tw_words<N>());
-}
-template <int N> static size_t smem_ky() {
-    return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
-}
 template <int N> static size_t smem_kx() {
     return sizeof(double2) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
-}
-template <int N> static size_t smem_k5() {
-    return sizeof(double2) * ((size_t)tile_rows<N, PS>() * LP + tw_words<N>());
 }
 
 template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
@@ -575,16 +385,13 @@ cudaError_t configure_kernels(const Geo& g) {
     cudaError_t e = cudaSuccess;
 #define PD_CFG(N)                                                                     \
     if (g.nz == N) {                                                                  \
-        if ((e = set_smem(k_zpass_inv<N>, smem_k1<N>()))) return e;                   \
-        if ((e = set_smem(k_zpass_fwd<N>, smem_k5<N>()))) return e;                   \
-        if ((e = set_smem(k_zinv_io<N>, TCfg<N>::SMEM))) return e;                    \
-        if ((e = set_smem(k_zfwd_io<N>, TCfg<N>::SMEM))) return e;                    \
+        if ((e = set_smem(k_zpass_inv<N, false>, TCfg<N>::SMEM))) return e;             \
+        if ((e = set_smem(k_zpass_inv<N, true>, TCfg<N>::SMEM))) return e;              \
+        if ((e = set_smem(k_zpass_fwd<N>, TCfg<N>::SMEM))) return e;                    \
     }                                                                                 \
     if (g.ny == N) {                                                                  \
-        if ((e = set_smem(k_ypass_inv<N>, smem_ky<N>()))) return e;                   \
-        if ((e = set_smem(k_ypass_fwd<N>, smem_ky<N>()))) return e;                   \
-        if ((e = set_smem(k_yinv_io<N>, TCfg<N>::SMEM))) return e;                    \
-        if ((e = set_smem(k_yfwd_io<N>, TCfg<N>::SMEM))) return e;                    \
+        if ((e = set_smem(k_ypass_inv<N>, TCfg<N>::SMEM))) return e;                    \
+        if ((e = set_smem(k_ypass_fwd<N>, TCfg<N>::SMEM))) return e;                    \
     }                                                                                 \
     if (g.nx == N) {                                                                  \
         if ((e = set_smem(k_xpass<N>, smem_kx<N>()))) return e;                       \
@@ -598,10 +405,10 @@ cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStrea
     switch (g.nz) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        if (tile_io())                                                                \
-            k_zinv_io<N><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
+        if (g.shear)                                                                  \
+            k_zpass_inv<N, true><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
         else                                                                          \
-            k_zpass_inv<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k1<N>(), st>>>(f, g, stage); \
+            k_zpass_inv<N, false><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -614,10 +421,7 @@ cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        if (tile_io())                                                                \
-            k_yinv_io<N><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
-        else                                                                          \
-            k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), NT, smem_ky<N>(), st>>>(f, g); \
+        k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -646,10 +450,7 @@ cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                       \
     case N:                                                                           \
-        if (tile_io())                                                                \
-            k_yfwd_io<N><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
-        else                                                                          \
-            k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), NT, smem_ky<N>(), st>>>(f, g); \
+        k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -664,10 +465,7 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, in
     switch (g.nz) {
 #define PD_L(N)                                                                             \
     case N:                                                                                 \
-        if (tile_io())                                                                      \
-            k_zfwd_io<N><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, nlh); \
-        else                                                                                \
-            k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj), NT, smem_k5<N>(), st>>>(f, g, nlh);   \
+        k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, nlh); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -675,7 +473,8 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, in
     }
     cudaError_t e = cudaGetLastError();
     if (e || mode == 1) return e;
-    k_rk_update<<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
+    if (g.shear) k_rk_update<true><<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
+    else k_rk_update<false><<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
     return cudaGetLastError();
 }
 

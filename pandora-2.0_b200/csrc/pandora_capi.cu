@@ -22,6 +22,8 @@ struct pandora_handle {
     int dev = 0;
     cudaStream_t own = nullptr;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;      // particle branch of a stage (forked from st, joined back)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     Fields F{};
     double2* fbuf = nullptr;          // u[3], rk[3] contiguous
     double2* tw = nullptr;            // tw_x | tw_y | tw_z
@@ -148,6 +150,9 @@ static void release(pandora_handle* h) {
     cudaFree(h->sort.key); cudaFree(h->sort.count); cudaFree(h->sort.block_sums);
     if (h->clock_host) cudaFreeHost(h->clock_host);
     if (h->shell_host) cudaFreeHost(h->shell_host);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->own) cudaStreamDestroy(h->own);
     delete h;
 }
@@ -233,7 +238,10 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
         cudaMallocHost((void**)&h->shell_host, sizeof(double) * nsh) != cudaSuccess) {
         cudaGetLastError(); release(h); return PANDORA_ERR_OOM;
     }
-    if ((e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking)) != cudaSuccess) {
+    if ((e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming)) != cudaSuccess) {
         release(h); return cuda_fail(e, "cudaStreamCreate");
     }
     h->st = h->own;
@@ -286,6 +294,9 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     h->pp.order = p->p_interp_order; h->pp.release = p->p_ts_release; h->pp.f_nu = p->f_nu;
     h->pp.p_rho = p->p_rho; h->pp.f_rho = p->f_rho;
     if ((e = configure_kernels(g)) != cudaSuccess) { release(h); return cuda_fail(e, "configure_kernels"); }
+    if ((e = configure_fluid_kernels(g, h->fp)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "configure_fluid_kernels");
+    }
     // zero state (the reference zero-initialises its Vecs and rk3 registers)
     if ((e = cudaMemsetAsync(h->fbuf, 0, sizeof(double2) * 6 * (size_t)g.S, h->st)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st)) != cudaSuccess ||
@@ -483,6 +494,12 @@ extern "C" int pandora_init_particles(pandora_handle* h) {
 // f_RK3Stage{s} (src/pf_rk3.f90:40-200): [s=1: statistics of the state],
 // vorticity + z pass, y pass, x pass with NL (and CFL / physical velocity),
 // dt + forcing, particles, forward y, forward z + RK update, time advance.
+// One stage.  With particles the stage forks a second stream: at stage 1 the
+// spatial sort of the particles runs beside the statistics and the first three
+// passes, and every stage's particle advance (which needs the physical velocity
+// of K3 and the stage's dt) runs beside K4 and K5; the branch joins the main
+// stream before the stage clock advances.  Captured into the step graph, the
+// fork and join become graph edges.
 static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     const Geo& g = h->g;
     int n = 0;
@@ -491,7 +508,9 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
         PD_CK(launch_remesh(g, h->F, h->P, h->st)); n += part ? 2 : 1;
     }
     if (stage == 1 && part) {
-        PD_CK(launch_particle_sort(g, h->P, h->sort, h->st, &n));
+        PD_CK(cudaEventRecord(h->ev_fork, h->st));
+        PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        PD_CK(launch_particle_sort(g, h->P, h->sort, h->side, &n));
     }
     if (stage == 1) {
         Fields Fs = h->F;
@@ -502,9 +521,15 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
     PD_CK(launch_ypass_inv(g, h->F, h->st)); n++;
     PD_CK(launch_xpass(g, h->F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
     PD_CK(launch_stage_scalars(g, h->F, h->sp, h->fp, stage, h->st)); n++;
-    if (part) { PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->st)); n++; }
+    if (part) {
+        PD_CK(cudaEventRecord(h->ev_fork, h->st));
+        PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->side)); n++;
+        PD_CK(cudaEventRecord(h->ev_join, h->side));
+    }
     PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
     PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
+    if (part) PD_CK(cudaStreamWaitEvent(h->st, h->ev_join, 0));
     PD_CK(launch_advance_time(g, h->F, stage, h->st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;

@@ -160,5 +160,6 @@ size_t shell_words(const Geo& g);
 
 // Shared-memory configuration (set once per process per device).
 cudaError_t configure_kernels(const Geo& g);
+cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp);
 
 }  // namespace pd

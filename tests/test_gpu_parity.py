@@ -133,6 +133,23 @@ def test_forced_parity(gpu_lib):
     s.close()
 
 
+def test_forced_parity_wide_band(gpu_lib):
+    """Forcing radius 6.5 (3315 normal pairs per stage, 61 KB of shared memory in the
+    stage-scalar kernel, above the 48 KB launch default): forcing and u after 3 steps."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_track_part = 0
+    p.force_kf = 6.5
+    p.force_sigma = 0.01
+    o, s = _pair(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 4):
+        t, _ = o.step(step, t)
+        s.step(step)
+    assert rel_l2_fields(s.get_forcing(), o.get_forcing()) < 1e-13
+    assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10
+    s.close()
+
+
 def test_particle_parity(gpu_lib):
     """Tracers: positions within 1e-10 after 10 steps (same initial positions)."""
     p = gpu_lib.workload_params("iso_forced_particles", 32)
@@ -170,6 +187,30 @@ def test_particle_init_matches_oracle(gpu_lib):
     assert np.abs(xg - xo).max() < 1e-14
     dx = 2 * np.pi / 32
     assert xg.min() >= -dx / 2 and xg.max() < 2 * np.pi - dx / 2
+
+
+@pytest.mark.parametrize("order", [1, 2, 3, 5, 6])
+def test_particle_parity_orders(gpu_lib, order):
+    """Interpolation orders other than 4 (p_InterpInterpolate3D takes 1..6), 1001 tracers
+    (a partial thread group and a partial CTA at the tail): positions after 3 steps."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 1001
+    p.p_interp_order = order
+    o, s = _pair(gpu_lib, p)
+    s.init_particles()
+    xp, up, ur, pr, dp = s.get_particles()
+    o.set_particles(xp, up, ur, pr, dp)
+    t = 0.0
+    for step in range(1, 4):
+        t, _ = o.step(step, t)
+        s.step(step)
+    xg = s.get_particles()[0]
+    xo = o.get_particles(p.p_np_global)[0]
+    d = np.abs(xg - xo)
+    d = np.minimum(d, 2 * np.pi - d)
+    assert d.max() < 1e-10, d.max()
+    s.check_status()
+    s.close()
 
 
 def test_inertial_particles(gpu_lib):
