@@ -22,14 +22,16 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "pandora-2.0_b200"))
 
 METRIC = "Mpts·RK3steps/s"
 WORKLOAD = "iso_forced_particles"
 # per-launch DRAM traffic (read + write) of the dominant pass, from the ncu capture
-# summarised in profiles/ (None until captured for this workload)
-NCU_TRAFFIC_BYTES = {}
+# summarised in profiles/xpass_iso_forced_particles_256_dram.md (None where not captured)
+NCU_TRAFFIC_BYTES = {(256, "xpass_nl"): 553721856 + 620178432}
 
 
 def _args():
@@ -251,8 +253,15 @@ def run_ours(a, p):
     sim.set_stream(stream.cuda_stream)
     npts = p.nodes_x * p.nodes_y * p.nodes_z
 
-    # warm-up (builds the CUDA graph of one step)
+    # warm-up with event pairs around every pass inside the step graph, to find the
+    # dominant pass; the timed region then carries the pair around that pass only
+    # (6 event nodes per step), whose durations in the last timed step give the roofline
+    sim.set_pass_timing(0x3F)
     sim.advance(max(a.warmup, 3), sync=True)
+    warm = sim.pass_times()
+    dom_pid = int(np.argmax([warm[1:, q].mean() for q in range(6)])) + 1
+    sim.set_pass_timing(1 << (dom_pid - 1))
+    sim.advance(3, sync=True)
     sim.check_status()
 
     # ---- device-resident timing ----
@@ -269,6 +278,7 @@ def run_ours(a, p):
     torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
+    live = sim.pass_times()          # [stage][pass] ms of the last timed step
     sim.check_status()
 
     # ---- end to end through the C-ABI: one synchronous g_RK3Calc call per step
@@ -286,10 +296,19 @@ def run_ours(a, p):
     sampler.stop()
     clocks = sampler.summary()
 
-    # ---- roofline of the dominant pass, timed alone with CUDA events ----
+    # ---- roofline of the dominant pass: its launches in the last timed step
+    # (CUDA event pairs recorded inside the step graph, stages 2 and 3, whose
+    # traffic pass_bytes counts); each pass also timed alone for reference ----
     peak, peak_kind = _peaks()
     passes = {1: "zpass_inv", 2: "ypass_inv", 3: "xpass_nl", 4: "ypass_fwd", 5: "zpass_fwd_update",
               6: "particles"}
+    per_pass_live = {}
+    for pid, name in passes.items():
+        v = live[1:, pid - 1] if pid == dom_pid else warm[1:, pid - 1]
+        if (v > 0).all():
+            b = sim.pass_bytes(pid)
+            d = float(v.mean()) / 1e3
+            per_pass_live[name] = {"ms": d * 1e3, "gbs": b / d / 1e9}
     per_pass = {}
     reps = 20
     for pid, name in passes.items():
@@ -305,12 +324,18 @@ def run_ours(a, p):
         dur = q0.elapsed_time(q1) / reps / 1e3
         b = sim.pass_bytes(pid)
         per_pass[name] = {"ms": dur * 1e3, "gbs": b / dur / 1e9, "bytes": b}
-    dom = max(per_pass, key=lambda k: per_pass[k]["ms"])
-    dom_gbs = per_pass[dom]["gbs"]
+    src = per_pass_live if per_pass_live else per_pass
+    dom = max(src, key=lambda k: src[k]["ms"])
+    dom_gbs = src[dom]["gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": dom_gbs, "peak": peak, "unit": "GB/s",
                 "frac": dom_gbs / peak, "peak_kind": f"{peak_kind} (burst copy)",
+                "timed": ("dominant pass: event pair in the step graph, stages 2-3 of the last timed step; "
+                          "other passes: the same in the last warm-up step") if per_pass_live
+                         else "alone, 20 back-to-back launches",
                 "traffic": NCU_TRAFFIC_BYTES.get((a.n, dom)),
-                "per_pass": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)} for k, v in per_pass.items()}}
+                "per_pass": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)} for k, v in src.items()},
+                "per_pass_alone": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)}
+                                   for k, v in per_pass.items()}}
     launches = sim.launches_per_step()
     value = npts * a.steps * ws / (ms / 1e3) / 1e6
     e2e_value = npts * n_e2e * ws / e2e_s / 1e6

@@ -222,6 +222,15 @@ int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps);
  * output written once, at the stored, unpadded extents). */
 int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes);
 
+/* Instrumentation (no counterpart in the reference): every step records a CUDA
+ * event pair around each pass p whose bit p-1 is set in `passes` (passes 1..6 as
+ * in pandora_profile_pass; pass 6 on the particle stream), in each stage, inside
+ * the step graph; passes = 0 turns it off.  pandora_pass_times waits for the
+ * handle's stream and writes the durations of the most recent step,
+ * ms[(stage-1)*6 + pass-1] in milliseconds (-1 where a pass was not timed). */
+int pandora_set_pass_timing(pandora_handle* h, int32_t passes);
+int pandora_pass_times(pandora_handle* h, float* ms);
+
 /*
  * No counterpart in the reference.  The nonlinear term omega x u of a spectral
  * velocity field (the output of pandora_nonlinear), for callers that may not

@@ -24,6 +24,9 @@ struct pandora_handle {
     cudaStream_t st = nullptr;
     cudaStream_t side = nullptr;      // particle branch of a stage (forked from st, joined back)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int timing = 0;                   // pandora_set_pass_timing: bit p-1 times pass p
+    bool timed[3][6] = {};
+    cudaEvent_t tev[3][6][2] = {};
     Fields F{};
     double2* fbuf = nullptr;          // u[3], rk[3] contiguous
     double2* tw = nullptr;            // tw_x | tw_y | tw_z
@@ -150,6 +153,10 @@ static void release(pandora_handle* h) {
     cudaFree(h->sort.key); cudaFree(h->sort.count); cudaFree(h->sort.block_sums);
     if (h->clock_host) cudaFreeHost(h->clock_host);
     if (h->shell_host) cudaFreeHost(h->shell_host);
+    for (auto& st3 : h->tev)
+        for (auto& pr : st3)
+            for (cudaEvent_t e : pr)
+                if (e) cudaEventDestroy(e);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->side) cudaStreamDestroy(h->side);
@@ -517,18 +524,38 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
         Fs.shell = h->shell_step;
         PD_CK(launch_stats(g, Fs, h->st)); n += 1;   // one kernel (plus a memset node)
     }
+    // instrumentation: event pair around pass `ps` (1..6) when pass timing is on
+    auto mark = [&](int ps, int end, cudaStream_t s) -> cudaError_t {
+        if (!(h->timing & (1 << (ps - 1)))) return cudaSuccess;
+        h->timed[stage - 1][ps - 1] = true;
+        // External: captured as an event record node (a plain record inside a capture
+        // only orders the streams and never fires the event)
+        return cudaEventRecordWithFlags(h->tev[stage - 1][ps - 1][end], s, cudaEventRecordExternal);
+    };
+    PD_CK(mark(1, 0, h->st));
     PD_CK(launch_zpass_inv(g, h->F, stage, h->st)); n++;
+    PD_CK(mark(1, 1, h->st));
+    PD_CK(mark(2, 0, h->st));
     PD_CK(launch_ypass_inv(g, h->F, h->st)); n++;
+    PD_CK(mark(2, 1, h->st));
+    PD_CK(mark(3, 0, h->st));
     PD_CK(launch_xpass(g, h->F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
+    PD_CK(mark(3, 1, h->st));
     PD_CK(launch_stage_scalars(g, h->F, h->sp, h->fp, stage, h->st)); n++;
     if (part) {
         PD_CK(cudaEventRecord(h->ev_fork, h->st));
         PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        PD_CK(mark(6, 0, h->side));
         PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->side)); n++;
+        PD_CK(mark(6, 1, h->side));
         PD_CK(cudaEventRecord(h->ev_join, h->side));
     }
+    PD_CK(mark(4, 0, h->st));
     PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
+    PD_CK(mark(4, 1, h->st));
+    PD_CK(mark(5, 0, h->st));
     PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
+    PD_CK(mark(5, 1, h->st));
     if (part) PD_CK(cudaStreamWaitEvent(h->st, h->ev_join, 0));
     PD_CK(launch_advance_time(g, h->F, stage, h->st)); n++;
     if (nlaunch) *nlaunch += n;
@@ -734,6 +761,35 @@ extern "C" int pandora_launches_per_step(pandora_handle* h, int32_t* n) {
         h->launches_per_step = 1 + 3 * (8 + (part ? 1 : 0)) + (part ? 5 : 0) + (h->g.shear ? (part ? 2 : 1) : 0);
     }
     *n = h->launches_per_step;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_set_pass_timing(pandora_handle* h, int32_t passes) {
+    if (!h || passes < 0 || passes > 0x3F) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(cudaStreamSynchronize(h->st));
+    if (passes && !h->tev[0][0][0]) {
+        for (auto& st3 : h->tev)
+            for (auto& pr : st3)
+                for (cudaEvent_t& e : pr) PD_CK(cudaEventCreate(&e));
+    }
+    h->timing = passes;
+    for (auto& st3 : h->timed)
+        for (bool& t : st3) t = false;
+    drop_graph(h);   // the next step captures the graph with (or without) the event nodes
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_pass_times(pandora_handle* h, float* ms) {
+    if (!h || !ms) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    PD_CK(cudaStreamSynchronize(h->st));
+    for (int st = 0; st < 3; st++)
+        for (int ps = 0; ps < 6; ps++) {
+            float v = -1.0f;
+            if ((h->timing & (1 << ps)) && h->timed[st][ps]) PD_CK(cudaEventElapsedTime(&v, h->tev[st][ps][0], h->tev[st][ps][1]));
+            ms[st * 6 + ps] = v;
+        }
     return PANDORA_OK;
 }
 

@@ -73,6 +73,8 @@ SIGNATURES = {
     "pandora_launches_per_step": [_vp, ctypes.POINTER(_i32)],
     "pandora_profile_pass": [_vp, _i32, _i32],
     "pandora_pass_bytes": [_vp, _i32, _dp],
+    "pandora_set_pass_timing": [_vp, _i32],
+    "pandora_pass_times": [_vp, ctypes.POINTER(ctypes.c_float)],
     "pandora_frame": [_vp, _dp, _dp],
     "pandora_nonlinear_static": [ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }

@@ -192,6 +192,17 @@ class Simulation:
         _lib.check(self.L.pandora_pass_bytes(self.h, pass_id, ctypes.byref(b)), "pandora_pass_bytes")
         return b.value
 
+    def set_pass_timing(self, passes: int) -> None:
+        """Record a CUDA event pair around the passes in the bitmask (bit p-1 = pass p,
+        0x3F = all six, 0 = off) in every stage of each step."""
+        _lib.check(self.L.pandora_set_pass_timing(self.h, int(passes)), "pandora_set_pass_timing")
+
+    def pass_times(self) -> np.ndarray:
+        """Durations (ms) of the passes of the most recent step, [stage 1..3][pass 1..6]; -1 = not run."""
+        out = (ctypes.c_float * 18)()
+        _lib.check(self.L.pandora_pass_times(self.h, out), "pandora_pass_times")
+        return np.array(out, dtype=np.float64).reshape(3, 6)
+
     def launches_per_step(self) -> int:
         n = ctypes.c_int32()
         _lib.check(self.L.pandora_launches_per_step(self.h, ctypes.byref(n)), "pandora_launches_per_step")

@@ -281,3 +281,33 @@ def test_nan_detection(gpu_lib):
         assert ei.value.status == -4
         s.init_fluid()
         s.check_status()   # status word was cleared and the state is finite again
+
+
+def test_pass_timing_instrumentation(gpu_lib):
+    """Event pairs around every pass: durations for all 3 stages x 6 passes, and the
+    instrumented step computes exactly what the plain step does."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 512
+    a = gpu_lib.Simulation(p)
+    b = gpu_lib.Simulation(p)
+    for s in (a, b):
+        s.init_fluid()
+        s.init_particles()
+    b.set_pass_timing(0x3F)
+    for step in range(1, 3):
+        a.step(step)
+        b.step(step)
+    t = b.pass_times()
+    assert t.shape == (3, 6) and (t > 0).all(), t
+    for x, y in zip(a.get_state(), b.get_state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.get_particles()[0], b.get_particles()[0])
+    b.set_pass_timing(1 << 2)          # the x pass only
+    b.step(3)
+    t = b.pass_times()
+    assert (t[:, 2] > 0).all() and (np.delete(t, 2, axis=1) == -1).all(), t
+    b.set_pass_timing(0)
+    b.step(4)
+    assert (b.pass_times() == -1).all()
+    a.close()
+    b.close()
