@@ -41,8 +41,8 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--np", type=int, default=1 << 20)
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=256)
+    ap.add_argument("--np", "--particles", dest="np", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -60,6 +60,47 @@ def _dist():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+class Ranks:
+    """The replicas' only cross-rank traffic: a barrier around the timed region and the
+    max over ranks of each timing (NCCL on GPUs; gloo with device "cpu" in the tests)."""
+
+    def __init__(self, backend: str = "nccl", device: str = "cuda", timeout_s: int = 120):
+        self.ws, self.rank, self.local = _dist()
+        self.device = device
+        if self.ws > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+
+    def barrier(self):
+        if self.ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.ws == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+def replica_seeds(p, rank: int):
+    """Each replica runs its own member of the ensemble: same workload, own seeds."""
+    p.seed_fluid = 1 + rank
+    p.seed_force = 1000 + rank
+    p.seed_particles = 2000 + rank
+    return p
 
 
 class ClockSampler:
@@ -222,29 +263,12 @@ def run_ours(a, p):
     import pandora
 
     ws, rank, local = _dist()
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
+    torch.cuda.set_device(local if ws > 1 else 0)
+    ranks = Ranks("nccl", "cuda")
     dev = torch.cuda.current_device()
-
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
-    p.seed_fluid = 1 + rank
-    p.seed_force = 1000 + rank
-    p.seed_particles = 2000 + rank
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
+    replica_seeds(p, rank)
     sim = pandora.Simulation(p)
     sim.init_fluid()
     if p.p_track_part:
@@ -364,9 +388,7 @@ def run_ours(a, p):
     sim.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    ranks.close()
     return 0
 
 
