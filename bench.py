@@ -43,15 +43,18 @@ def _args():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--n", "--grid", dest="n", type=int, default=256)
     ap.add_argument("--np", "--particles", dest="np", type=int, default=1 << 20)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed"],
+                    help="fp32_mixed: FP32 fields and transforms, FP64 bookkeeping (our arm only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
-def _params(a):
-    from pandora.params import workload_params
+def _params(a, fp64=False):
+    from pandora.params import PREC_FP32_MIXED, PREC_FP64, workload_params
     p = workload_params(a.workload, a.n)
     if p.p_track_part:
         p.p_np_global = a.np
+    p.precision = PREC_FP32_MIXED if (a.precision == "fp32_mixed" and not fp64) else PREC_FP64
     return p
 
 
@@ -236,9 +239,10 @@ def _config(a, p):
     else:
         phys = f"decaying, nu={p.f_nu}, dt={p.rk3_dt}"
     ws = (6 * 16 * (p.nodes_x // 3 + 8) * p.nodes_y * p.nodes_z) / 1e9
-    return {"workload": f"{a.workload} {p.nodes_x}^3 FP64 plain, {phys}, {npart} tracers (order {p.p_interp_order})",
+    form = "FP32-mixed" if p.precision == 1 else "FP64 plain"
+    return {"workload": f"{a.workload} {p.nodes_x}^3 {form}, {phys}, {npart} tracers (order {p.p_interp_order})",
             "grid": [p.nodes_x, p.nodes_y, p.nodes_z], "nu": p.f_nu,
-            "particles": npart, "form": "fp64_plain",
+            "particles": npart, "form": "fp32_mixed" if p.precision == 1 else "fp64_plain",
             "parallelism": f"replicas x{a.gpus}",
             "l2": f"no flush needed: each pass streams > 126 MB (y-pencil buffer alone {ws:.2f} GB)"}
 
@@ -336,7 +340,7 @@ def run_ours(a, p):
     per_pass = {}
     reps = 20
     for pid, name in passes.items():
-        if pid == 6 and not p.p_track_part:
+        if pid == 6 and not (p.p_track_part and p.p_np_global > 0):
             continue
         sim.profile_pass(pid, 2)
         q0 = torch.cuda.Event(enable_timing=True)
@@ -368,7 +372,8 @@ def run_ours(a, p):
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded Rogallo field, seeded tracers)",
+        "dtype": "f32+f64" if p.precision == 1 else "f64",
+        "data": "synthetic (seeded Rogallo field, seeded tracers)",
         "config": _config(a, p),
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 48, "d2h_bytes_per_step": d2h,
@@ -381,7 +386,7 @@ def run_ours(a, p):
     # complex words; particles add 6 R + 18 Np words per stage; stage-1 stats read 3 S)
     line["step_model_gbs"] = _step_model(p, ms / a.steps, peak)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        v, cores, secs = cpu_baseline(_params(a))
+        v, cores, secs = cpu_baseline(_params(a, fp64=True))
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
                                 "sample": f"one RK3 step (3 stages) of the same workload on the host, "
                                           f"{secs:.1f} s, OpenMP C restatement (oracle/pandora_oracle.c)"}
@@ -394,9 +399,9 @@ def run_ours(a, p):
 
 def main():
     a = _args()
-    p = _params(a)
     if a.impl == "reference":
-        return run_reference(a, p)
+        return run_reference(a, _params(a, fp64=True))
+    p = _params(a)
     return run_ours(a, p)
 
 

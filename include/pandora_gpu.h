@@ -59,6 +59,12 @@ extern "C" {
 #define PANDORA_F_INIT_AHMED_ELGHOBASHI 10
 #define PANDORA_P_INIT_RANDOM        2   /* pg_parameters.f90:236 */
 #define PANDORA_PREC_FP64            0
+/* FP32-mixed form (no counterpart in the reference, which is FP64 throughout): fields,
+ * transforms and the nonlinear term in FP32; twiddles generated in long double, the
+ * clock, the Rogallo frame B(t), the remesh, the forcing coefficients, the per-mode
+ * RHS/RK3 arithmetic, the particles and the E(k)/epsilon shell sums in FP64.  Every
+ * boundary call still takes and returns FP64 arrays. */
+#define PANDORA_PREC_FP32_MIXED      1
 
 /*
  * Namelist fields of ip_file.in that the RK3 step reads (src/pg_control.f90:385-436),
@@ -101,7 +107,7 @@ typedef struct pandora_params {
     double  p_dia_vals;     /* single diameter level (P_DIA_LVLS = 1); 0 => tracers */
     /* random seeds (see above) */
     uint64_t seed_fluid, seed_force, seed_particles;
-    /* arithmetic of the step: PANDORA_PREC_FP64 */
+    /* arithmetic of the step: PANDORA_PREC_FP64 or PANDORA_PREC_FP32_MIXED */
     int32_t precision;
     int32_t reserved[7];
 } pandora_params;
@@ -146,7 +152,8 @@ int pandora_get_rk(pandora_handle* h, double* r1, double* r2, double* r3);
 int pandora_forcing_size(pandora_handle* h, int64_t* ndoubles_per_component);
 int pandora_set_forcing(pandora_handle* h, const double* f1, const double* f2, const double* f3);
 int pandora_get_forcing(pandora_handle* h, double* f1, double* f2, double* f3);
-/* Device pointers of u1..u3 (for zero-copy users; valid until destroy). */
+/* Device pointers of u1..u3 (for zero-copy users; valid until destroy), in the
+ * stored precision: double2 [i][j][k] (FP64 form) or float2 (FP32-mixed form). */
 int pandora_state_device_ptrs(pandora_handle* h, void** u1, void** u2, void** u3);
 
 /* Seeded solenoidal initial field, f_InitialiseFluid (src/pf_initialise.f90:97-512),

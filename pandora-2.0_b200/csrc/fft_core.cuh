@@ -22,53 +22,67 @@
 #else
 #include <cstddef>
 struct double2 { double x, y; };
+struct float2 { float x, y; };
 #define PD_HD inline
 #endif
 
 namespace pdfft {
 
+// Complex values are double2 (the FP64 form) or float2 (the FP32-mixed form);
+// every helper below is generic over the two, the real type following the
+// arguments.  Constants are written in FP64 and rounded once to the real type.
+template <class T> struct cplx;
+template <> struct cplx<double> { using type = double2; };
+template <> struct cplx<float> { using type = float2; };
+template <class C> using real_of = decltype(C{}.x);
+
 PD_HD double2 mk(double x, double y) { double2 r; r.x = x; r.y = y; return r; }
-PD_HD double2 add(double2 a, double2 b) { return mk(a.x + b.x, a.y + b.y); }
-PD_HD double2 sub(double2 a, double2 b) { return mk(a.x - b.x, a.y - b.y); }
-PD_HD double2 scl(double2 a, double s) { return mk(a.x * s, a.y * s); }
-PD_HD double2 cmul(double2 a, double2 b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
-PD_HD double2 cmulc(double2 a, double2 b) { return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }
+PD_HD float2 mk(float x, float y) { float2 r; r.x = x; r.y = y; return r; }
+template <class C> PD_HD C add(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
+template <class C> PD_HD C sub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+template <class C> PD_HD C scl(C a, double s) {
+    const real_of<C> t = (real_of<C>)s;
+    return mk(a.x * t, a.y * t);
+}
+template <class C> PD_HD C cmul(C a, C b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <class C> PD_HD C cmulc(C a, C b) { return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }
 
 // Sign convention: a DFT of sign S computes X_r = sum_q x_q exp(S * 2 pi i q r / R);
 // S = -1 is FFTW_FORWARD, S = +1 is FFTW_BACKWARD.  Twiddle tables hold
 // tw[e] = exp(-2 pi i e / N); a sign-S pass multiplies by tw (S=-1) or conj(tw).
-template <int S> PD_HD double2 twmul(double2 a, double2 w) { return S < 0 ? cmul(a, w) : cmulc(a, w); }
+template <int S, class C> PD_HD C twmul(C a, C w) { return S < 0 ? cmul(a, w) : cmulc(a, w); }
 // a * (S i)
-template <int S> PD_HD double2 mul_si(double2 a) { return S > 0 ? mk(-a.y, a.x) : mk(a.y, -a.x); }
+template <int S, class C> PD_HD C mul_si(C a) { return S > 0 ? mk(-a.y, a.x) : mk(a.y, -a.x); }
 // a * (c + S i s)
-template <int S> PD_HD double2 mul_cs(double2 a, double c, double s) {
-    const double ss = S > 0 ? s : -s;
-    return mk(a.x * c - a.y * ss, a.x * ss + a.y * c);
+template <int S, class C> PD_HD C mul_cs(C a, double c, double s) {
+    using T = real_of<C>;
+    const T cc = (T)c, ss = (T)(S > 0 ? s : -s);
+    return mk(a.x * cc - a.y * ss, a.x * ss + a.y * cc);
 }
 
 constexpr double kSqrtHalf = 0.7071067811865475244008444;
 constexpr double kSin60 = 0.8660254037844386467637232;
 
-template <int S> PD_HD void dft2(double2* v) {
-    double2 a = v[0], b = v[1];
+template <int S, class C> PD_HD void dft2(C* v) {
+    C a = v[0], b = v[1];
     v[0] = add(a, b); v[1] = sub(a, b);
 }
-template <int S> PD_HD void dft3(double2* v) {
-    double2 t = add(v[1], v[2]), d = sub(v[1], v[2]);
-    double2 m = sub(v[0], scl(t, 0.5));
-    double2 e = mul_si<S>(scl(d, kSin60));
+template <int S, class C> PD_HD void dft3(C* v) {
+    C t = add(v[1], v[2]), d = sub(v[1], v[2]);
+    C m = sub(v[0], scl(t, 0.5));
+    C e = mul_si<S>(scl(d, kSin60));
     v[0] = add(v[0], t);
     v[1] = add(m, e);
     v[2] = sub(m, e);
 }
-template <int S> PD_HD void dft4(double2* v) {
-    double2 a0 = add(v[0], v[2]), a1 = sub(v[0], v[2]);
-    double2 b0 = add(v[1], v[3]), b1 = mul_si<S>(sub(v[1], v[3]));
+template <int S, class C> PD_HD void dft4(C* v) {
+    C a0 = add(v[0], v[2]), a1 = sub(v[0], v[2]);
+    C b0 = add(v[1], v[3]), b1 = mul_si<S>(sub(v[1], v[3]));
     v[0] = add(a0, b0); v[2] = sub(a0, b0);
     v[1] = add(a1, b1); v[3] = sub(a1, b1);
 }
-template <int S> PD_HD void dft8(double2* v) {
-    double2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+template <int S, class C> PD_HD void dft8(C* v) {
+    C e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
     dft4<S>(e); dft4<S>(o);
     o[1] = mul_cs<S>(o[1], kSqrtHalf, kSqrtHalf);
     o[2] = mul_si<S>(o[2]);
@@ -76,8 +90,8 @@ template <int S> PD_HD void dft8(double2* v) {
 #pragma unroll
     for (int r = 0; r < 4; r++) { v[r] = add(e[r], o[r]); v[r + 4] = sub(e[r], o[r]); }
 }
-template <int S> PD_HD void dft16(double2* v) {
-    double2 e[8], o[8];
+template <int S, class C> PD_HD void dft16(C* v) {
+    C e[8], o[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) { e[q] = v[2 * q]; o[q] = v[2 * q + 1]; }
     dft8<S>(e); dft8<S>(o);
@@ -114,15 +128,15 @@ template <> struct PrimeTab<7> {
              : m == 5 ? -0.9749279121818236070181317 : -0.7818314824680298087084445;
     }
 };
-template <int R, int S> PD_HD void dft_prime(double2* v) {
-    double2 sum[(R - 1) / 2], dif[(R - 1) / 2];
+template <int R, int S, class C> PD_HD void dft_prime(C* v) {
+    C sum[(R - 1) / 2], dif[(R - 1) / 2];
 #pragma unroll
     for (int q = 1; q <= (R - 1) / 2; q++) { sum[q - 1] = add(v[q], v[R - q]); dif[q - 1] = sub(v[q], v[R - q]); }
-    double2 out[R];
-    double2 x0 = v[0];
+    C out[R];
+    C x0 = v[0];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-        double2 acc = x0;
+        C acc = x0;
 #pragma unroll
         for (int q = 1; q <= (R - 1) / 2; q++) {
             const int m = (q * r) % R;
@@ -135,7 +149,7 @@ template <int R, int S> PD_HD void dft_prime(double2* v) {
     for (int r = 0; r < R; r++) v[r] = out[r];
 }
 
-template <int R, int S> PD_HD void dft(double2* v) {
+template <int R, int S, class C> PD_HD void dft(C* v) {
     if constexpr (R == 2) dft2<S>(v);
     else if constexpr (R == 3) dft3<S>(v);
     else if constexpr (R == 4) dft4<S>(v);
@@ -194,8 +208,8 @@ template <int LP, int PS, int AS> PD_HD int tidx(int n, int l) {
     return AS ? l * AS + prow<PS>(n) : prow<PS>(n) * LP + l;
 }
 
-template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0>
-PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0, class C>
+PD_HD void pass_load(const C* s, const C* tw, int w, C* v) {
     constexpr int NR = N / R;
     const int l = w % L, j = w / L;
 #pragma unroll
@@ -208,8 +222,8 @@ PD_HD void pass_load(const double2* s, const double2* tw, int w, double2* v) {
     }
     dft<R, S>(v);
 }
-template <int N, int R, int NS, int L, int LP, int PS = 0, int AS = 0>
-PD_HD void pass_store(double2* s, int w, const double2* v) {
+template <int N, int R, int NS, int L, int LP, int PS = 0, int AS = 0, class C>
+PD_HD void pass_store(C* s, int w, const C* v) {
     const int l = w % L, j = w / L;
     const int k = j % NS;
     const int d = (j / NS) * NS * R + k;
@@ -226,21 +240,21 @@ PD_HD void pass_store(double2* s, int w, const double2* v) {
 // The first pass takes element n of line l from ld(n, l); the last pass hands
 // output n of line l to st(n, l, value).  A two-pass length costs one shared-memory
 // round trip per element instead of four.
-template <int N, int R, int S, int L, class Ld>
-PD_HD void pass_first(double2* s, int w, Ld& ld) {
+template <int N, int R, int S, int L, class C, class Ld>
+PD_HD void pass_first(C* s, int w, Ld& ld) {
     constexpr int NR = N / R;
     const int l = w % L, j = w / L;
-    double2 v[R];
+    C v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = ld(j + r * NR, l);
     dft<R, S>(v);
 #pragma unroll
     for (int r = 0; r < R; r++) s[(j * R + r) * L + l] = v[r];
 }
-template <int N, int R, int S, int L, class St>
-PD_HD void pass_last(const double2* s, const double2* tw, int w, St& st) {
+template <int N, int R, int S, int L, class C, class St>
+PD_HD void pass_last(const C* s, const C* tw, int w, St& st) {
     constexpr int NS = N / R;
-    double2 v[R];
+    C v[R];
     pass_load<N, R, NS, S, L, L, 0>(s, tw, w, v);
     const int l = w % L, j = w / L;
 #pragma unroll
@@ -249,7 +263,8 @@ PD_HD void pass_last(const double2* s, const double2* tw, int w, St& st) {
 // Single-pass lengths: global to global, no shared memory.
 template <int N, int S, int L, class Ld, class St>
 PD_HD void pass_only(int l, Ld& ld, St& st) {
-    double2 v[N];
+    using C = decltype(ld(0, 0));
+    C v[N];
 #pragma unroll
     for (int r = 0; r < N; r++) v[r] = ld(r, l);
     dft<N, S>(v);
@@ -307,11 +322,11 @@ template <int N> constexpr bool wplanl_ok() {
 #if defined(__CUDACC__)
 // One pass of a single line owned by one warp: the line is column 0 of `s`
 // (element n at s[prow<PS>(n)*LP]); only __syncwarp() separates the halves.
-template <int N, int R, int NS, int S, int LP, int PS>
-__device__ __forceinline__ void wpass(double2* s, const double2* __restrict__ tw, int lane) {
+template <int N, int R, int NS, int S, int LP, int PS, class C>
+__device__ __forceinline__ void wpass(C* s, const C* __restrict__ tw, int lane) {
     constexpr int WORK = N / R;
     constexpr int IT = (WORK + 31) / 32;
-    double2 v[IT][R];
+    C v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
@@ -330,11 +345,11 @@ __device__ __forceinline__ void wpass(double2* s, const double2* __restrict__ tw
 // AS = 0, else separate arrays AS elements apart): each pass has NA times the
 // independent work of a single line, which fills the lanes a radix-16 pass of
 // one line leaves idle.
-template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0>
-__device__ __forceinline__ void wpass_n(double2* s, const double2* __restrict__ tw, int lane) {
+template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0, class C>
+__device__ __forceinline__ void wpass_n(C* s, const C* __restrict__ tw, int lane) {
     constexpr int WORK = (N / R) * NA;
     constexpr int IT = (WORK + 31) / 32;
-    double2 v[IT][R];
+    C v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
@@ -349,8 +364,8 @@ __device__ __forceinline__ void wpass_n(double2* s, const double2* __restrict__ 
     __syncwarp();
 }
 
-template <int N, int S, int LP, int PS, int NA, bool LOWPASS = false, int AS = 0>
-__device__ __forceinline__ void fft_warp_n(double2* s, const double2* __restrict__ tw, int lane) {
+template <int N, int S, int LP, int PS, int NA, bool LOWPASS = false, int AS = 0, class C>
+__device__ __forceinline__ void fft_warp_n(C* s, const C* __restrict__ tw, int lane) {
     static_assert(wplan_ok<N>() && wplanl_ok<N>(), "no warp radix plan for this length");
     constexpr int R0 = LOWPASS ? WPlanL<N>::r0 : WPlan<N>::r0;
     constexpr int R1 = LOWPASS ? WPlanL<N>::r1 : WPlan<N>::r1;
@@ -362,8 +377,8 @@ __device__ __forceinline__ void fft_warp_n(double2* s, const double2* __restrict
 
 // Full length-N transform of the line at column 0 of `s` by the calling warp
 // (the caller makes the line's data visible to the warp before the call).
-template <int N, int S, int LP, int PS, bool LOWPASS = false>
-__device__ __forceinline__ void fft_warp(double2* s, const double2* __restrict__ tw, int lane) {
+template <int N, int S, int LP, int PS, bool LOWPASS = false, class C>
+__device__ __forceinline__ void fft_warp(C* s, const C* __restrict__ tw, int lane) {
     static_assert(wplan_ok<N>() && wplanl_ok<N>(), "no warp radix plan for this length");
     constexpr int R0 = LOWPASS ? WPlanL<N>::r0 : WPlan<N>::r0;
     constexpr int R1 = LOWPASS ? WPlanL<N>::r1 : WPlan<N>::r1;
@@ -374,11 +389,11 @@ __device__ __forceinline__ void fft_warp(double2* s, const double2* __restrict__
 }
 
 // In-place pass over a [N][LP] shared tile with NT threads; items w = tid + it*NT.
-template <int N, int R, int NS, int S, int L, int LP, int NT>
-__device__ __forceinline__ void pass(double2* s, const double2* __restrict__ tw, int tid) {
+template <int N, int R, int NS, int S, int L, int LP, int NT, class C>
+__device__ __forceinline__ void pass(C* s, const C* __restrict__ tw, int tid) {
     constexpr int WORK = (N / R) * L;
     constexpr int IT = (WORK + NT - 1) / NT;
-    double2 v[IT][R];
+    C v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = tid + it * NT;
@@ -396,8 +411,8 @@ __device__ __forceinline__ void pass(double2* s, const double2* __restrict__ tw,
 // Direct tile transform of L interleaved lines by NT threads (see pass_first).
 // The caller makes `s` free before the call (a barrier after any earlier use);
 // on return other threads may still read `s`.
-template <int N, int S, int L, int NT, class Ld, class St>
-__device__ __forceinline__ void fft_tile_io(double2* s, const double2* __restrict__ tw, int tid, Ld& ld, St& st) {
+template <int N, int S, int L, int NT, class C, class Ld, class St>
+__device__ __forceinline__ void fft_tile_io(C* s, const C* __restrict__ tw, int tid, Ld& ld, St& st) {
     static_assert(plan_ok<N>(), "no radix plan for this length");
     constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
     if constexpr (R1 == 0) {

@@ -24,7 +24,8 @@ size_t shell_words(const Geo& g) { return (size_t)3 * (g.kkmax + 1) + 3; }
 // u_lab = B^-1 u (f_FluidstatsFsPrimaryQuantsBFRot, src/pf_fluidstats.f90:1586-1960),
 // with the per-shell mode counts of f_FluidstatsModeDensityBFRot
 // (src/pf_fluidstats.f90:1977-2229), which change with B every step.
-__global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
+template <class T>
+__global__ void __launch_bounds__(256) k_stats(FieldsT<T> F, Geo g) {
     extern __shared__ double sh[];
     const int K = g.kkmax;
     double* se = sh;                // [K+1]
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(256) k_stats(Fields F, Geo g) {
         const long long ij = m / g.nkk;
         const int jj = (int)(ij % g.nkj), i = (int)(ij / g.nkj);
         double kv[3] = {(double)i, wvn(jj, g.kj), wvn(k, g.kk)};
-        double2 uv[3] = {F.u[0][m], F.u[1][m], F.u[2][m]};
+        double2 uv[3] = {to_d(F.u[0][m]), to_d(F.u[1][m]), to_d(F.u[2][m])};
         if (g.shear) {
             double kl[3] = {0.0, 0.0, 0.0};
             double2 ul[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
@@ -112,7 +113,8 @@ __device__ int normal_pair(uint64_t key, uint64_t call, double& r1, double& r2) 
     return 0;
 }
 
-__global__ void __launch_bounds__(256) k_stage_scalars(Fields F, Geo g, StepParams sp, ForceParams fp,
+template <class T>
+__global__ void __launch_bounds__(256) k_stage_scalars(FieldsT<T> F, Geo g, StepParams sp, ForceParams fp,
                                                        int stage) {
     extern __shared__ double nrm[];   // [2 * calls] normal pairs, then the i = 0 plane [3][FW][FW]
     Clock* ck = F.clock;
@@ -213,7 +215,8 @@ __global__ void __launch_bounds__(256) k_stage_scalars(Fields F, Geo g, StepPara
 
 // simtime after stage s: t0 + {1/3, 3/4, 1} dt (src/pg_rk3.f90:109-127); the step
 // counter advances after stage 3.
-__global__ void k_advance_time(Fields F, Geo g, int stage) {
+template <class T>
+__global__ void k_advance_time(FieldsT<T> F, Geo g, int stage) {
     Clock* ck = F.clock;
     if (stage == 1) ck->simtime = ck->t0 + (1.0 / 3.0) * ck->dt;
     else if (stage == 2) ck->simtime = ck->t0 + (3.0 / 4.0) * ck->dt;
@@ -344,7 +347,9 @@ __global__ void k_init_fluid(Fields F, Geo g, InitParams ip) {
 // dropped, BF-rot u1 += u3; the frame jumps from S t = +B110/2 to -B110/2.  The
 // step number is read on the device, so the launch sits in every step's graph
 // and returns at once on the other steps.  One CTA per row, row staged in shared memory.
-__global__ void __launch_bounds__(256) k_remesh(Fields F, Geo g) {
+template <class T>
+__global__ void __launch_bounds__(256) k_remesh(FieldsT<T> F, Geo g) {
+    using C = typename FieldsT<T>::C;
     Clock* ck = F.clock;
     if (!remesh_due(g, ck->tstep)) return;
     extern __shared__ double2 rowbuf[];   // [3][NKK]
@@ -358,15 +363,15 @@ __global__ void __launch_bounds__(256) k_remesh(Fields F, Geo g) {
         int knew = actualk - i;
         if (knew >= -KK) {
             if (knew < 0) knew += nodes;
-            for (int c = 0; c < 3; c++) rowbuf[c * NKK + knew] = F.u[c][ij * NKK + k];
+            for (int c = 0; c < 3; c++) rowbuf[c * NKK + knew] = to_d(F.u[c][ij * NKK + k]);
         }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < NKK; k += blockDim.x) {
         const double2 a = rowbuf[k], b3 = rowbuf[2 * NKK + k];
-        F.u[0][ij * NKK + k] = mk(a.x + b3.x, a.y + b3.y);
-        F.u[1][ij * NKK + k] = rowbuf[NKK + k];
-        F.u[2][ij * NKK + k] = b3;
+        F.u[0][ij * NKK + k] = from_d<C>(mk(a.x + b3.x, a.y + b3.y));
+        F.u[1][ij * NKK + k] = from_d<C>(rowbuf[NKK + k]);
+        F.u[2][ij * NKK + k] = from_d<C>(b3);
     }
     if (ij == 0 && threadIdx.x == 0) {
         const double half_b = (double)g.b110 * 0.5;
@@ -387,19 +392,21 @@ __global__ void k_remesh_particles(Particles P, Geo g, const Clock* ck) {
     P.xp[0][n] = x;
 }
 
-cudaError_t launch_remesh(const Geo& g, const Fields& f, const Particles& p, cudaStream_t st) {
+template <class T>
+cudaError_t launch_remesh(const Geo& g, const FieldsT<T>& f, const Particles& p, cudaStream_t st) {
     if (p.np > 0) k_remesh_particles<<<(unsigned)((p.np + 255) / 256), 256, 0, st>>>(p, g, f.clock);
     k_remesh<<<(unsigned)((long long)g.nki * g.nkj), 256, sizeof(double2) * 3 * g.nkk, st>>>(f, g);
     return cudaGetLastError();
 }
 
 // Non-finite check of the spectral state (sets PD_ST_NAN).
-__global__ void k_check_finite(Fields F, Geo g) {
+template <class T>
+__global__ void k_check_finite(FieldsT<T> F, Geo g) {
     bool bad = false;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.S;
          m += (long long)gridDim.x * blockDim.x) {
         for (int c = 0; c < 3; c++) {
-            const double2 v = F.u[c][m];
+            const double2 v = to_d(F.u[c][m]);
             if (!isfinite(v.x) || !isfinite(v.y)) bad = true;
         }
     }
@@ -420,7 +427,7 @@ static int sm_count() {
     return n;
 }
 
-cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st) {
+template <class T> cudaError_t launch_stats(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
     const size_t nsh = shell_words(g);
     cudaError_t e = cudaMemsetAsync(f.shell, 0, sizeof(double) * nsh, st);
     if (e) return e;
@@ -439,17 +446,20 @@ static size_t stage_scalars_smem(const Geo& g, const ForceParams& fp) {
 }
 
 cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp) {
-    return cudaFuncSetAttribute(k_stage_scalars, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)stage_scalars_smem(g, fp));
+    const int b = (int)stage_scalars_smem(g, fp);
+    cudaError_t e = cudaFuncSetAttribute(k_stage_scalars<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e) return e;
+    return cudaFuncSetAttribute(k_stage_scalars<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
-cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams& sp, const ForceParams& fp,
+template <class T>
+cudaError_t launch_stage_scalars(const Geo& g, const FieldsT<T>& f, const StepParams& sp, const ForceParams& fp,
                                  int stage, cudaStream_t st) {
     k_stage_scalars<<<1, 256, stage_scalars_smem(g, fp), st>>>(f, g, sp, fp, stage);
     return cudaGetLastError();
 }
 
-cudaError_t launch_advance_time(const Geo& g, const Fields& f, int stage, cudaStream_t st) {
+template <class T> cudaError_t launch_advance_time(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st) {
     k_advance_time<<<1, 1, 0, st>>>(f, g, stage);
     return cudaGetLastError();
 }
@@ -464,12 +474,23 @@ cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& i
     return cudaGetLastError();
 }
 
-cudaError_t launch_check_finite(const Geo& g, const Fields& f, cudaStream_t st) {
+template <class T> cudaError_t launch_check_finite(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
     long long nb = (g.S + 255) / 256;
     const long long cap = 4LL * sm_count();
     if (nb > cap) nb = cap;
     k_check_finite<<<(unsigned)nb, 256, 0, st>>>(f, g);
     return cudaGetLastError();
 }
+
+#define PD_INST(T)                                                                                   \
+    template cudaError_t launch_stats<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
+    template cudaError_t launch_stage_scalars<T>(const Geo&, const FieldsT<T>&, const StepParams&,   \
+                                                 const ForceParams&, int, cudaStream_t);            \
+    template cudaError_t launch_advance_time<T>(const Geo&, const FieldsT<T>&, int, cudaStream_t);   \
+    template cudaError_t launch_check_finite<T>(const Geo&, const FieldsT<T>&, cudaStream_t);        \
+    template cudaError_t launch_remesh<T>(const Geo&, const FieldsT<T>&, const Particles&, cudaStream_t);
+PD_INST(double)
+PD_INST(float)
+#undef PD_INST
 
 }  // namespace pd

@@ -43,8 +43,10 @@ __device__ __forceinline__ double lagrange_weight(double x, const double* nodes,
 // first thread does the update.
 template <int ORD> constexpr int part_group() { return ORD <= 1 ? 1 : (ORD <= 2 ? 2 : (ORD <= 4 ? 4 : 8)); }
 
-template <int ORD>
-__global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const double* __restrict__ phys,
+// T: precision of the stored physical velocity (the particle state and its
+// arithmetic are FP64 in both forms).
+template <int ORD, class T>
+__global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const T* __restrict__ phys,
                                                    Clock* ck, PartParams pp, int stage) {
     constexpr int G = part_group<ORD>();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -112,17 +114,17 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
             for (int yi = 0; yi < ORD; yi++) rowoff[zi][yi] = ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const double* f = phys + (long long)c * g.R;
+            const T* f = phys + (long long)c * g.R;
             double acc_z = 0.0;
 #pragma unroll
             for (int zi = 0; zi < ORD; zi++) {
                 double acc_y = 0.0;
 #pragma unroll
                 for (int yi = 0; yi < ORD; yi++) {
-                    const double* row = f + rowoff[zi][yi];
+                    const T* row = f + rowoff[zi][yi];
                     double acc_x = 0.0;
 #pragma unroll
-                    for (int xi = 0; xi < ORD; xi++) acc_x += w[0][xi] * __ldg(row + idx[0][xi]);
+                    for (int xi = 0; xi < ORD; xi++) acc_x += w[0][xi] * (double)__ldg(row + idx[0][xi]);
                     acc_y += w[1][yi] * acc_x;
                 }
                 acc_z += w[2][zi] * acc_y;
@@ -138,14 +140,14 @@ __global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const 
             if (sub == xi) { xs = idx[0][xi]; wx = w[0][xi]; }
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            const double* f = phys + (long long)c * g.R + xs;
+            const T* f = phys + (long long)c * g.R + xs;
             double acc_z = 0.0;
 #pragma unroll
             for (int zi = 0; zi < ORD; zi++) {
                 double acc_y = 0.0;
 #pragma unroll
                 for (int yi = 0; yi < ORD; yi++)
-                    acc_y += w[1][yi] * __ldg(f + ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx);
+                    acc_y += w[1][yi] * (double)__ldg(f + ((long long)idx[2][zi] * g.ny + idx[1][yi]) * g.nx);
                 acc_z += w[2][zi] * acc_y;
             }
             double v = wx * acc_z;
@@ -328,13 +330,14 @@ __global__ void k_part_scatter(Particles src, PartSort s) {
     t.pid[d] = src.pid[n];
 }
 
-cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp, int stage,
+template <class T>
+cudaError_t launch_particles(const Geo& g, const FieldsT<T>& f, const Particles& p, const PartParams& pp, int stage,
                              cudaStream_t st) {
     if (p.np == 0) return cudaSuccess;
     switch (pp.order) {
 #define PD_ORD(O)                                                                                  \
     case O:                                                                                        \
-        k_particles<O><<<(unsigned)((p.np * part_group<O>() + 255) / 256), 256, 0, st>>>(p, g, f.phys, \
+        k_particles<O, T><<<(unsigned)((p.np * part_group<O>() + 255) / 256), 256, 0, st>>>(p, g, f.phys, \
                                                                                        f.clock, pp, stage); \
         break;
         PD_ORD(1) PD_ORD(2) PD_ORD(3) PD_ORD(4) PD_ORD(5) PD_ORD(6)
@@ -373,5 +376,10 @@ cudaError_t launch_particle_sort(const Geo& g, const Particles& P, const PartSor
     if (nlaunch) *nlaunch += 5;
     return e;
 }
+
+template cudaError_t launch_particles<double>(const Geo&, const FieldsT<double>&, const Particles&,
+                                             const PartParams&, int, cudaStream_t);
+template cudaError_t launch_particles<float>(const Geo&, const FieldsT<float>&, const Particles&,
+                                            const PartParams&, int, cudaStream_t);
 
 }  // namespace pd

@@ -29,13 +29,19 @@ using pdfft::mk;
 using pdfft::prow;
 using pdfft::tile_rows;
 
+// Shared memory of every kernel here, viewed as the kernel's complex type.
+extern __shared__ __align__(16) unsigned char pd_smem[];
+template <class C> __device__ __forceinline__ C* smem_as() { return reinterpret_cast<C*>(pd_smem); }
+
 constexpr int L = 8;              // lines per tile of the z and y passes (one 128-byte row)
-constexpr int NT = 256;           // threads per CTA of the x pass (8 warps, one line each)
 
 // K3 holds three complex arrays per warp, so long lines get fewer warps per CTA.
 template <int N> struct Cfg {
     static constexpr int NWX = (N <= 512) ? 8 : 4;
-    static constexpr int MINBX = (N <= 256) ? 2 : 1;   // K3 CTAs per SM (shared memory allows 2 up to 256)
+    // K3 CTAs per SM: shared memory allows 2 FP64 CTAs up to N = 256, FP32 twice that
+    template <class T> static constexpr int minbx() {
+        return sizeof(T) == 8 ? ((N <= 256) ? 2 : 1) : ((N <= 256) ? 3 : (N <= 512 ? 2 : 1));
+    }
 };
 
 #define PD_FOR_EACH_N(X) \
@@ -74,33 +80,36 @@ template <int N> constexpr int xps() {
 template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
 template <int N> constexpr int xna() { return N <= 256 ? 2 : 1; }
 
-template <int NX>
-__global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, int want_phys, int want_cfl) {
+template <int NX, class T>
+__global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(FieldsT<T> F, Geo g,
+                                                                                        int want_phys,
+                                                                                        int want_cfl) {
+    using C = typename FieldsT<T>::C;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
-    extern __shared__ double2 smem[];
+    C* smem = smem_as<C>();
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const long long lines = (long long)g.ny * g.nz;
-    const double2* tw = F.tw_x;
+    const C* tw = F.tw_x;
     const long long q = (long long)blockIdx.x * Cfg<NX>::NWX + w;
     if (q >= lines) return;                       // whole warp; no block barrier follows
-    double2* s = smem + (size_t)w * 3 * XAS;
+    C* s = smem + (size_t)w * 3 * XAS;
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int KI = g.ki, NKI = g.nki;
-    double2* b = F.yb + q * g.nkip;
+    C* b = F.yb + q * g.nkip;
     BF bf;
     if (g.shear) bf = make_bf(g, F.clock);
     for (int m = lane; m < NKI; m += 32) {
 #pragma unroll
         for (int p = 0; p < 3; p++) {
-            double2 X = b[(2 * p) * fstride + m], Y = b[(2 * p + 1) * fstride + m];
-            if (m == 0) { X.y = 0.0; Y.y = 0.0; }
+            C X = b[(2 * p) * fstride + m], Y = b[(2 * p + 1) * fstride + m];
+            if (m == 0) { X.y = T(0); Y.y = T(0); }
             s[p * XAS + prow<XPS>(m)] = mk(X.x - Y.y, X.y + Y.x);
             if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
         }
     }
     for (int n = KI + 1 + lane; n < NX - KI; n += 32) {
 #pragma unroll
-        for (int p = 0; p < 3; p++) s[p * XAS + prow<XPS>(n)] = mk(0.0, 0.0);
+        for (int p = 0; p < 3; p++) s[p * XAS + prow<XPS>(n)] = mk(T(0), T(0));
     }
     __syncwarp();
     if constexpr (NA == 2) {
@@ -110,31 +119,31 @@ __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, i
         fft_warp<NX, +1, 1, XPS, true>(s + XAS, tw, lane);
     }
     fft_warp<NX, +1, 1, XPS, true>(s + 2 * XAS, tw, lane);
-    double umax = 0.0;
+    T umax = T(0);
     for (int n = lane; n < NX; n += 32) {
-        double2* e = s + prow<XPS>(n);
-        const double2 a = e[0], bb = e[XAS], c = e[2 * XAS];
-        const double u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
+        C* e = s + prow<XPS>(n);
+        const C a = e[0], bb = e[XAS], c = e[2 * XAS];
+        const T u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
         if (want_phys) {
             F.phys[q * NX + n] = u1;
             F.phys[g.R + q * NX + n] = u2;
             F.phys[2 * g.R + q * NX + n] = u3;
         }
         if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
-        if (g.shear) {   // f_RK3ComputeNonlinearBFRot
+        if (g.shear) {   // f_RK3ComputeNonlinearBFRot (FP64 registers in both forms)
             const double uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
             double nl[3];
             nl_bf(bf, uu, om, nl);
-            e[0] = mk(nl[0], nl[1]);
-            e[XAS] = mk(nl[2], 0.0);
+            e[0] = mk(T(nl[0]), T(nl[1]));
+            e[XAS] = mk(T(nl[2]), T(0));
         } else {
             e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
-            e[XAS] = mk(u2 * w1 - u1 * w2, 0.0);
+            e[XAS] = mk(u2 * w1 - u1 * w2, T(0));
         }
     }
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-        if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong(umax));
+        if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
     }
     __syncwarp();
     if constexpr (NA == 2) {
@@ -143,15 +152,16 @@ __global__ void __launch_bounds__(NT, Cfg<NX>::MINBX) k_xpass(Fields F, Geo g, i
         fft_warp<NX, -1, 1, XPS, true>(s, tw, lane);
         fft_warp<NX, -1, 1, XPS, true>(s + XAS, tw, lane);
     }
+    const T half = T(0.5);
     for (int m = lane; m < g.nkip; m += 32) {
-        double2 n1 = mk(0.0, 0.0), n2 = n1, n3 = n1;
+        C n1 = mk(T(0), T(0)), n2 = n1, n3 = n1;
         if (m < NKI) {
             const int mc = (NX - m) % NX;
-            const double2 Z = s[prow<XPS>(m)], Zc = s[prow<XPS>(mc)];
-            n1 = mk(0.5 * (Z.x + Zc.x), 0.5 * (Z.y - Zc.y));
-            n2 = mk(0.5 * (Z.y + Zc.y), -0.5 * (Z.x - Zc.x));
-            const double2 W = s[XAS + prow<XPS>(m)], Wc = s[XAS + prow<XPS>(mc)];
-            n3 = mk(0.5 * (W.x + Wc.x), 0.5 * (W.y - Wc.y));
+            const C Z = s[prow<XPS>(m)], Zc = s[prow<XPS>(mc)];
+            n1 = mk(half * (Z.x + Zc.x), half * (Z.y - Zc.y));
+            n2 = mk(half * (Z.y + Zc.y), -half * (Z.x - Zc.x));
+            const C W = s[XAS + prow<XPS>(m)], Wc = s[XAS + prow<XPS>(mc)];
+            n3 = mk(half * (W.x + Wc.x), half * (W.y - Wc.y));
         }
         b[m] = n1;
         b[fstride + m] = n2;
@@ -173,15 +183,20 @@ __device__ __forceinline__ void rk_coeffs(int stage, double& beta, double& gamma
     else { beta = -(153.0 / 128.0); gamma = 8.0 / 15.0; }
 }
 
-struct Out3 { double2* p[3]; };
+template <class C> struct Out3 { C* p[3]; };
 
 // K5b: per mode f_RK3FormFIsotropic / f_RK3FormFBFRot + f_RK3RungeKutta +
 // f_RK3ContinuityFixIsotropic (src/pf_rk3.f90:2323-2673, 3457-3531), one thread
 // per mode, streaming NL-hat, u and rk.
 // Separate instantiations for the isotropic (with forcing) and the BF-rot right-hand
 // side: 3 and 4 CTAs of 256 threads per SM, without spills.
-template <bool SHEAR>
-__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(Fields F, Geo g, const double2* __restrict__ nlh, int stage) {
+// The per-mode arithmetic runs in FP64 registers in both forms (the FP32-mixed
+// form loads FP32 values and rounds once on the store).
+template <bool SHEAR, class T>
+__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(FieldsT<T> F, Geo g,
+                                                               const typename FieldsT<T>::C* __restrict__ nlh,
+                                                               int stage) {
+    using C = typename FieldsT<T>::C;
     const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= g.S) return;
     const int NKK = g.nkk;
@@ -197,14 +212,14 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(Fields F, Geo 
     const double kv[3] = {k1, k2, k3};
     double2 nl[3], uu[3], tot[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) { nl[c] = nlh[c * g.S + m]; uu[c] = F.u[c][m]; }
+    for (int c = 0; c < 3; c++) { nl[c] = to_d(nlh[c * g.S + m]); uu[c] = to_d(F.u[c][m]); }
     if constexpr (SHEAR) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
         const BF bf = make_bf(g, F.clock);
         rhs_bf(bf, g.nu, kv, uu, nl, tot);
     } else {
         const double2 kdn = mk(k1 * nl[0].x + k2 * nl[1].x + k3 * nl[2].x,
                                k1 * nl[0].y + k2 * nl[1].y + k3 * nl[2].y);
-        double2 force[3] = {mk(0, 0), mk(0, 0), mk(0, 0)};
+        double2 force[3] = {mk(0.0, 0.0), mk(0.0, 0.0), mk(0.0, 0.0)};
         const double kmag = sqrt(kmag2);
         if (kmag <= g.force_kf && kmag > 0.0) {
             const int NK = g.fnk, FW = 2 * NK + 1;
@@ -232,16 +247,16 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(Fields F, Geo 
         double2 r;
         if (stage == 1) r = tot[c];   // beta = 0; registers start at zero (src/pf_arrays.f90:805-832)
         else {
-            const double2 r0 = F.rk[c][m];
+            const double2 r0 = to_d(F.rk[c][m]);
             r = mk((beta * r0.x) + tot[c].x, (beta * r0.y) + tot[c].y);
         }
-        F.rk[c][m] = r;
+        F.rk[c][m] = from_d<C>(r);
         uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
     }
     const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x, k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
 #pragma unroll
     for (int c = 0; c < 3; c++)
-        F.u[c][m] = mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2));
+        F.u[c][m] = from_d<C>(mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2)));
 }
 
 // ---------------------------------------------------------------------------
@@ -252,8 +267,12 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(Fields F, Geo 
 // ---------------------------------------------------------------------------
 template <int N> struct TCfg {
     static constexpr int NT = pdfft::tile_threads<N>();
-    static constexpr int MINB = NT <= 128 ? 5 : (NT <= 256 ? 2 : 1);
-    static constexpr size_t SMEM = sizeof(double2) * (size_t)N * L;
+    // resident CTAs per SM asked of the register allocator: FP32 tiles need half the
+    // registers and shared memory of FP64 ones
+    template <class T> static constexpr int minb() {
+        return sizeof(T) == 8 ? (NT <= 128 ? 5 : (NT <= 256 ? 2 : 1)) : (NT <= 128 ? 8 : (NT <= 256 ? 4 : 2));
+    }
+    template <class T> static constexpr size_t smem() { return sizeof(typename Cplx<T>::type) * (size_t)N * L; }
 };
 
 // K1: spectral velocity and vorticity, backward z transforms.  Field f =
@@ -263,83 +282,87 @@ template <int N> struct TCfg {
 // k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.
-template <int NZ, bool SHEAR>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zpass_inv(Fields F, Geo g, int stage) {
-    extern __shared__ double2 s[];
+template <int NZ, bool SHEAR, class T>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_inv(FieldsT<T> F, Geo g, int stage) {
+    using C = typename FieldsT<T>::C;
+    C* s = smem_as<C>();
     const int f = blockIdx.x, i0 = blockIdx.y * L, j = blockIdx.z;
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const double k2 = wvn(j, g.kj);
+    const T k2t = (T)k2;
     const long long istride = (long long)g.nkj * NKK;
     const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
     // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1)
-    const double2* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
-    const double2* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
+    const C* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
+    const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
     BF bf;
     if constexpr (SHEAR) {
         if (f >= 3) bf = make_bf(g, F.clock);
     }
-    auto ld = [&](int z, int l) -> double2 {
+    auto ld = [&](int z, int l) -> C {
         const int i = i0 + l;
         int k;
         if (z <= KK) k = z;
         else if (z >= NZ - KK) k = z - NZ + NKK;
-        else return mk(0.0, 0.0);
-        if (i >= nki) return mk(0.0, 0.0);
+        else return mk(T(0), T(0));
+        if (i >= nki) return mk(T(0), T(0));
         const long long m = row0 + l * istride + k;
         if (f < 3) return pa[m];
-        const double k1 = (double)i, k3 = wvn(k, KK);
-        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot)
-            const double kv[3] = {k1, k2, k3};
-            const double2 uv[3] = {F.u[0][m], F.u[1][m], F.u[2][m]};
+        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot), FP64 registers
+            const double kv[3] = {(double)i, k2, wvn(k, KK)};
+            const double2 uv[3] = {to_d(F.u[0][m]), to_d(F.u[1][m]), to_d(F.u[2][m])};
             double2 w3[3];
             vort_bf(bf, uv, kv, w3);
-            return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
+            return from_d<C>(f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]));
         } else {
-            const double ka = (f == 3) ? k2 : ((f == 4) ? k3 : k1);
-            const double kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2);
-            const double2 a = pa[m], b = pb[m];
+            const T k1 = (T)i, k3 = (T)wvn(k, KK);
+            const T ka = (f == 3) ? k2t : ((f == 4) ? k3 : k1);
+            const T kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2t);
+            const C a = pa[m], b = pb[m];
             return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
         }
     };
-    double2* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+    C* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
     const long long zs = (long long)g.nkj * g.nkip;
-    auto st = [&](int z, int l, double2 v) { dst[z * zs + l] = v; };
+    auto st = [&](int z, int l, C v) { dst[z * zs + l] = v; };
     pdfft::fft_tile_io<NZ, +1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
 // [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).
-template <int NY>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_ypass_inv(Fields F, Geo g) {
-    extern __shared__ double2 s[];
+template <int NY, class T>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_inv(FieldsT<T> F, Geo g) {
+    using C = typename FieldsT<T>::C;
+    C* s = smem_as<C>();
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
-    const double2* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
-    double2* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
-    auto ld = [&](int y, int l) -> double2 {
+    const C* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
+    C* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
+    auto ld = [&](int y, int l) -> C {
         if (y <= KJ) return src[y * rs + l];
         if (y >= NY - KJ) return src[(y - NY + NKJ) * rs + l];
-        return mk(0.0, 0.0);
+        return mk(T(0), T(0));
     };
-    auto st = [&](int y, int l, double2 v) { dst[y * rs + l] = v; };
+    auto st = [&](int y, int l, C v) { dst[y * rs + l] = v; };
     pdfft::fft_tile_io<NY, +1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
 }
 
 // K4: forward y transforms of NL field f = blockIdx.z, truncated to j
 // (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
-template <int NY>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_ypass_fwd(Fields F, Geo g) {
-    extern __shared__ double2 s[];
+template <int NY, class T>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_fwd(FieldsT<T> F, Geo g) {
+    using C = typename FieldsT<T>::C;
+    C* s = smem_as<C>();
     const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
-    const double2* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
-    double2* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
-    auto ld = [&](int y, int l) -> double2 { return src[y * rs + l]; };
-    auto st = [&](int y, int l, double2 v) {
+    const C* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
+    C* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
+    auto ld = [&](int y, int l) -> C { return src[y * rs + l]; };
+    auto st = [&](int y, int l, C v) {
         if (y <= KJ) dst[y * rs + l] = v;
         else if (y >= NY - KJ) dst[(y - NY + NKJ) * rs + l] = v;
     };
@@ -348,18 +371,20 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::MINB) k_ypass_fwd(Fiel
 
 // K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
 // to k, stored as rows of NL-hat [c][i][j][k].
-template <int NZ>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zpass_fwd(Fields F, Geo g, Out3 nlh) {
-    extern __shared__ double2 s[];
+template <int NZ, class T>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_fwd(FieldsT<T> F, Geo g,
+                                                                          Out3<typename FieldsT<T>::C> nlh) {
+    using C = typename FieldsT<T>::C;
+    C* s = smem_as<C>();
     const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const long long zs = (long long)g.nkj * g.nkip;
-    const double2* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
-    double2* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
+    const C* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+    C* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
     const long long istride = (long long)g.nkj * NKK;
-    const double norm = g.norm;
-    auto ld = [&](int z, int l) -> double2 { return src[z * zs + l]; };
-    auto st = [&](int z, int l, double2 v) {
+    const T norm = (T)g.norm;
+    auto ld = [&](int z, int l) -> C { return src[z * zs + l]; };
+    auto st = [&](int z, int l, C v) {
         if (i0 + l >= nki) return;
         int k;
         if (z <= KK) k = z;
@@ -371,45 +396,47 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::MINB) k_zpass_fwd(Fiel
 }
 
 // ---------------------------------------------------------------------------
-// host launchers
+// host launchers (T = double: FP64 form; T = float: FP32-mixed form)
 // ---------------------------------------------------------------------------
-template <int N> static size_t smem_kx() {
-    return sizeof(double2) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
+template <int N, class T> static size_t smem_kx() {
+    return sizeof(typename Cplx<T>::type) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
 }
 
 template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-cudaError_t configure_kernels(const Geo& g) {
+template <class T> cudaError_t configure_kernels(const Geo& g) {
     cudaError_t e = cudaSuccess;
-#define PD_CFG(N)                                                                     \
-    if (g.nz == N) {                                                                  \
-        if ((e = set_smem(k_zpass_inv<N, false>, TCfg<N>::SMEM))) return e;             \
-        if ((e = set_smem(k_zpass_inv<N, true>, TCfg<N>::SMEM))) return e;              \
-        if ((e = set_smem(k_zpass_fwd<N>, TCfg<N>::SMEM))) return e;                    \
-    }                                                                                 \
-    if (g.ny == N) {                                                                  \
-        if ((e = set_smem(k_ypass_inv<N>, TCfg<N>::SMEM))) return e;                    \
-        if ((e = set_smem(k_ypass_fwd<N>, TCfg<N>::SMEM))) return e;                    \
-    }                                                                                 \
-    if (g.nx == N) {                                                                  \
-        if ((e = set_smem(k_xpass<N>, smem_kx<N>()))) return e;                       \
+#define PD_CFG(N)                                                                        \
+    if (g.nz == N) {                                                                     \
+        if ((e = set_smem(k_zpass_inv<N, false, T>, TCfg<N>::template smem<T>()))) return e; \
+        if ((e = set_smem(k_zpass_inv<N, true, T>, TCfg<N>::template smem<T>()))) return e;  \
+        if ((e = set_smem(k_zpass_fwd<N, T>, TCfg<N>::template smem<T>()))) return e;        \
+    }                                                                                    \
+    if (g.ny == N) {                                                                     \
+        if ((e = set_smem(k_ypass_inv<N, T>, TCfg<N>::template smem<T>()))) return e;        \
+        if ((e = set_smem(k_ypass_fwd<N, T>, TCfg<N>::template smem<T>()))) return e;        \
+    }                                                                                    \
+    if (g.nx == N) {                                                                     \
+        if ((e = set_smem(k_xpass<N, T>, smem_kx<N, T>()))) return e;                    \
     }
     PD_FOR_EACH_N(PD_CFG)
 #undef PD_CFG
     return cudaSuccess;
 }
 
-cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStream_t st) {
+template <class T> cudaError_t launch_zpass_inv(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st) {
     switch (g.nz) {
-#define PD_L(N)                                                                       \
-    case N:                                                                           \
-        if (g.shear)                                                                  \
-            k_zpass_inv<N, true><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
-        else                                                                          \
-            k_zpass_inv<N, false><<<dim3(6, g.nkip / L, g.nkj), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, stage); \
-        break;
+#define PD_L(N)                                                                                   \
+    case N: {                                                                                     \
+        const dim3 grid(6, g.nkip / L, g.nkj);                                                    \
+        if (g.shear)                                                                              \
+            k_zpass_inv<N, true, T><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, stage); \
+        else                                                                                      \
+            k_zpass_inv<N, false, T><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, stage); \
+        break;                                                                                    \
+    }
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
@@ -417,11 +444,11 @@ cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStrea
     return cudaGetLastError();
 }
 
-cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st) {
+template <class T> cudaError_t launch_ypass_inv(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
     switch (g.ny) {
-#define PD_L(N)                                                                       \
-    case N:                                                                           \
-        k_ypass_inv<N><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
+#define PD_L(N)                                                                                   \
+    case N:                                                                                       \
+        k_ypass_inv<N, T><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -430,14 +457,15 @@ cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_xpass(const Geo& g, const Fields& f, int want_phys, int want_cfl, cudaStream_t st) {
+template <class T>
+cudaError_t launch_xpass(const Geo& g, const FieldsT<T>& f, int want_phys, int want_cfl, cudaStream_t st) {
     const long long lines = (long long)g.ny * g.nz;
     switch (g.nx) {
-#define PD_L(N)                                                                             \
-    case N: {                                                                               \
-        const long long nb = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                       \
-        k_xpass<N><<<(unsigned)nb, 32 * Cfg<N>::NWX, smem_kx<N>(), st>>>(f, g, want_phys, want_cfl); \
-        break;                                                                              \
+#define PD_L(N)                                                                                   \
+    case N: {                                                                                     \
+        const long long nb = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                             \
+        k_xpass<N, T><<<(unsigned)nb, 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(f, g, want_phys, want_cfl); \
+        break;                                                                                    \
     }
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -446,11 +474,11 @@ cudaError_t launch_xpass(const Geo& g, const Fields& f, int want_phys, int want_
     return cudaGetLastError();
 }
 
-cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
+template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
     switch (g.ny) {
-#define PD_L(N)                                                                       \
-    case N:                                                                           \
-        k_ypass_fwd<N><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g); \
+#define PD_L(N)                                                                                   \
+    case N:                                                                                       \
+        k_ypass_fwd<N, T><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -459,13 +487,14 @@ cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, int mode, cudaStream_t st) {
-    Out3 nlh;
+template <class T>
+cudaError_t launch_zpass_fwd_update(const Geo& g, const FieldsT<T>& f, int stage, int mode, cudaStream_t st) {
+    Out3<typename FieldsT<T>::C> nlh;
     for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? f.rk[c] : f.yb + c * g.S;
     switch (g.nz) {
-#define PD_L(N)                                                                             \
-    case N:                                                                                 \
-        k_zpass_fwd<N><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::SMEM, st>>>(f, g, nlh); \
+#define PD_L(N)                                                                                   \
+    case N:                                                                                       \
+        k_zpass_fwd<N, T><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, nlh); \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -473,9 +502,43 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, in
     }
     cudaError_t e = cudaGetLastError();
     if (e || mode == 1) return e;
-    if (g.shear) k_rk_update<true><<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
-    else k_rk_update<false><<<(unsigned)((g.S + 255) / 256), 256, 0, st>>>(f, g, f.yb, stage);
+    const unsigned nb = (unsigned)((g.S + 255) / 256);
+    if (g.shear) k_rk_update<true, T><<<nb, 256, 0, st>>>(f, g, f.yb, stage);
+    else k_rk_update<false, T><<<nb, 256, 0, st>>>(f, g, f.yb, stage);
     return cudaGetLastError();
 }
+
+// conversions at the FP64 boundary of the FP32-mixed form
+__global__ void k_to_f32(const double2* __restrict__ in, float2* __restrict__ out, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        out[q] = make_float2((float)in[q].x, (float)in[q].y);
+}
+__global__ void k_to_f64(const float2* __restrict__ in, double2* __restrict__ out, long long n) {
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        out[q] = make_double2(in[q].x, in[q].y);
+}
+static unsigned conv_blocks(long long n) {
+    const long long b = (n + 255) / 256;
+    return (unsigned)(b < 4096 ? (b > 0 ? b : 1) : 4096);
+}
+cudaError_t launch_convert(const double2* in, float2* out, long long n, cudaStream_t st) {
+    k_to_f32<<<conv_blocks(n), 256, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStream_t st) {
+    k_to_f64<<<conv_blocks(n), 256, 0, st>>>(in, out, n);
+    return cudaGetLastError();
+}
+
+#define PD_INST(T)                                                                                       \
+    template cudaError_t configure_kernels<T>(const Geo&);                                               \
+    template cudaError_t launch_zpass_inv<T>(const Geo&, const FieldsT<T>&, int, cudaStream_t);          \
+    template cudaError_t launch_ypass_inv<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
+    template cudaError_t launch_xpass<T>(const Geo&, const FieldsT<T>&, int, int, cudaStream_t);         \
+    template cudaError_t launch_ypass_fwd<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
+    template cudaError_t launch_zpass_fwd_update<T>(const Geo&, const FieldsT<T>&, int, int, cudaStream_t);
+PD_INST(double)
+PD_INST(float)
+#undef PD_INST
 
 }  // namespace pd

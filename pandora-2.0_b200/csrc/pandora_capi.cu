@@ -27,9 +27,12 @@ struct pandora_handle {
     int timing = 0;                   // pandora_set_pass_timing: bit p-1 times pass p
     bool timed[3][6] = {};
     cudaEvent_t tev[3][6][2] = {};
-    Fields F{};
-    double2* fbuf = nullptr;          // u[3], rk[3] contiguous
-    double2* tw = nullptr;            // tw_x | tw_y | tw_z
+    Fields F{};                       // FP64 view of the buffers (and the FP64 scratch of the mixed form)
+    FieldsT<float> Ff{};              // FP32 view of the same buffers (FP32-mixed form)
+    bool mixed = false;               // PANDORA_PREC_FP32_MIXED
+    size_t celem = sizeof(double2);   // bytes of one stored complex value
+    void* fbuf = nullptr;             // u[3], rk[3] contiguous
+    void* tw = nullptr;               // tw_x | tw_y | tw_z
     Clock* clock = nullptr;
     Clock* clock_host = nullptr;      // pinned mirror
     double* shell_step = nullptr;     // stats of the state at stage 1 of the last step
@@ -44,7 +47,7 @@ struct pandora_handle {
     double* pbuf = nullptr;           // 13 * np doubles + np pid
     double* pbuf2 = nullptr;          // sort destination, same layout
     PartSort sort{};
-    double2* nlbuf = nullptr;         // scratch for pandora_nonlinear
+    void* nlbuf = nullptr;            // scratch for pandora_nonlinear
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
@@ -166,7 +169,7 @@ static void release(pandora_handle* h) {
 
 static int validate(const pandora_params* p) {
     if (!p) return PANDORA_ERR_INVALID_ARG;
-    if (p->precision != PANDORA_PREC_FP64) return PANDORA_ERR_UNSUPPORTED;
+    if (p->precision != PANDORA_PREC_FP64 && p->precision != PANDORA_PREC_FP32_MIXED) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type != PANDORA_F_ISOTROPIC && p->f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type == PANDORA_F_SHEAR_DNS) {
         if (p->ns_deformed != PANDORA_NS_BF_ROT) return PANDORA_ERR_UNSUPPORTED;
@@ -222,6 +225,9 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.bvol = (double)p->b110 * (double)p->b220 * (double)p->b330;
     h->nforce = (long long)(g.fnk + 1) * (2 * g.fnk + 1) * (2 * g.fnk + 1);
     h->particles_on = p->p_track_part != 0;
+    h->mixed = p->precision == PANDORA_PREC_FP32_MIXED;
+    h->celem = h->mixed ? sizeof(float2) : sizeof(double2);
+    const size_t ce = h->celem;
 
     cudaError_t e;
 #define PD_ALLOC(ptr, bytes)                                              \
@@ -229,13 +235,14 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
         e = cudaMalloc((void**)&(ptr), (bytes));                          \
         if (e != cudaSuccess) { cudaGetLastError(); release(h); return PANDORA_ERR_OOM; } \
     } while (0)
-    PD_ALLOC(h->fbuf, sizeof(double2) * 6 * (size_t)g.S);
-    for (int c = 0; c < 3; c++) { h->F.u[c] = h->fbuf + c * g.S; h->F.rk[c] = h->fbuf + (3 + c) * g.S; }
-    PD_ALLOC(h->F.zb, sizeof(double2) * 6 * (size_t)g.nz * g.nkj * g.nkip);
-    PD_ALLOC(h->F.yb, sizeof(double2) * 6 * (size_t)g.nz * g.ny * g.nkip);
-    if (h->particles_on) PD_ALLOC(h->F.phys, sizeof(double) * 3 * (size_t)g.R);
+    // fields in the stored precision; zb (6 x NZ x NKJ x NKIP values, NZ >= NKK and
+    // NKIP >= NKI) always holds 3S FP64 values, the conversion scratch of the mixed form
+    PD_ALLOC(h->fbuf, ce * 6 * (size_t)g.S);
+    PD_ALLOC(h->F.zb, ce * 6 * (size_t)g.nz * g.nkj * g.nkip);
+    PD_ALLOC(h->F.yb, ce * 6 * (size_t)g.nz * g.ny * g.nkip);
+    if (h->particles_on) PD_ALLOC(h->F.phys, ce / 2 * 3 * (size_t)g.R);
     PD_ALLOC(h->F.forcing, sizeof(double2) * 3 * (size_t)h->nforce);
-    PD_ALLOC(h->tw, sizeof(double2) * (size_t)(g.nx + g.ny + g.nz));
+    PD_ALLOC(h->tw, ce * (size_t)(g.nx + g.ny + g.nz));
     PD_ALLOC(h->clock, sizeof(Clock));
     const size_t nsh = shell_words(g);
     PD_ALLOC(h->shell_step, sizeof(double) * nsh);
@@ -252,22 +259,31 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
         release(h); return cuda_fail(e, "cudaStreamCreate");
     }
     h->st = h->own;
-    // twiddles tw[e] = exp(-2 pi i e / N), long double on the host
-    std::vector<double2> tw((size_t)(g.nx + g.ny + g.nz));
-    int off = 0;
-    const int lens[3] = {g.nx, g.ny, g.nz};
-    const double2** dst[3] = {&h->F.tw_x, &h->F.tw_y, &h->F.tw_z};
-    for (int d = 0; d < 3; d++) {
-        const int n = lens[d];
-        for (int q = 0; q < n; q++) {
-            const long double a = 6.283185307179586476925286766559005768L * (long double)q / (long double)n;
-            tw[off + q] = make_double2((double)cosl(a), -(double)sinl(a));
+    // twiddles tw[e] = exp(-2 pi i e / N), long double on the host, rounded once to
+    // the stored precision
+    {
+        const size_t ntw = (size_t)(g.nx + g.ny + g.nz);
+        std::vector<double2> tw(ntw);
+        std::vector<float2> twf(ntw);
+        int off = 0;
+        const int lens[3] = {g.nx, g.ny, g.nz};
+        const int offs[3] = {0, g.nx, g.nx + g.ny};
+        for (int d = 0; d < 3; d++) {
+            const int n = lens[d];
+            for (int q = 0; q < n; q++) {
+                const long double a = 6.283185307179586476925286766559005768L * (long double)q / (long double)n;
+                tw[off + q] = make_double2((double)cosl(a), -(double)sinl(a));
+                twf[off + q] = make_float2((float)cosl(a), -(float)sinl(a));
+            }
+            off += n;
         }
-        *dst[d] = h->tw + off;
-        off += n;
-    }
-    if ((e = cudaMemcpy(h->tw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice)) != cudaSuccess) {
-        release(h); return cuda_fail(e, "twiddles");
+        const double2* twd = (const double2*)h->tw;
+        const float2* tws = (const float2*)h->tw;
+        h->F.tw_x = twd + offs[0]; h->F.tw_y = twd + offs[1]; h->F.tw_z = twd + offs[2];
+        h->Ff.tw_x = tws + offs[0]; h->Ff.tw_y = tws + offs[1]; h->Ff.tw_z = tws + offs[2];
+        e = h->mixed ? cudaMemcpy(h->tw, twf.data(), sizeof(float2) * ntw, cudaMemcpyHostToDevice)
+                     : cudaMemcpy(h->tw, tw.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { release(h); return cuda_fail(e, "twiddles"); }
     }
     // mode density (src/pf_fluidstats.f90:696-780), integer counts -> exact
     h->dens_mod.assign(g.kkmax + 1, 0.0);
@@ -290,8 +306,14 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
             h->dens_mod[q] = (double)cnt[q] / (4.0 / 3.0 * pi * (up * up * up - lo * lo * lo));
         }
     }
-    h->F.clock = h->clock;
-    h->F.shell = h->shell_step;
+    for (int c = 0; c < 3; c++) {
+        h->F.u[c] = (double2*)h->fbuf + c * g.S; h->F.rk[c] = (double2*)h->fbuf + (3 + c) * g.S;
+        h->Ff.u[c] = (float2*)h->fbuf + c * g.S; h->Ff.rk[c] = (float2*)h->fbuf + (3 + c) * g.S;
+    }
+    h->Ff.zb = (float2*)h->F.zb; h->Ff.yb = (float2*)h->F.yb; h->Ff.phys = (float*)h->F.phys;
+    h->Ff.forcing = h->F.forcing;
+    h->F.clock = h->clock; h->Ff.clock = h->clock;
+    h->F.shell = h->shell_step; h->Ff.shell = h->shell_step;
     h->sp.rk3_timestep = p->rk3_timestep; h->sp.f_type = p->f_type; h->sp.rk3_dt = p->rk3_dt;
     h->sp.rk3_cfl = p->rk3_cfl; h->sp.force_tf = p->force_tf; h->sp.f_deform_s = p->f_deform_s;
     h->sp.f_remesh_t = p->f_remesh_t;
@@ -300,12 +322,14 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     h->fp.calls_per_stage = force_calls(g.fnk);
     h->pp.order = p->p_interp_order; h->pp.release = p->p_ts_release; h->pp.f_nu = p->f_nu;
     h->pp.p_rho = p->p_rho; h->pp.f_rho = p->f_rho;
-    if ((e = configure_kernels(g)) != cudaSuccess) { release(h); return cuda_fail(e, "configure_kernels"); }
+    if ((e = h->mixed ? configure_kernels<float>(g) : configure_kernels<double>(g)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "configure_kernels");
+    }
     if ((e = configure_fluid_kernels(g, h->fp)) != cudaSuccess) {
         release(h); return cuda_fail(e, "configure_fluid_kernels");
     }
     // zero state (the reference zero-initialises its Vecs and rk3 registers)
-    if ((e = cudaMemsetAsync(h->fbuf, 0, sizeof(double2) * 6 * (size_t)g.S, h->st)) != cudaSuccess ||
+    if ((e = cudaMemsetAsync(h->fbuf, 0, ce * 6 * (size_t)g.S, h->st)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->clock, 0, sizeof(Clock), h->st)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->shell_step, 0, sizeof(double) * nsh, h->st)) != cudaSuccess ||
@@ -386,21 +410,42 @@ static int copy3(pandora_handle* h, double2* const* dev, const double* a, const 
     return PANDORA_OK;
 }
 
+// Three spectral fields of S complex values at the FP64 boundary.  The mixed form
+// stores FP32: the host's FP64 values pass through the z-pencil buffer (free between
+// steps) and are converted on the device in either direction.
+static int copy_fields(pandora_handle* h, double2* const* dev64, float2* const* dev32, const double* a,
+                       const double* b, const double* c, bool to_dev) {
+    if (!a || !b || !c) return PANDORA_ERR_INVALID_ARG;
+    if (!h->mixed) return copy3(h, dev64, a, b, c, (size_t)h->g.S, to_dev);
+    cudaSetDevice(h->dev);
+    const long long S = h->g.S;
+    double2* scr[3] = {h->F.zb, h->F.zb + S, h->F.zb + 2 * S};
+    if (to_dev) {
+        int rc = copy3(h, scr, a, b, c, (size_t)S, true);
+        if (rc) return rc;
+        for (int q = 0; q < 3; q++) PD_CK(launch_convert(scr[q], dev32[q], S, h->st));
+        PD_CK(cudaStreamSynchronize(h->st));
+        return PANDORA_OK;
+    }
+    for (int q = 0; q < 3; q++) PD_CK(launch_convert(dev32[q], scr[q], S, h->st));
+    return copy3(h, scr, a, b, c, (size_t)S, false);
+}
+
 extern "C" int pandora_set_state(pandora_handle* h, const double* u1, const double* u2, const double* u3) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
-    return copy3(h, h->F.u, u1, u2, u3, (size_t)h->g.S, true);
+    return copy_fields(h, h->F.u, h->Ff.u, u1, u2, u3, true);
 }
 extern "C" int pandora_get_state(pandora_handle* h, double* u1, double* u2, double* u3) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
-    return copy3(h, h->F.u, u1, u2, u3, (size_t)h->g.S, false);
+    return copy_fields(h, h->F.u, h->Ff.u, u1, u2, u3, false);
 }
 extern "C" int pandora_set_rk(pandora_handle* h, const double* r1, const double* r2, const double* r3) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
-    return copy3(h, h->F.rk, r1, r2, r3, (size_t)h->g.S, true);
+    return copy_fields(h, h->F.rk, h->Ff.rk, r1, r2, r3, true);
 }
 extern "C" int pandora_get_rk(pandora_handle* h, double* r1, double* r2, double* r3) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
-    return copy3(h, h->F.rk, r1, r2, r3, (size_t)h->g.S, false);
+    return copy_fields(h, h->F.rk, h->Ff.rk, r1, r2, r3, false);
 }
 extern "C" int pandora_forcing_size(pandora_handle* h, int64_t* n) {
     if (!h || !n) return PANDORA_ERR_INVALID_ARG;
@@ -419,7 +464,8 @@ extern "C" int pandora_get_forcing(pandora_handle* h, double* f1, double* f2, do
 }
 extern "C" int pandora_state_device_ptrs(pandora_handle* h, void** u1, void** u2, void** u3) {
     if (!h || !u1 || !u2 || !u3) return PANDORA_ERR_INVALID_ARG;
-    *u1 = h->F.u[0]; *u2 = h->F.u[1]; *u3 = h->F.u[2];
+    if (h->mixed) { *u1 = h->Ff.u[0]; *u2 = h->Ff.u[1]; *u3 = h->Ff.u[2]; }
+    else { *u1 = h->F.u[0]; *u2 = h->F.u[1]; *u3 = h->F.u[2]; }
     return PANDORA_OK;
 }
 
@@ -432,7 +478,14 @@ extern "C" int pandora_init_fluid(pandora_handle* h) {
     ip.b110 = h->p.b110; ip.b220 = h->p.b220; ip.b330 = h->p.b330;
     ip.deformed = (h->p.b110 + h->p.b220 + h->p.b330) > 3 ? 1 : 0;
     ip.key = stream_key(h->p.seed_fluid, TAG_FLUID);
-    PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
+    if (h->mixed) {   // generated in FP64 into the z-pencil buffer, then rounded once
+        Fields Fd = h->F;
+        for (int c = 0; c < 3; c++) Fd.u[c] = h->F.zb + c * h->g.S;
+        PD_CK(launch_init_fluid(h->g, Fd, ip, h->st));
+        for (int c = 0; c < 3; c++) PD_CK(launch_convert(Fd.u[c], h->Ff.u[c], h->g.S, h->st));
+    } else {
+        PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
+    }
     PD_CK(cudaStreamSynchronize(h->st));
     return PANDORA_OK;
 }
@@ -497,6 +550,11 @@ extern "C" int pandora_init_particles(pandora_handle* h) {
     return PANDORA_OK;
 }
 
+// The handle's buffers as fields of the stored precision.
+template <class T> static FieldsT<T>& fields(pandora_handle* h);
+template <> FieldsT<double>& fields<double>(pandora_handle* h) { return h->F; }
+template <> FieldsT<float>& fields<float>(pandora_handle* h) { return h->Ff; }
+
 // ---- stage sequencing ----
 // f_RK3Stage{s} (src/pf_rk3.f90:40-200): [s=1: statistics of the state],
 // vorticity + z pass, y pass, x pass with NL (and CFL / physical velocity),
@@ -507,12 +565,13 @@ extern "C" int pandora_init_particles(pandora_handle* h) {
 // of K3 and the stage's dt) runs beside K4 and K5; the branch joins the main
 // stream before the stage clock advances.  Captured into the step graph, the
 // fork and join become graph edges.
-static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
+template <class T> static int enqueue_stage_t(pandora_handle* h, int stage, int* nlaunch) {
+    const FieldsT<T>& F = fields<T>(h);
     const Geo& g = h->g;
     int n = 0;
     const bool part = h->particles_on && h->P.np > 0;
     if (stage == 1 && g.shear) {
-        PD_CK(launch_remesh(g, h->F, h->P, h->st)); n += part ? 2 : 1;
+        PD_CK(launch_remesh(g, F, h->P, h->st)); n += part ? 2 : 1;
     }
     if (stage == 1 && part) {
         PD_CK(cudaEventRecord(h->ev_fork, h->st));
@@ -520,7 +579,7 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
         PD_CK(launch_particle_sort(g, h->P, h->sort, h->side, &n));
     }
     if (stage == 1) {
-        Fields Fs = h->F;
+        FieldsT<T> Fs = F;
         Fs.shell = h->shell_step;
         PD_CK(launch_stats(g, Fs, h->st)); n += 1;   // one kernel (plus a memset node)
     }
@@ -533,33 +592,37 @@ static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
         return cudaEventRecordWithFlags(h->tev[stage - 1][ps - 1][end], s, cudaEventRecordExternal);
     };
     PD_CK(mark(1, 0, h->st));
-    PD_CK(launch_zpass_inv(g, h->F, stage, h->st)); n++;
+    PD_CK(launch_zpass_inv(g, F, stage, h->st)); n++;
     PD_CK(mark(1, 1, h->st));
     PD_CK(mark(2, 0, h->st));
-    PD_CK(launch_ypass_inv(g, h->F, h->st)); n++;
+    PD_CK(launch_ypass_inv(g, F, h->st)); n++;
     PD_CK(mark(2, 1, h->st));
     PD_CK(mark(3, 0, h->st));
-    PD_CK(launch_xpass(g, h->F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
+    PD_CK(launch_xpass(g, F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
     PD_CK(mark(3, 1, h->st));
-    PD_CK(launch_stage_scalars(g, h->F, h->sp, h->fp, stage, h->st)); n++;
+    PD_CK(launch_stage_scalars(g, F, h->sp, h->fp, stage, h->st)); n++;
     if (part) {
         PD_CK(cudaEventRecord(h->ev_fork, h->st));
         PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
         PD_CK(mark(6, 0, h->side));
-        PD_CK(launch_particles(g, h->F, h->P, h->pp, stage, h->side)); n++;
+        PD_CK(launch_particles(g, F, h->P, h->pp, stage, h->side)); n++;
         PD_CK(mark(6, 1, h->side));
         PD_CK(cudaEventRecord(h->ev_join, h->side));
     }
     PD_CK(mark(4, 0, h->st));
-    PD_CK(launch_ypass_fwd(g, h->F, h->st)); n++;
+    PD_CK(launch_ypass_fwd(g, F, h->st)); n++;
     PD_CK(mark(4, 1, h->st));
     PD_CK(mark(5, 0, h->st));
-    PD_CK(launch_zpass_fwd_update(g, h->F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
+    PD_CK(launch_zpass_fwd_update(g, F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
     PD_CK(mark(5, 1, h->st));
     if (part) PD_CK(cudaStreamWaitEvent(h->st, h->ev_join, 0));
-    PD_CK(launch_advance_time(g, h->F, stage, h->st)); n++;
+    PD_CK(launch_advance_time(g, F, stage, h->st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;
+}
+
+static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
+    return h->mixed ? enqueue_stage_t<float>(h, stage, nlaunch) : enqueue_stage_t<double>(h, stage, nlaunch);
 }
 
 static int enqueue_step(pandora_handle* h) {
@@ -685,9 +748,15 @@ extern "C" int pandora_stats(pandora_handle* h, double* ek, int32_t kkmax, doubl
                              double* ucfl) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(h->dev);
-    Fields Fs = h->F;
-    Fs.shell = h->shell_now;
-    PD_CK(launch_stats(h->g, Fs, h->st));
+    if (h->mixed) {
+        FieldsT<float> Fs = h->Ff;
+        Fs.shell = h->shell_now;
+        PD_CK(launch_stats(h->g, Fs, h->st));
+    } else {
+        Fields Fs = h->F;
+        Fs.shell = h->shell_now;
+        PD_CK(launch_stats(h->g, Fs, h->st));
+    }
     const size_t nsh = shell_words(h->g);
     PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_now, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
@@ -714,12 +783,23 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
     if (!h || !n1 || !n2 || !n3) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(h->dev);
     if (!h->nlbuf) {
-        if (cudaMalloc((void**)&h->nlbuf, sizeof(double2) * 3 * (size_t)h->g.S) != cudaSuccess) {
+        if (cudaMalloc((void**)&h->nlbuf, h->celem * 3 * (size_t)h->g.S) != cudaSuccess) {
             cudaGetLastError(); return PANDORA_ERR_OOM;
         }
     }
+    if (h->mixed) {
+        FieldsT<float> Fn = h->Ff;
+        for (int c = 0; c < 3; c++) Fn.rk[c] = (float2*)h->nlbuf + c * h->g.S;
+        PD_CK(launch_zpass_inv(h->g, Fn, 0, h->st));
+        PD_CK(launch_ypass_inv(h->g, Fn, h->st));
+        PD_CK(launch_xpass(h->g, Fn, 0, 0, h->st));
+        PD_CK(launch_ypass_fwd(h->g, Fn, h->st));
+        PD_CK(launch_zpass_fwd_update(h->g, Fn, 1, 1, h->st));
+        double2* none[3] = {nullptr, nullptr, nullptr};
+        return copy_fields(h, none, Fn.rk, n1, n2, n3, false);
+    }
     Fields Fn = h->F;
-    for (int c = 0; c < 3; c++) Fn.rk[c] = h->nlbuf + c * h->g.S;
+    for (int c = 0; c < 3; c++) Fn.rk[c] = (double2*)h->nlbuf + c * h->g.S;
     PD_CK(launch_zpass_inv(h->g, Fn, 0, h->st));
     PD_CK(launch_ypass_inv(h->g, Fn, h->st));
     PD_CK(launch_xpass(h->g, Fn, 0, 0, h->st));
@@ -733,6 +813,16 @@ extern "C" int pandora_get_physical_velocity(pandora_handle* h, double* u1, doub
     if (!h->F.phys) return PANDORA_ERR_UNSUPPORTED;
     cudaSetDevice(h->dev);
     double* d[3] = {u1, u2, u3};
+    if (h->mixed) {   // stored FP32: widened on the host
+        std::vector<float> tmp((size_t)h->g.R);
+        for (int c = 0; c < 3; c++) {
+            PD_CK(cudaMemcpyAsync(tmp.data(), h->Ff.phys + c * h->g.R, sizeof(float) * h->g.R,
+                                  cudaMemcpyDeviceToHost, h->st));
+            PD_CK(cudaStreamSynchronize(h->st));
+            for (long long q = 0; q < h->g.R; q++) d[c][q] = tmp[(size_t)q];
+        }
+        return PANDORA_OK;
+    }
     for (int c = 0; c < 3; c++)
         PD_CK(cudaMemcpyAsync(d[c], h->F.phys + c * h->g.R, sizeof(double) * h->g.R, cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
@@ -742,7 +832,7 @@ extern "C" int pandora_get_physical_velocity(pandora_handle* h, double* u1, doub
 extern "C" int pandora_check_status(pandora_handle* h) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(h->dev);
-    PD_CK(launch_check_finite(h->g, h->F, h->st));
+    PD_CK(h->mixed ? launch_check_finite(h->g, h->Ff, h->st) : launch_check_finite(h->g, h->F, h->st));
     PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
     const unsigned int st = h->clock_host->status;
@@ -793,22 +883,21 @@ extern "C" int pandora_pass_times(pandora_handle* h, float* ms) {
     return PANDORA_OK;
 }
 
-extern "C" int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps) {
-    if (!h || reps < 0) return PANDORA_ERR_INVALID_ARG;
-    cudaSetDevice(h->dev);
+template <class T> static int profile_pass_t(pandora_handle* h, int32_t pass, int32_t reps) {
     const bool part = h->particles_on && h->P.np > 0;
-    Fields Fs = h->F;
+    const FieldsT<T>& F = fields<T>(h);
+    FieldsT<T> Fs = F;
     Fs.shell = h->shell_now;
     for (int r = 0; r < reps; r++) {
         switch (pass) {
-        case 1: PD_CK(launch_zpass_inv(h->g, h->F, 2, h->st)); break;
-        case 2: PD_CK(launch_ypass_inv(h->g, h->F, h->st)); break;
-        case 3: PD_CK(launch_xpass(h->g, h->F, part ? 1 : 0, 0, h->st)); break;
-        case 4: PD_CK(launch_ypass_fwd(h->g, h->F, h->st)); break;
-        case 5: PD_CK(launch_zpass_fwd_update(h->g, h->F, 2, 0, h->st)); break;
+        case 1: PD_CK(launch_zpass_inv(h->g, F, 2, h->st)); break;
+        case 2: PD_CK(launch_ypass_inv(h->g, F, h->st)); break;
+        case 3: PD_CK(launch_xpass(h->g, F, part ? 1 : 0, 0, h->st)); break;
+        case 4: PD_CK(launch_ypass_fwd(h->g, F, h->st)); break;
+        case 5: PD_CK(launch_zpass_fwd_update(h->g, F, 2, 0, h->st)); break;
         case 6:
             if (!part) return PANDORA_ERR_INVALID_ARG;
-            PD_CK(launch_particles(h->g, h->F, h->P, h->pp, 2, h->st));
+            PD_CK(launch_particles(h->g, F, h->P, h->pp, 2, h->st));
             break;
         case 7: PD_CK(launch_stats(h->g, Fs, h->st)); break;
         default: return PANDORA_ERR_INVALID_ARG;
@@ -817,10 +906,17 @@ extern "C" int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t rep
     return PANDORA_OK;
 }
 
+extern "C" int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps) {
+    if (!h || reps < 0) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    return h->mixed ? profile_pass_t<float>(h, pass, reps) : profile_pass_t<double>(h, pass, reps);
+}
+
 extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes) {
     if (!h || !bytes) return PANDORA_ERR_INVALID_ARG;
     const Geo& g = h->g;
-    const double c16 = 16.0;
+    const double c16 = (double)h->celem;          // one stored complex value
+    const double r8 = (double)h->celem / 2.0;     // one stored real value
     const double S = (double)g.S;
     const double Z = (double)g.nz * g.nkj * g.nki;
     const double Y = (double)g.nz * g.ny * g.nki;
@@ -829,10 +925,10 @@ extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes
     switch (pass) {
     case 1: *bytes = c16 * (3 * S + 6 * Z); break;
     case 2: *bytes = c16 * (6 * Z + 6 * Y); break;
-    case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? 8.0 * 3 * R : 0.0); break;
+    case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? r8 * 3 * R : 0.0); break;
     case 4: *bytes = c16 * (3 * Y + 3 * Z); break;
     case 5: *bytes = c16 * (3 * Z + 3 * S) + c16 * (3 * S + 6 * S + 6 * S); break;   // K5a + K5b
-    case 6: *bytes = part ? 8.0 * (3 * R + 24.0 * (double)h->P.np) : 0.0; break;
+    case 6: *bytes = part ? r8 * 3 * R + 8.0 * 24.0 * (double)h->P.np : 0.0; break;
     case 7: *bytes = c16 * 3 * S; break;
     default: return PANDORA_ERR_INVALID_ARG;
     }

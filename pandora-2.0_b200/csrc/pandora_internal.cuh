@@ -73,18 +73,38 @@ __host__ __device__ __forceinline__ double wvn(int idx, int K) {
     return (double)(idx <= K ? idx : idx - (2 * K + 1));
 }
 
-// Launchers (kernels_*.cu).  All enqueue on `st` and return cudaGetLastError().
-struct Fields {
-    double2* u[3];
-    double2* rk[3];
-    double2* zb;        // [6][NZ][NKJ][NKIP]  after the z pass
-    double2* yb;        // [6][NZ][NY][NKIP]   after the y pass; NL written into fields 0..2
-    double* phys;       // [3][NZ][NY][NX]     physical velocity (particles), may be null
+// Device buffers of one simulation.  T is the real type of the fields and of the
+// transforms: double for the FP64 form, float for the FP32-mixed form, whose
+// forcing coefficients, clock and shell sums stay FP64.
+template <class T> struct Cplx;
+template <> struct Cplx<double> { using type = double2; };
+template <> struct Cplx<float> { using type = float2; };
+
+template <class T> struct FieldsT {
+    using C = typename Cplx<T>::type;
+    C* u[3];
+    C* rk[3];
+    C* zb;              // [6][NZ][NKJ][NKIP]  after the z pass
+    C* yb;              // [6][NZ][NY][NKIP]   after the y pass; NL written into fields 0..2
+    T* phys;            // [3][NZ][NY][NX]     physical velocity (particles), may be null
     double2* forcing;   // [3][NK+1][2NK+1][2NK+1]
-    const double2 *tw_x, *tw_y, *tw_z;
+    const C *tw_x, *tw_y, *tw_z;
     Clock* clock;
     double* shell;      // [3*(kkmax+1) + 3] shell sums (e, d), p11,p22,p33, mode counts
 };
+using Fields = FieldsT<double>;
+
+// FP64 view of a stored value and its rounding back (identity for the FP64 form).
+__host__ __device__ __forceinline__ double2 to_d(double2 v) { return v; }
+__host__ __device__ __forceinline__ double2 to_d(float2 v) { return make_double2(v.x, v.y); }
+template <class C> __host__ __device__ __forceinline__ C from_d(double2 v);
+template <> __host__ __device__ __forceinline__ double2 from_d<double2>(double2 v) { return v; }
+template <> __host__ __device__ __forceinline__ float2 from_d<float2>(double2 v) {
+    return make_float2((float)v.x, (float)v.y);
+}
+
+// Launchers (kernels_*.cu), instantiated for T = double and float.  All enqueue
+// on `st` and return cudaGetLastError().
 
 // Particle arrays, structure of arrays: 13 doubles + the particle's index in
 // the caller's order (pid).  The device keeps them sorted by spatial bin.
@@ -138,28 +158,37 @@ struct InitParams {
 
 bool supported_length(int n);
 
-cudaError_t launch_zpass_inv(const Geo& g, const Fields& f, int stage, cudaStream_t st);
-cudaError_t launch_ypass_inv(const Geo& g, const Fields& f, cudaStream_t st);
-cudaError_t launch_xpass(const Geo& g, const Fields& f, int want_phys, int want_cfl, cudaStream_t st);
-cudaError_t launch_ypass_fwd(const Geo& g, const Fields& f, cudaStream_t st);
-cudaError_t launch_zpass_fwd_update(const Geo& g, const Fields& f, int stage, int mode, cudaStream_t st);
-cudaError_t launch_stats(const Geo& g, const Fields& f, cudaStream_t st);
-cudaError_t launch_stage_scalars(const Geo& g, const Fields& f, const StepParams& sp,
+template <class T> cudaError_t launch_zpass_inv(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st);
+template <class T> cudaError_t launch_ypass_inv(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+template <class T>
+cudaError_t launch_xpass(const Geo& g, const FieldsT<T>& f, int want_phys, int want_cfl, cudaStream_t st);
+template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+template <class T>
+cudaError_t launch_zpass_fwd_update(const Geo& g, const FieldsT<T>& f, int stage, int mode, cudaStream_t st);
+template <class T> cudaError_t launch_stats(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+template <class T>
+cudaError_t launch_stage_scalars(const Geo& g, const FieldsT<T>& f, const StepParams& sp,
                                  const ForceParams& fp, int stage, cudaStream_t st);
-cudaError_t launch_advance_time(const Geo& g, const Fields& f, int stage, cudaStream_t st);
+template <class T> cudaError_t launch_advance_time(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st);
+// The initial field is generated in FP64 (the FP32-mixed form converts it).
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);
-cudaError_t launch_particles(const Geo& g, const Fields& f, const Particles& p, const PartParams& pp,
+template <class T>
+cudaError_t launch_particles(const Geo& g, const FieldsT<T>& f, const Particles& p, const PartParams& pp,
                              int stage, cudaStream_t st);
 cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia,
                                   cudaStream_t st);
 cudaError_t launch_particle_sort(const Geo& g, const Particles& p, const PartSort& s, cudaStream_t st,
                                  int* nlaunch);
-cudaError_t launch_check_finite(const Geo& g, const Fields& f, cudaStream_t st);
-cudaError_t launch_remesh(const Geo& g, const Fields& f, const Particles& p, cudaStream_t st);
+template <class T> cudaError_t launch_check_finite(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+template <class T>
+cudaError_t launch_remesh(const Geo& g, const FieldsT<T>& f, const Particles& p, cudaStream_t st);
+// n complex values from one precision to the other (FP64 <-> FP32 at the boundary).
+cudaError_t launch_convert(const double2* in, float2* out, long long n, cudaStream_t st);
+cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStream_t st);
 size_t shell_words(const Geo& g);
 
 // Shared-memory configuration (set once per process per device).
-cudaError_t configure_kernels(const Geo& g);
+template <class T> cudaError_t configure_kernels(const Geo& g);
 cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp);
 
 }  // namespace pd

@@ -113,7 +113,7 @@ extern "C" int pandora_nonlinear_static(const pandora_params* p, const double* u
         off += lens[d];
     }
     if (cudaMemcpyAsync(sp->tw, tw, sizeof(double2) * off, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        pd::configure_kernels(g) != cudaSuccess) {
+        pd::configure_kernels<double>(g) != cudaSuccess) {
         cudaGetLastError();
         return PANDORA_ERR_CUDA;
     }

@@ -25,6 +25,7 @@ F_INIT_KERR = 4
 F_INIT_AHMED_ELGHOBASHI = 10
 P_INIT_RANDOM = 2
 PREC_FP64 = 0
+PREC_FP32_MIXED = 1   # FP32 fields and transforms, FP64 bookkeeping (include/pandora_gpu.h)
 
 
 class Params(ctypes.Structure):
@@ -100,6 +101,8 @@ def workload_params(name: str, n: int | None = None) -> Params:
     ``iso_forced_particles``: forced isotropic turbulence, nu=0.002, dt=0.002
     fixed, OU forcing on |k| <= 2.5 with sigma^2 T_F = 0.1, kp=3, 2^20 tracers
     (P_INIT_RANDOM, 4th-order interpolation, released at step 1).
+    ``iso_forced``: the same forcing at nu=0.0008, dt=0.001, no particles (1024^3).
+    ``shear``: homogeneous shear S=1 in the Rogallo frame (BF-rot), B110=2, 2^18 tracers.
     """
     if name == "iso_decay":
         p = default_params(n or 64)
@@ -119,6 +122,13 @@ def workload_params(name: str, n: int | None = None) -> Params:
         p.f_init_type, p.f_init_kp, p.f_init_u0 = F_INIT_AHMED_ELGHOBASHI, 3.0, 2.0 / 3.0
         p.p_track_part, p.p_init_type, p.p_np_global = 1, P_INIT_RANDOM, 1 << 20
         p.p_interp_order, p.p_ts_release, p.p_dia_vals = 4, 1, 0.0
+        return p
+    if name == "iso_forced":
+        # forced isotropic turbulence without particles at the mixed-precision size:
+        # nu = 0.0008, dt = 0.001, forcing as iso_forced_particles, kp = 3
+        p = workload_params("iso_forced_particles", n or 1024)
+        p.f_nu, p.rk3_dt, p.tsteps = 0.0008, 0.001, 200
+        p.p_track_part, p.p_np_global = 0, 0
         return p
     if name == "shear":
         # homogeneous shear dU1/dx3 = S in Rogallo (moving-frame) coordinates,

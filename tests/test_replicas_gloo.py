@@ -20,7 +20,8 @@ r = bench.Ranks("gloo", "cpu", timeout_s=60)
 r.barrier()
 m = r.max(0.25 + r.rank)
 p = bench.replica_seeds(workload_params("iso_forced_particles", 16), r.rank)
-print(json.dumps({{"rank": r.rank, "ws": r.ws, "max": m, "seeds": [p.seed_fluid, p.seed_force, p.seed_particles]}}), flush=True)
+with open(os.path.join({out!r}, "rank%d.json" % r.rank), "w") as fh:
+    json.dump({{"rank": r.rank, "ws": r.ws, "max": m, "seeds": [p.seed_fluid, p.seed_force, p.seed_particles]}}, fh)
 r.close()
 """
 
@@ -34,10 +35,10 @@ def _torchrun(nproc, args, port, timeout=240):
 
 def test_two_gloo_ranks_barrier_and_max(tmp_path):
     child = tmp_path / "child.py"
-    child.write_text(_CHILD.format(root=ROOT))
+    child.write_text(_CHILD.format(root=ROOT, out=str(tmp_path)))
     r = _torchrun(2, [str(child)], 29611)
     assert r.returncode == 0, r.stdout + r.stderr
-    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    lines = [json.loads((tmp_path / f"rank{k}.json").read_text()) for k in (0, 1)]
     assert sorted(x["rank"] for x in lines) == [0, 1]
     assert all(x["ws"] == 2 and x["max"] == 1.25 for x in lines)      # max of 0.25 and 1.25
     assert lines[0]["seeds"] != lines[1]["seeds"]                      # each replica its own member
