@@ -239,6 +239,42 @@ int pandora_set_pass_timing(pandora_handle* h, int32_t passes);
 int pandora_pass_times(pandora_handle* h, float* ms);
 
 /*
+ * Batches (no counterpart in the reference: the device side of the ensemble
+ * server).  A batch holds `capacity` slots of one class -- grid size, precision,
+ * flow type with its B110..B330, particles per member and their interpolation
+ * order, forcing radius -- each slot a full simulation with its own state.
+ * Members may differ in seeds, viscosity, dt, forcing amplitude and time scale and
+ * shear rate.  One step of the batch advances every occupied slot: each kernel
+ * launch serves up to 32 members, and members admitted at different times advance
+ * side by side, each with its own step counter and time.  Results are those of
+ * the same simulation run alone (the kernels do the same arithmetic per member).
+ * All calls on one batch run in its stream order; the batch is not re-entrant.
+ */
+typedef struct pandora_batch pandora_batch;
+/* Device bytes a batch of this class and capacity allocates (for admission control). */
+int pandora_batch_bytes(const pandora_params* cls, int32_t capacity, int64_t* bytes);
+int pandora_batch_create(const pandora_params* cls, int32_t capacity, pandora_batch** out);
+int pandora_batch_destroy(pandora_batch* b);
+int pandora_batch_capacity(pandora_batch* b, int32_t* capacity, int32_t* free_slots);
+/* Start a member in a free slot: seeded initial field (and particles), step 1 at
+ * time 0.  PANDORA_ERR_BAD_LAYOUT if `member` is not of the batch's class,
+ * PANDORA_ERR_OOM if no slot is free. */
+int pandora_batch_admit(pandora_batch* b, const pandora_params* member, int32_t* slot);
+int pandora_batch_release(pandora_batch* b, int32_t slot);
+/* Enqueue nsteps RK3 steps of every occupied slot (asynchronous). */
+int pandora_batch_step(pandora_batch* b, int32_t nsteps);
+int pandora_batch_sync(pandora_batch* b);
+int pandora_batch_launches_per_step(pandora_batch* b, int32_t* n);
+/* Next step number, time and dt of a slot's member (waits for the batch). */
+int pandora_batch_member_time(pandora_batch* b, int32_t slot, int32_t* tstep, double* simtime, double* dt);
+int pandora_batch_get_state(pandora_batch* b, int32_t slot, double* u1, double* u2, double* u3);
+int pandora_batch_get_particles(pandora_batch* b, int32_t slot, int64_t np, double* xp, double* up,
+                                double* up_rk3, double* rk3, double* dp);
+/* Statistics of the member's state at stage 1 of its last step. */
+int pandora_batch_last_step_stats(pandora_batch* b, int32_t slot, double* ek, int32_t kkmax, double* tke,
+                                  double* eps);
+
+/*
  * No counterpart in the reference.  The nonlinear term omega x u of a spectral
  * velocity field (the output of pandora_nonlinear), for callers that may not
  * allocate device memory: they pass device buffers u1..u3 (input) and n1..n3

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <math.h>
+#include <type_traits>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
@@ -24,8 +25,12 @@ size_t shell_words(const Geo& g) { return (size_t)3 * (g.kkmax + 1) + 3; }
 // u_lab = B^-1 u (f_FluidstatsFsPrimaryQuantsBFRot, src/pf_fluidstats.f90:1586-1960),
 // with the per-shell mode counts of f_FluidstatsModeDensityBFRot
 // (src/pf_fluidstats.f90:1977-2229), which change with B every step.
-template <class T>
-__global__ void __launch_bounds__(256) k_stats(FieldsT<T> F, Geo g) {
+template <class T, int CAP>
+__global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     extern __shared__ double sh[];
     const int K = g.kkmax;
     double* se = sh;                // [K+1]
@@ -113,9 +118,14 @@ __device__ int normal_pair(uint64_t key, uint64_t call, double& r1, double& r2) 
     return 0;
 }
 
-template <class T>
-__global__ void __launch_bounds__(256) k_stage_scalars(FieldsT<T> F, Geo g, StepParams sp, ForceParams fp,
-                                                       int stage) {
+template <class T, int CAP>
+__global__ void __launch_bounds__(256) k_stage_scalars(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+    const StepParams sp = mm.sp;
+    const ForceParams fp = mm.fp;
     extern __shared__ double nrm[];   // [2 * calls] normal pairs, then the i = 0 plane [3][FW][FW]
     Clock* ck = F.clock;
     const int tid = threadIdx.x;
@@ -215,8 +225,13 @@ __global__ void __launch_bounds__(256) k_stage_scalars(FieldsT<T> F, Geo g, Step
 
 // simtime after stage s: t0 + {1/3, 3/4, 1} dt (src/pg_rk3.f90:109-127); the step
 // counter advances after stage 3.
-template <class T>
-__global__ void k_advance_time(FieldsT<T> F, Geo g, int stage) {
+template <class T, int CAP>
+__global__ void k_advance_time(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+
     Clock* ck = F.clock;
     if (stage == 1) ck->simtime = ck->t0 + (1.0 / 3.0) * ck->dt;
     else if (stage == 2) ck->simtime = ck->t0 + (3.0 / 4.0) * ck->dt;
@@ -347,8 +362,13 @@ __global__ void k_init_fluid(Fields F, Geo g, InitParams ip) {
 // dropped, BF-rot u1 += u3; the frame jumps from S t = +B110/2 to -B110/2.  The
 // step number is read on the device, so the launch sits in every step's graph
 // and returns at once on the other steps.  One CTA per row, row staged in shared memory.
-template <class T>
-__global__ void __launch_bounds__(256) k_remesh(FieldsT<T> F, Geo g) {
+template <class T, int CAP>
+__global__ void __launch_bounds__(256) k_remesh(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+
     using C = typename FieldsT<T>::C;
     Clock* ck = F.clock;
     if (!remesh_due(g, ck->tstep)) return;
@@ -381,7 +401,13 @@ __global__ void __launch_bounds__(256) k_remesh(FieldsT<T> F, Geo g) {
 }
 
 // Particle positions at the remesh (p_MPIRemeshPosition, src/pp_mpi.f90:1062-1092).
-__global__ void k_remesh_particles(Particles P, Geo g, const Clock* ck) {
+template <class T, int CAP>
+__global__ void k_remesh_particles(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const Particles P = mm.P;
+    const Geo g = mm.g;
+    const Clock* ck = mm.F.clock;
     if (!remesh_due(g, ck->tstep)) return;
     const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= P.np) return;
@@ -392,16 +418,25 @@ __global__ void k_remesh_particles(Particles P, Geo g, const Clock* ck) {
     P.xp[0][n] = x;
 }
 
+// np: particles per member (0: none)
+#define PD_CAP(S) std::decay_t<decltype(S)>::cap
 template <class T>
-cudaError_t launch_remesh(const Geo& g, const FieldsT<T>& f, const Particles& p, cudaStream_t st) {
-    if (p.np > 0) k_remesh_particles<<<(unsigned)((p.np + 255) / 256), 256, 0, st>>>(p, g, f.clock);
-    k_remesh<<<(unsigned)((long long)g.nki * g.nkj), 256, sizeof(double2) * 3 * g.nkk, st>>>(f, g);
-    return cudaGetLastError();
+cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np, cudaStream_t st) {
+    return for_member_sets(M, B, [&](const auto& ms, int nb) {
+        constexpr int CAP = PD_CAP(ms);
+        if (np > 0) k_remesh_particles<T, CAP><<<dim3((unsigned)((np + 255) / 256), nb), 256, 0, st>>>(ms);
+        k_remesh<T, CAP><<<dim3((unsigned)((long long)g.nki * g.nkj), nb), 256, sizeof(double2) * 3 * g.nkk, st>>>(ms);
+    });
 }
 
 // Non-finite check of the spectral state (sets PD_ST_NAN).
-template <class T>
-__global__ void k_check_finite(FieldsT<T> F, Geo g) {
+template <class T, int CAP>
+__global__ void k_check_finite(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+
     bool bad = false;
     for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.S;
          m += (long long)gridDim.x * blockDim.x) {
@@ -427,15 +462,21 @@ static int sm_count() {
     return n;
 }
 
-template <class T> cudaError_t launch_stats(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
+// The shell sums of every member start at zero: `shell` is the first member's
+// buffer, members' buffers are contiguous (B x shell_words).
+template <class T>
+cudaError_t launch_stats(const Geo& g, const Member<T>* M, int B, double* shell, cudaStream_t st) {
     const size_t nsh = shell_words(g);
-    cudaError_t e = cudaMemsetAsync(f.shell, 0, sizeof(double) * nsh, st);
+    cudaError_t e = cudaMemsetAsync(shell, 0, sizeof(double) * nsh * B, st);
     if (e) return e;
     long long nb = (g.S + 255) / 256;
     const long long cap = 4LL * sm_count();
     if (nb > cap) nb = cap;
-    k_stats<<<(unsigned)nb, 256, sizeof(double) * nsh, st>>>(f, g);
-    return cudaGetLastError();
+    // each launch's members take consecutive shell blocks (member i of a chunk uses its
+    // own F.shell, which the batch points into `shell`)
+    return for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_stats<T, PD_CAP(ms)><<<dim3((unsigned)nb, nm), 256, sizeof(double) * nsh, st>>>(ms);
+    });
 }
 
 // Shared memory of k_stage_scalars: the normal pairs of one stage, then the i = 0
@@ -447,21 +488,27 @@ static size_t stage_scalars_smem(const Geo& g, const ForceParams& fp) {
 
 cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp) {
     const int b = (int)stage_scalars_smem(g, fp);
-    cudaError_t e = cudaFuncSetAttribute(k_stage_scalars<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-    if (e) return e;
-    return cudaFuncSetAttribute(k_stage_scalars<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_stage_scalars<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)) ||
+        (e = cudaFuncSetAttribute(k_stage_scalars<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)) ||
+        (e = cudaFuncSetAttribute(k_stage_scalars<double, kBatchChunk>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)))
+        return e;
+    return cudaFuncSetAttribute(k_stage_scalars<float, kBatchChunk>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
 }
 
 template <class T>
-cudaError_t launch_stage_scalars(const Geo& g, const FieldsT<T>& f, const StepParams& sp, const ForceParams& fp,
-                                 int stage, cudaStream_t st) {
-    k_stage_scalars<<<1, 256, stage_scalars_smem(g, fp), st>>>(f, g, sp, fp, stage);
-    return cudaGetLastError();
+cudaError_t launch_stage_scalars(const Geo& g, const Member<T>* M, int B, const ForceParams& fp, int stage,
+                                 cudaStream_t st) {
+    return for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_stage_scalars<T, PD_CAP(ms)><<<nm, 256, stage_scalars_smem(g, fp), st>>>(ms, stage);
+    });
 }
 
-template <class T> cudaError_t launch_advance_time(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st) {
-    k_advance_time<<<1, 1, 0, st>>>(f, g, stage);
-    return cudaGetLastError();
+template <class T>
+cudaError_t launch_advance_time(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st) {
+    return for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_advance_time<T, PD_CAP(ms)><<<nm, 1, 0, st>>>(ms, stage);
+    });
 }
 
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st) {
@@ -474,21 +521,24 @@ cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& i
     return cudaGetLastError();
 }
 
-template <class T> cudaError_t launch_check_finite(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
+template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
     long long nb = (g.S + 255) / 256;
     const long long cap = 4LL * sm_count();
     if (nb > cap) nb = cap;
-    k_check_finite<<<(unsigned)nb, 256, 0, st>>>(f, g);
-    return cudaGetLastError();
+    return for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_check_finite<T, PD_CAP(ms)><<<dim3((unsigned)nb, nm), 256, 0, st>>>(ms);
+    });
 }
 
+#undef PD_CAP
+
 #define PD_INST(T)                                                                                   \
-    template cudaError_t launch_stats<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
-    template cudaError_t launch_stage_scalars<T>(const Geo&, const FieldsT<T>&, const StepParams&,   \
-                                                 const ForceParams&, int, cudaStream_t);            \
-    template cudaError_t launch_advance_time<T>(const Geo&, const FieldsT<T>&, int, cudaStream_t);   \
-    template cudaError_t launch_check_finite<T>(const Geo&, const FieldsT<T>&, cudaStream_t);        \
-    template cudaError_t launch_remesh<T>(const Geo&, const FieldsT<T>&, const Particles&, cudaStream_t);
+    template cudaError_t launch_stats<T>(const Geo&, const Member<T>*, int, double*, cudaStream_t);  \
+    template cudaError_t launch_stage_scalars<T>(const Geo&, const Member<T>*, int, const ForceParams&, int, \
+                                                 cudaStream_t);                                      \
+    template cudaError_t launch_advance_time<T>(const Geo&, const Member<T>*, int, int, cudaStream_t); \
+    template cudaError_t launch_check_finite<T>(const Geo&, const Member<T>*, int, cudaStream_t);    \
+    template cudaError_t launch_remesh<T>(const Geo&, const Member<T>*, int, long long, cudaStream_t);
 PD_INST(double)
 PD_INST(float)
 #undef PD_INST

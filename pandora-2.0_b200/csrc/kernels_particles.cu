@@ -14,6 +14,7 @@
 // so that a wave of threads reads a compact set of velocity rows that stays in
 // L2 instead of gathering at random from a field larger than L2.
 #include <cuda_runtime.h>
+#include <type_traits>
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
 
@@ -45,15 +46,21 @@ template <int ORD> constexpr int part_group() { return ORD <= 1 ? 1 : (ORD <= 2 
 
 // T: precision of the stored physical velocity (the particle state and its
 // arithmetic are FP64 in both forms).
-template <int ORD, class T>
-__global__ void __launch_bounds__(256, 2) k_particles(Particles P, Geo g, const T* __restrict__ phys,
-                                                   Clock* ck, PartParams pp, int stage) {
+template <int ORD, class T, int CAP>
+__global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     constexpr int G = part_group<ORD>();
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;                             // uniform over the CTA
+    const Particles P = mm.P;
+    const Geo g = mm.g;
+    const T* __restrict__ phys = mm.F.phys;
+    Clock* ck = mm.F.clock;
+    const PartParams pp = mm.pp;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n = t / G;
     const int sub = (int)(t % G);
     const int tstep = ck->tstep;
-    if (tstep < pp.release) return;                     // uniform over the launch
+    if (tstep < pp.release) return;                     // uniform over the member
     if (G == 1 && n >= P.np) return;
     // With G > 1 every lane of a warp reaches the shuffles: lanes past the last
     // particle (whole groups at the tail) gather for the last particle and store nothing.
@@ -331,20 +338,20 @@ __global__ void k_part_scatter(Particles src, PartSort s) {
 }
 
 template <class T>
-cudaError_t launch_particles(const Geo& g, const FieldsT<T>& f, const Particles& p, const PartParams& pp, int stage,
+cudaError_t launch_particles(const Geo& g, const Member<T>* M, int B, long long np, int order, int stage,
                              cudaStream_t st) {
-    if (p.np == 0) return cudaSuccess;
-    switch (pp.order) {
+    if (np == 0) return cudaSuccess;
+    switch (order) {
 #define PD_ORD(O)                                                                                  \
     case O:                                                                                        \
-        k_particles<O, T><<<(unsigned)((p.np * part_group<O>() + 255) / 256), 256, 0, st>>>(p, g, f.phys, \
-                                                                                       f.clock, pp, stage); \
-        break;
+        return for_member_sets(M, B, [&](const auto& ms, int nm) {                                 \
+            constexpr int CAP = std::decay_t<decltype(ms)>::cap;                                   \
+            k_particles<O, T, CAP><<<dim3((unsigned)((np * part_group<O>() + 255) / 256), nm), 256, 0, st>>>(ms, stage); \
+        });
         PD_ORD(1) PD_ORD(2) PD_ORD(3) PD_ORD(4) PD_ORD(5) PD_ORD(6)
 #undef PD_ORD
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia, cudaStream_t st) {
@@ -377,9 +384,9 @@ cudaError_t launch_particle_sort(const Geo& g, const Particles& P, const PartSor
     return e;
 }
 
-template cudaError_t launch_particles<double>(const Geo&, const FieldsT<double>&, const Particles&,
-                                             const PartParams&, int, cudaStream_t);
-template cudaError_t launch_particles<float>(const Geo&, const FieldsT<float>&, const Particles&,
-                                            const PartParams&, int, cudaStream_t);
+template cudaError_t launch_particles<double>(const Geo&, const Member<double>*, int, long long, int, int,
+                                             cudaStream_t);
+template cudaError_t launch_particles<float>(const Geo&, const Member<float>*, int, long long, int, int,
+                                            cudaStream_t);
 
 }  // namespace pd

@@ -18,6 +18,7 @@
 // pass owns whole lines per warp and needs no block barrier at all.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <type_traits>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
@@ -80,11 +81,15 @@ template <int N> constexpr int xps() {
 template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
 template <int N> constexpr int xna() { return N <= 256 ? 2 : 1; }
 
-template <int NX, class T>
-__global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(FieldsT<T> F, Geo g,
+template <int NX, class T, int CAP>
+__global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                         int want_phys,
                                                                                         int want_cfl) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
     C* smem = smem_as<C>();
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -192,11 +197,14 @@ template <class C> struct Out3 { C* p[3]; };
 // side: 3 and 4 CTAs of 256 threads per SM, without spills.
 // The per-mode arithmetic runs in FP64 registers in both forms (the FP32-mixed
 // form loads FP32 values and rounds once on the store).
-template <bool SHEAR, class T>
-__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(FieldsT<T> F, Geo g,
-                                                               const typename FieldsT<T>::C* __restrict__ nlh,
-                                                               int stage) {
+template <bool SHEAR, class T, int CAP>
+__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+    const C* __restrict__ nlh = F.yb;   // NL-hat from K5a
     const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= g.S) return;
     const int NKK = g.nkk;
@@ -282,11 +290,15 @@ template <int N> struct TCfg {
 // k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.
-template <int NZ, bool SHEAR, class T>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_inv(FieldsT<T> F, Geo g, int stage) {
+template <int NZ, bool SHEAR, class T, int CAP>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / 6];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int f = blockIdx.x, i0 = blockIdx.y * L, j = blockIdx.z;
+    const int f = blockIdx.x % 6, i0 = blockIdx.y * L, j = blockIdx.z;
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const double k2 = wvn(j, g.kj);
@@ -332,11 +344,15 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
 // [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).
-template <int NY, class T>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_inv(FieldsT<T> F, Geo g) {
+template <int NY, class T, int CAP>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 6];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z % 6;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
@@ -352,11 +368,15 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
 
 // K4: forward y transforms of NL field f = blockIdx.z, truncated to j
 // (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
-template <int NY, class T>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_fwd(FieldsT<T> F, Geo g) {
+template <int NY, class T, int CAP>
+__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_fwd(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z;
+    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z % 3;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
     const C* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
@@ -371,12 +391,18 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
 
 // K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
 // to k, stored as rows of NL-hat [c][i][j][k].
-template <int NZ, class T>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_fwd(FieldsT<T> F, Geo g,
-                                                                          Out3<typename FieldsT<T>::C> nlh) {
+template <int NZ, class T, int CAP>
+__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_fwd(const __grid_constant__ MemberSet<T, CAP> ms, int mode) {
     using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z;
+    const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z % 3;
+    // NL-hat into the y-pencil buffer, or (mode 1) into rk
+    Out3<C> nlh;
+    for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? F.rk[c] : F.yb + c * g.S;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const long long zs = (long long)g.nkj * g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
@@ -406,107 +432,133 @@ template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Lengths with batched (kBatchChunk-member) instantiations: the ensemble's sizes.
+template <int N> constexpr bool batch_len() { return N >= 32 && N <= 256; }
+
 template <class T> cudaError_t configure_kernels(const Geo& g) {
     cudaError_t e = cudaSuccess;
-#define PD_CFG(N)                                                                        \
-    if (g.nz == N) {                                                                     \
-        if ((e = set_smem(k_zpass_inv<N, false, T>, TCfg<N>::template smem<T>()))) return e; \
-        if ((e = set_smem(k_zpass_inv<N, true, T>, TCfg<N>::template smem<T>()))) return e;  \
-        if ((e = set_smem(k_zpass_fwd<N, T>, TCfg<N>::template smem<T>()))) return e;        \
-    }                                                                                    \
-    if (g.ny == N) {                                                                     \
-        if ((e = set_smem(k_ypass_inv<N, T>, TCfg<N>::template smem<T>()))) return e;        \
-        if ((e = set_smem(k_ypass_fwd<N, T>, TCfg<N>::template smem<T>()))) return e;        \
-    }                                                                                    \
-    if (g.nx == N) {                                                                     \
-        if ((e = set_smem(k_xpass<N, T>, smem_kx<N, T>()))) return e;                    \
+#define PD_CFG1(N, CAP)                                                                        \
+    if (g.nz == N) {                                                                           \
+        if ((e = set_smem(k_zpass_inv<N, false, T, CAP>, TCfg<N>::template smem<T>()))) return e; \
+        if ((e = set_smem(k_zpass_inv<N, true, T, CAP>, TCfg<N>::template smem<T>()))) return e;  \
+        if ((e = set_smem(k_zpass_fwd<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
+    }                                                                                          \
+    if (g.ny == N) {                                                                           \
+        if ((e = set_smem(k_ypass_inv<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
+        if ((e = set_smem(k_ypass_fwd<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
+    }                                                                                          \
+    if (g.nx == N) {                                                                           \
+        if ((e = set_smem(k_xpass<N, T, CAP>, smem_kx<N, T>()))) return e;                     \
     }
+#define PD_CFG(N)                                                                              \
+    PD_CFG1(N, 1)                                                                              \
+    if constexpr (batch_len<N>()) { PD_CFG1(N, kBatchChunk) }
     PD_FOR_EACH_N(PD_CFG)
 #undef PD_CFG
+#undef PD_CFG1
     return cudaSuccess;
 }
 
-template <class T> cudaError_t launch_zpass_inv(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st) {
+// Every launcher takes the batch's geometry g (grid sizes and flow type, common to
+// all members), the host array M of its B member descriptors and the stream; the
+// members go to the kernels by value, kBatchChunk per launch.
+#define PD_CAP(S) std::decay_t<decltype(S)>::cap
+
+template <class T>
+cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st) {
     switch (g.nz) {
 #define PD_L(N)                                                                                   \
-    case N: {                                                                                     \
-        const dim3 grid(6, g.nkip / L, g.nkj);                                                    \
-        if (g.shear)                                                                              \
-            k_zpass_inv<N, true, T><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, stage); \
-        else                                                                                      \
-            k_zpass_inv<N, false, T><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, stage); \
-        break;                                                                                    \
-    }
+    case N:                                                                                       \
+        return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
+            constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1 || batch_len<N>()) {                                           \
+                const dim3 grid(6 * nb, g.nkip / L, g.nkj);                                       \
+                if (g.shear)                                                                      \
+                    k_zpass_inv<N, true, T, CAP><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, stage); \
+                else                                                                              \
+                    k_zpass_inv<N, false, T, CAP><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, stage); \
+            }                                                                                     \
+        });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
-template <class T> cudaError_t launch_ypass_inv(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
+template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                                   \
     case N:                                                                                       \
-        k_ypass_inv<N, T><<<dim3(g.nkip / L, g.nz, 6), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g); \
-        break;
+        return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
+            constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1 || batch_len<N>())                                             \
+                k_ypass_inv<N, T, CAP><<<dim3(g.nkip / L, g.nz, 6 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+        });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t launch_xpass(const Geo& g, const FieldsT<T>& f, int want_phys, int want_cfl, cudaStream_t st) {
+cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys, int want_cfl, cudaStream_t st) {
     const long long lines = (long long)g.ny * g.nz;
     switch (g.nx) {
 #define PD_L(N)                                                                                   \
-    case N: {                                                                                     \
-        const long long nb = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                             \
-        k_xpass<N, T><<<(unsigned)nb, 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(f, g, want_phys, want_cfl); \
-        break;                                                                                    \
-    }
+    case N:                                                                                       \
+        return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
+            constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1 || batch_len<N>()) {                                           \
+                const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                     \
+                k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl); \
+            }                                                                                     \
+        });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
-template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const FieldsT<T>& f, cudaStream_t st) {
+template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
     switch (g.ny) {
 #define PD_L(N)                                                                                   \
     case N:                                                                                       \
-        k_ypass_fwd<N, T><<<dim3(g.nkip / L, g.nz, 3), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g); \
-        break;
+        return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
+            constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1 || batch_len<N>())                                             \
+                k_ypass_fwd<N, T, CAP><<<dim3(g.nkip / L, g.nz, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+        });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t launch_zpass_fwd_update(const Geo& g, const FieldsT<T>& f, int stage, int mode, cudaStream_t st) {
-    Out3<typename FieldsT<T>::C> nlh;
-    for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? f.rk[c] : f.yb + c * g.S;
+cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int stage, int mode, cudaStream_t st) {
+    cudaError_t e = cudaErrorInvalidValue;
     switch (g.nz) {
 #define PD_L(N)                                                                                   \
     case N:                                                                                       \
-        k_zpass_fwd<N, T><<<dim3(g.nkip / L, g.nkj, 3), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(f, g, nlh); \
+        e = for_member_sets(M, B, [&](const auto& ms, int nb) {                                   \
+            constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1 || batch_len<N>())                                             \
+                k_zpass_fwd<N, T, CAP><<<dim3(g.nkip / L, g.nkj, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, mode); \
+        });                                                                                       \
         break;
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
     }
-    cudaError_t e = cudaGetLastError();
     if (e || mode == 1) return e;
-    const unsigned nb = (unsigned)((g.S + 255) / 256);
-    if (g.shear) k_rk_update<true, T><<<nb, 256, 0, st>>>(f, g, f.yb, stage);
-    else k_rk_update<false, T><<<nb, 256, 0, st>>>(f, g, f.yb, stage);
-    return cudaGetLastError();
+    return for_member_sets(M, B, [&](const auto& ms, int nb) {
+        constexpr int CAP = PD_CAP(ms);
+        const dim3 grid((unsigned)((g.S + 255) / 256), nb);
+        if (g.shear) k_rk_update<true, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+        else k_rk_update<false, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+    });
 }
+#undef PD_CAP
 
 // conversions at the FP64 boundary of the FP32-mixed form
 __global__ void k_to_f32(const double2* __restrict__ in, float2* __restrict__ out, long long n) {
@@ -532,11 +584,11 @@ cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStre
 
 #define PD_INST(T)                                                                                       \
     template cudaError_t configure_kernels<T>(const Geo&);                                               \
-    template cudaError_t launch_zpass_inv<T>(const Geo&, const FieldsT<T>&, int, cudaStream_t);          \
-    template cudaError_t launch_ypass_inv<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
-    template cudaError_t launch_xpass<T>(const Geo&, const FieldsT<T>&, int, int, cudaStream_t);         \
-    template cudaError_t launch_ypass_fwd<T>(const Geo&, const FieldsT<T>&, cudaStream_t);               \
-    template cudaError_t launch_zpass_fwd_update<T>(const Geo&, const FieldsT<T>&, int, int, cudaStream_t);
+    template cudaError_t launch_zpass_inv<T>(const Geo&, const Member<T>*, int, int, cudaStream_t);      \
+    template cudaError_t launch_ypass_inv<T>(const Geo&, const Member<T>*, int, cudaStream_t);           \
+    template cudaError_t launch_xpass<T>(const Geo&, const Member<T>*, int, int, int, cudaStream_t);     \
+    template cudaError_t launch_ypass_fwd<T>(const Geo&, const Member<T>*, int, cudaStream_t);           \
+    template cudaError_t launch_zpass_fwd_update<T>(const Geo&, const Member<T>*, int, int, int, cudaStream_t);
 PD_INST(double)
 PD_INST(float)
 #undef PD_INST

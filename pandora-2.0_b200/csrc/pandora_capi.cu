@@ -167,6 +167,25 @@ static void release(pandora_handle* h) {
     delete h;
 }
 
+// The handle's buffers as fields of the stored precision.
+template <class T> static FieldsT<T>& fields(pandora_handle* h);
+template <> FieldsT<double>& fields<double>(pandora_handle* h) { return h->F; }
+template <> FieldsT<float>& fields<float>(pandora_handle* h) { return h->Ff; }
+
+// This simulation as a batch of one (every step kernel takes a member array).
+template <class T> static Member<T> member_of(pandora_handle* h, const FieldsT<T>& F) {
+    Member<T> m{};
+    m.F = F;
+    m.g = h->g;
+    m.P = h->P;
+    m.sp = h->sp;
+    m.fp = h->fp;
+    m.pp = h->pp;
+    m.active = 1;
+    return m;
+}
+template <class T> static Member<T> self_of(pandora_handle* h) { return member_of<T>(h, fields<T>(h)); }
+
 static int validate(const pandora_params* p) {
     if (!p) return PANDORA_ERR_INVALID_ARG;
     if (p->precision != PANDORA_PREC_FP64 && p->precision != PANDORA_PREC_FP32_MIXED) return PANDORA_ERR_UNSUPPORTED;
@@ -550,11 +569,6 @@ extern "C" int pandora_init_particles(pandora_handle* h) {
     return PANDORA_OK;
 }
 
-// The handle's buffers as fields of the stored precision.
-template <class T> static FieldsT<T>& fields(pandora_handle* h);
-template <> FieldsT<double>& fields<double>(pandora_handle* h) { return h->F; }
-template <> FieldsT<float>& fields<float>(pandora_handle* h) { return h->Ff; }
-
 // ---- stage sequencing ----
 // f_RK3Stage{s} (src/pf_rk3.f90:40-200): [s=1: statistics of the state],
 // vorticity + z pass, y pass, x pass with NL (and CFL / physical velocity),
@@ -565,60 +579,99 @@ template <> FieldsT<float>& fields<float>(pandora_handle* h) { return h->Ff; }
 // of K3 and the stage's dt) runs beside K4 and K5; the branch joins the main
 // stream before the stage clock advances.  Captured into the step graph, the
 // fork and join become graph edges.
-template <class T> static int enqueue_stage_t(pandora_handle* h, int stage, int* nlaunch) {
-    const FieldsT<T>& F = fields<T>(h);
-    const Geo& g = h->g;
+// What one stage of a batch needs: the batch's geometry, its device member array
+// of B slots, the particles per member, the shell sums (B x shell_words,
+// contiguous), the streams, and for a single simulation the particle sort and the
+// pass-timing events.
+template <class T> struct StepCtx {
+    const Geo* g;
+    const Member<T>* M;
+    int B;
+    long long np;
+    int order;
+    const ForceParams* fp;
+    double* shell;
+    cudaStream_t st, side;
+    cudaEvent_t ev_fork, ev_join;
+    const PartSort* sort;        // null: no per-step particle sort (batches)
+    const Particles* sortP;      // the particles the sort reorders
+    pandora_handle* timing;      // null: no pass timing
+};
+
+template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, int* nlaunch) {
+    const Geo& g = *c.g;
+    const Member<T>* M = c.M;
+    const int B = c.B;
     int n = 0;
-    const bool part = h->particles_on && h->P.np > 0;
+    const bool part = c.np > 0;
     if (stage == 1 && g.shear) {
-        PD_CK(launch_remesh(g, F, h->P, h->st)); n += part ? 2 : 1;
+        PD_CK(launch_remesh(g, M, B, c.np, c.st)); n += part ? 2 : 1;
     }
-    if (stage == 1 && part) {
-        PD_CK(cudaEventRecord(h->ev_fork, h->st));
-        PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
-        PD_CK(launch_particle_sort(g, h->P, h->sort, h->side, &n));
+    if (stage == 1 && part && c.sort) {
+        PD_CK(cudaEventRecord(c.ev_fork, c.st));
+        PD_CK(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+        PD_CK(launch_particle_sort(g, *c.sortP, *c.sort, c.side, &n));
     }
     if (stage == 1) {
-        FieldsT<T> Fs = F;
-        Fs.shell = h->shell_step;
-        PD_CK(launch_stats(g, Fs, h->st)); n += 1;   // one kernel (plus a memset node)
+        PD_CK(launch_stats(g, M, B, c.shell, c.st)); n += 1;   // one kernel (plus a memset node)
     }
     // instrumentation: event pair around pass `ps` (1..6) when pass timing is on
+    pandora_handle* h = c.timing;
     auto mark = [&](int ps, int end, cudaStream_t s) -> cudaError_t {
-        if (!(h->timing & (1 << (ps - 1)))) return cudaSuccess;
+        if (!h || !(h->timing & (1 << (ps - 1)))) return cudaSuccess;
         h->timed[stage - 1][ps - 1] = true;
         // External: captured as an event record node (a plain record inside a capture
         // only orders the streams and never fires the event)
         return cudaEventRecordWithFlags(h->tev[stage - 1][ps - 1][end], s, cudaEventRecordExternal);
     };
-    PD_CK(mark(1, 0, h->st));
-    PD_CK(launch_zpass_inv(g, F, stage, h->st)); n++;
-    PD_CK(mark(1, 1, h->st));
-    PD_CK(mark(2, 0, h->st));
-    PD_CK(launch_ypass_inv(g, F, h->st)); n++;
-    PD_CK(mark(2, 1, h->st));
-    PD_CK(mark(3, 0, h->st));
-    PD_CK(launch_xpass(g, F, part ? 1 : 0, stage == 1 ? 1 : 0, h->st)); n++;
-    PD_CK(mark(3, 1, h->st));
-    PD_CK(launch_stage_scalars(g, F, h->sp, h->fp, stage, h->st)); n++;
+    PD_CK(mark(1, 0, c.st));
+    PD_CK(launch_zpass_inv(g, M, B, stage, c.st)); n++;
+    PD_CK(mark(1, 1, c.st));
+    PD_CK(mark(2, 0, c.st));
+    PD_CK(launch_ypass_inv(g, M, B, c.st)); n++;
+    PD_CK(mark(2, 1, c.st));
+    PD_CK(mark(3, 0, c.st));
+    PD_CK(launch_xpass(g, M, B, part ? 1 : 0, stage == 1 ? 1 : 0, c.st)); n++;
+    PD_CK(mark(3, 1, c.st));
+    PD_CK(launch_stage_scalars(g, M, B, *c.fp, stage, c.st)); n++;
     if (part) {
-        PD_CK(cudaEventRecord(h->ev_fork, h->st));
-        PD_CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
-        PD_CK(mark(6, 0, h->side));
-        PD_CK(launch_particles(g, F, h->P, h->pp, stage, h->side)); n++;
-        PD_CK(mark(6, 1, h->side));
-        PD_CK(cudaEventRecord(h->ev_join, h->side));
+        PD_CK(cudaEventRecord(c.ev_fork, c.st));
+        PD_CK(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+        PD_CK(mark(6, 0, c.side));
+        PD_CK(launch_particles(g, M, B, c.np, c.order, stage, c.side)); n++;
+        PD_CK(mark(6, 1, c.side));
+        PD_CK(cudaEventRecord(c.ev_join, c.side));
     }
-    PD_CK(mark(4, 0, h->st));
-    PD_CK(launch_ypass_fwd(g, F, h->st)); n++;
-    PD_CK(mark(4, 1, h->st));
-    PD_CK(mark(5, 0, h->st));
-    PD_CK(launch_zpass_fwd_update(g, F, stage, 0, h->st)); n += 2;   // forward z FFT, RK update
-    PD_CK(mark(5, 1, h->st));
-    if (part) PD_CK(cudaStreamWaitEvent(h->st, h->ev_join, 0));
-    PD_CK(launch_advance_time(g, F, stage, h->st)); n++;
+    PD_CK(mark(4, 0, c.st));
+    PD_CK(launch_ypass_fwd(g, M, B, c.st)); n++;
+    PD_CK(mark(4, 1, c.st));
+    PD_CK(mark(5, 0, c.st));
+    PD_CK(launch_zpass_fwd_update(g, M, B, stage, 0, c.st)); n += 2;   // forward z FFT, RK update
+    PD_CK(mark(5, 1, c.st));
+    if (part) PD_CK(cudaStreamWaitEvent(c.st, c.ev_join, 0));
+    PD_CK(launch_advance_time(g, M, B, stage, c.st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;
+}
+
+template <class T> static int enqueue_stage_t(pandora_handle* h, int stage, int* nlaunch) {
+    const Member<T> self = self_of<T>(h);   // copied into each launch's parameters
+    StepCtx<T> c{};
+    c.g = &h->g;
+    c.M = &self;
+    c.B = 1;
+    c.np = (h->particles_on && h->P.np > 0) ? h->P.np : 0;
+    c.order = h->pp.order;
+    c.fp = &h->fp;
+    c.shell = h->shell_step;
+    c.st = h->st;
+    c.side = h->side;
+    c.ev_fork = h->ev_fork;
+    c.ev_join = h->ev_join;
+    c.sort = &h->sort;
+    c.sortP = &h->P;
+    c.timing = h;
+    return enqueue_stage_ctx(c, stage, nlaunch);
 }
 
 static int enqueue_stage(pandora_handle* h, int stage, int* nlaunch) {
@@ -751,11 +804,13 @@ extern "C" int pandora_stats(pandora_handle* h, double* ek, int32_t kkmax, doubl
     if (h->mixed) {
         FieldsT<float> Fs = h->Ff;
         Fs.shell = h->shell_now;
-        PD_CK(launch_stats(h->g, Fs, h->st));
+        const Member<float> mv = member_of<float>(h, Fs);
+        PD_CK(launch_stats(h->g, &mv, 1, h->shell_now, h->st));
     } else {
         Fields Fs = h->F;
         Fs.shell = h->shell_now;
-        PD_CK(launch_stats(h->g, Fs, h->st));
+        const Member<double> mv = member_of<double>(h, Fs);
+        PD_CK(launch_stats(h->g, &mv, 1, h->shell_now, h->st));
     }
     const size_t nsh = shell_words(h->g);
     PD_CK(cudaMemcpyAsync(h->shell_host, h->shell_now, sizeof(double) * nsh, cudaMemcpyDeviceToHost, h->st));
@@ -790,21 +845,25 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
     if (h->mixed) {
         FieldsT<float> Fn = h->Ff;
         for (int c = 0; c < 3; c++) Fn.rk[c] = (float2*)h->nlbuf + c * h->g.S;
-        PD_CK(launch_zpass_inv(h->g, Fn, 0, h->st));
-        PD_CK(launch_ypass_inv(h->g, Fn, h->st));
-        PD_CK(launch_xpass(h->g, Fn, 0, 0, h->st));
-        PD_CK(launch_ypass_fwd(h->g, Fn, h->st));
-        PD_CK(launch_zpass_fwd_update(h->g, Fn, 1, 1, h->st));
+        const Member<float> mv = member_of<float>(h, Fn);
+        const Member<float>* Mv = &mv;
+        PD_CK(launch_zpass_inv(h->g, Mv, 1, 0, h->st));
+        PD_CK(launch_ypass_inv(h->g, Mv, 1, h->st));
+        PD_CK(launch_xpass(h->g, Mv, 1, 0, 0, h->st));
+        PD_CK(launch_ypass_fwd(h->g, Mv, 1, h->st));
+        PD_CK(launch_zpass_fwd_update(h->g, Mv, 1, 1, 1, h->st));
         double2* none[3] = {nullptr, nullptr, nullptr};
         return copy_fields(h, none, Fn.rk, n1, n2, n3, false);
     }
     Fields Fn = h->F;
     for (int c = 0; c < 3; c++) Fn.rk[c] = (double2*)h->nlbuf + c * h->g.S;
-    PD_CK(launch_zpass_inv(h->g, Fn, 0, h->st));
-    PD_CK(launch_ypass_inv(h->g, Fn, h->st));
-    PD_CK(launch_xpass(h->g, Fn, 0, 0, h->st));
-    PD_CK(launch_ypass_fwd(h->g, Fn, h->st));
-    PD_CK(launch_zpass_fwd_update(h->g, Fn, 1, 1, h->st));
+    const Member<double> mv = member_of<double>(h, Fn);
+    const Member<double>* Mv = &mv;
+    PD_CK(launch_zpass_inv(h->g, Mv, 1, 0, h->st));
+    PD_CK(launch_ypass_inv(h->g, Mv, 1, h->st));
+    PD_CK(launch_xpass(h->g, Mv, 1, 0, 0, h->st));
+    PD_CK(launch_ypass_fwd(h->g, Mv, 1, h->st));
+    PD_CK(launch_zpass_fwd_update(h->g, Mv, 1, 1, 1, h->st));
     return copy3(h, Fn.rk, n1, n2, n3, (size_t)h->g.S, false);
 }
 
@@ -832,7 +891,13 @@ extern "C" int pandora_get_physical_velocity(pandora_handle* h, double* u1, doub
 extern "C" int pandora_check_status(pandora_handle* h) {
     if (!h) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(h->dev);
-    PD_CK(h->mixed ? launch_check_finite(h->g, h->Ff, h->st) : launch_check_finite(h->g, h->F, h->st));
+    if (h->mixed) {
+        const Member<float> self = self_of<float>(h);
+        PD_CK(launch_check_finite(h->g, &self, 1, h->st));
+    } else {
+        const Member<double> self = self_of<double>(h);
+        PD_CK(launch_check_finite(h->g, &self, 1, h->st));
+    }
     PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, h->st));
     PD_CK(cudaStreamSynchronize(h->st));
     const unsigned int st = h->clock_host->status;
@@ -885,21 +950,24 @@ extern "C" int pandora_pass_times(pandora_handle* h, float* ms) {
 
 template <class T> static int profile_pass_t(pandora_handle* h, int32_t pass, int32_t reps) {
     const bool part = h->particles_on && h->P.np > 0;
-    const FieldsT<T>& F = fields<T>(h);
-    FieldsT<T> Fs = F;
+    const Member<T> self = self_of<T>(h);
+    const Member<T>* M = &self;
+    FieldsT<T> Fs = fields<T>(h);
     Fs.shell = h->shell_now;
+    const Member<T> mv = member_of<T>(h, Fs);
+    const Member<T>* Mv = &mv;
     for (int r = 0; r < reps; r++) {
         switch (pass) {
-        case 1: PD_CK(launch_zpass_inv(h->g, F, 2, h->st)); break;
-        case 2: PD_CK(launch_ypass_inv(h->g, F, h->st)); break;
-        case 3: PD_CK(launch_xpass(h->g, F, part ? 1 : 0, 0, h->st)); break;
-        case 4: PD_CK(launch_ypass_fwd(h->g, F, h->st)); break;
-        case 5: PD_CK(launch_zpass_fwd_update(h->g, F, 2, 0, h->st)); break;
+        case 1: PD_CK(launch_zpass_inv(h->g, M, 1, 2, h->st)); break;
+        case 2: PD_CK(launch_ypass_inv(h->g, M, 1, h->st)); break;
+        case 3: PD_CK(launch_xpass(h->g, M, 1, part ? 1 : 0, 0, h->st)); break;
+        case 4: PD_CK(launch_ypass_fwd(h->g, M, 1, h->st)); break;
+        case 5: PD_CK(launch_zpass_fwd_update(h->g, M, 1, 2, 0, h->st)); break;
         case 6:
             if (!part) return PANDORA_ERR_INVALID_ARG;
-            PD_CK(launch_particles(h->g, F, h->P, h->pp, 2, h->st));
+            PD_CK(launch_particles(h->g, M, 1, h->P.np, h->pp.order, 2, h->st));
             break;
-        case 7: PD_CK(launch_stats(h->g, Fs, h->st)); break;
+        case 7: PD_CK(launch_stats(h->g, Mv, 1, h->shell_now, h->st)); break;
         default: return PANDORA_ERR_INVALID_ARG;
         }
     }
@@ -942,5 +1010,318 @@ extern "C" int pandora_frame(pandora_handle* h, double* bmat13, double* binv13) 
     PD_CK(cudaStreamSynchronize(h->st));
     *bmat13 = h->clock_host->b13;
     *binv13 = h->clock_host->bi13;
+    return PANDORA_OK;
+}
+
+// ===========================================================================
+// Batches of simulations (the ensemble server's device side; no counterpart in
+// the reference).  A batch holds `capacity` slots of one class: grid size,
+// precision, flow type (isotropic or BF-rot shear with its B110..B330), particles
+// per member, interpolation order and forcing radius.  Each slot is a full
+// simulation (its own fields, scratch pencils, clock, forcing and particles);
+// what may differ between members is everything else: seeds, viscosity, dt, the
+// forcing amplitude and time scale, the shear rate.  One step of the batch is a
+// CUDA graph captured once over all slots: every kernel launch of the step
+// serves every active member (the member index is a grid dimension), free slots
+// return at once, and members at different step numbers advance side by side
+// because each carries its own device clock.  Admitting or releasing a member
+// rewrites its slot's descriptor; the next step re-captures the graph with the new
+// descriptors (same topology: cudaGraphExecUpdate).
+// ===========================================================================
+struct pandora_batch {
+    pandora_params cls{};
+    Geo g{};                               // class geometry (grid sizes and flow type)
+    bool mixed = false;
+    int cap = 0;
+    int dev = 0;
+    std::vector<pandora_handle*> m;        // the slots' simulations
+    std::vector<int> active;
+    std::vector<Member<double>> md;        // slot descriptors (FP64 form)
+    std::vector<Member<float>> mf;         // slot descriptors (FP32-mixed form)
+    bool dirty = true;                     // descriptors changed since the graph was captured
+    double* shell = nullptr;               // [cap][shell_words]
+    size_t nsh = 0;
+    cudaStream_t st = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches_per_step = 0;
+};
+
+static void batch_release(pandora_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->dev);
+    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (pandora_handle* h : b->m) release(h);
+    cudaFree(b->shell);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+// The per-member parameters of a simulation (those a batch member may change).
+static void derive_member(pandora_handle* h, const pandora_params* p) {
+    h->p = *p;
+    Geo& g = h->g;
+    g.nu = p->f_nu;
+    g.shear_s = p->f_deform_s;
+    g.remesh_t = p->f_remesh_t;
+    g.rk3_decide = (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) ? 1 : 0;
+    h->sp.rk3_timestep = p->rk3_timestep; h->sp.f_type = p->f_type; h->sp.rk3_dt = p->rk3_dt;
+    h->sp.rk3_cfl = p->rk3_cfl; h->sp.force_tf = p->force_tf; h->sp.f_deform_s = p->f_deform_s;
+    h->sp.f_remesh_t = p->f_remesh_t;
+    h->fp.tf = p->force_tf; h->fp.sigma = p->force_sigma; h->fp.stop = p->force_stop;
+    h->fp.key = stream_key(p->seed_force, TAG_FORCE);
+    h->pp.release = p->p_ts_release; h->pp.f_nu = p->f_nu;
+    h->pp.p_rho = p->p_rho; h->pp.f_rho = p->f_rho;
+}
+
+// Do two parameter sets describe the same batch class?
+static bool same_class(const pandora_params* a, const pandora_params* b) {
+    const long long na = a->p_track_part ? a->p_np_global : 0, nb = b->p_track_part ? b->p_np_global : 0;
+    return a->nodes_x == b->nodes_x && a->nodes_y == b->nodes_y && a->nodes_z == b->nodes_z &&
+           a->precision == b->precision && a->f_type == b->f_type && a->ns_deformed == b->ns_deformed &&
+           a->b110 == b->b110 && a->b220 == b->b220 && a->b330 == b->b330 && a->dealiasing == b->dealiasing &&
+           na == nb && (na == 0 || a->p_interp_order == b->p_interp_order) &&
+           (int)a->force_kf == (int)b->force_kf;
+}
+
+template <class T> static Member<T> slot_member(pandora_batch* b, int slot, int on) {
+    pandora_handle* h = b->m[slot];
+    FieldsT<T> F = fields<T>(h);
+    F.shell = b->shell + (size_t)slot * b->nsh;
+    Member<T> mm = member_of<T>(h, F);
+    mm.active = on;
+    return mm;
+}
+static void set_slot(pandora_batch* b, int slot, int on) {
+    if (b->mixed) b->mf[slot] = slot_member<float>(b, slot, on);
+    else b->md[slot] = slot_member<double>(b, slot, on);
+    b->dirty = true;
+}
+
+template <class T> static int batch_enqueue_step(pandora_batch* b, int* nlaunch) {
+    StepCtx<T> c{};
+    c.g = &b->g;
+    c.M = b->mixed ? (const Member<T>*)(const void*)b->mf.data() : (const Member<T>*)(const void*)b->md.data();
+    c.B = b->cap;
+    c.np = b->cls.p_track_part ? b->cls.p_np_global : 0;
+    c.order = b->cls.p_interp_order;
+    c.fp = &b->m[0]->fp;         // only its size (the forcing radius) is used at launch
+    c.shell = b->shell;
+    c.st = b->st;
+    c.side = b->side;
+    c.ev_fork = b->ev_fork;
+    c.ev_join = b->ev_join;
+    for (int s = 1; s <= 3; s++) {
+        int rc = enqueue_stage_ctx(c, s, nlaunch);
+        if (rc) return rc;
+    }
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_bytes(const pandora_params* p, int32_t capacity, int64_t* bytes) {
+    if (!p || capacity < 1 || !bytes) return PANDORA_ERR_INVALID_ARG;
+    int rc = validate(p);
+    if (rc) return rc;
+    const long long nx = p->nodes_x, ny = p->nodes_y, nz = p->nodes_z;
+    const long long nki = nx / 3 + 1, nkj = 2 * (ny / 3) + 1, nkk = 2 * (nz / 3) + 1, nkip = (nki + 7) / 8 * 8;
+    const long long S = nki * nkj * nkk, R = nx * ny * nz;
+    const long long ce = p->precision == PANDORA_PREC_FP32_MIXED ? 8 : 16;
+    const long long np = p->p_track_part ? p->p_np_global : 0;
+    long long per = ce * 6 * S + ce * 6 * nz * nkj * nkip + ce * 6 * nz * ny * nkip + ce * (nx + ny + nz);
+    if (p->p_track_part) per += ce / 2 * 3 * R + 2 * 8 * 14 * np + 4 * np;
+    per += 1 << 20;   // clock, forcing, shells, member descriptors, allocator granularity
+    *bytes = per * capacity;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_create(const pandora_params* cls, int32_t capacity, pandora_batch** out) {
+    if (!cls || !out || capacity < 1 || capacity > 4096) return PANDORA_ERR_INVALID_ARG;
+    *out = nullptr;
+    int rc = validate(cls);
+    if (rc) return rc;
+    pandora_batch* b = new (std::nothrow) pandora_batch();
+    if (!b) return PANDORA_ERR_OOM;
+    cudaGetDevice(&b->dev);
+    b->cls = *cls;
+    b->mixed = cls->precision == PANDORA_PREC_FP32_MIXED;
+    b->cap = capacity;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming)) != cudaSuccess) {
+        batch_release(b); return cuda_fail(e, "batch streams");
+    }
+    b->m.assign(capacity, nullptr);
+    b->active.assign(capacity, 0);
+    for (int i = 0; i < capacity; i++) {
+        rc = pandora_create(cls, &b->m[i]);
+        if (rc) { batch_release(b); return rc; }
+        b->m[i]->st = b->st;      // every member's copies run in the batch's stream order
+    }
+    b->g = b->m[0]->g;
+    b->nsh = shell_words(b->g);
+    if (cudaMalloc((void**)&b->shell, sizeof(double) * b->nsh * capacity) != cudaSuccess) {
+        cudaGetLastError(); batch_release(b); return PANDORA_ERR_OOM;
+    }
+    b->md.resize(b->mixed ? 0 : capacity);
+    b->mf.resize(b->mixed ? capacity : 0);
+    for (int i = 0; i < capacity; i++) set_slot(b, i, 0);
+    if ((e = cudaStreamSynchronize(b->st)) != cudaSuccess) { batch_release(b); return cuda_fail(e, "batch"); }
+    *out = b;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_destroy(pandora_batch* b) {
+    if (!b) return PANDORA_ERR_INVALID_ARG;
+    batch_release(b);
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_capacity(pandora_batch* b, int32_t* capacity, int32_t* free_slots) {
+    if (!b) return PANDORA_ERR_INVALID_ARG;
+    int nfree = 0;
+    for (int a : b->active) nfree += a ? 0 : 1;
+    if (capacity) *capacity = b->cap;
+    if (free_slots) *free_slots = nfree;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_admit(pandora_batch* b, const pandora_params* p, int32_t* slot) {
+    if (!b || !p || !slot) return PANDORA_ERR_INVALID_ARG;
+    int rc = validate(p);
+    if (rc) return rc;
+    if (!same_class(p, &b->cls)) return PANDORA_ERR_BAD_LAYOUT;
+    int s = -1;
+    for (int i = 0; i < b->cap; i++)
+        if (!b->active[i]) { s = i; break; }
+    if (s < 0) return PANDORA_ERR_OOM;
+    cudaSetDevice(b->dev);
+    pandora_handle* h = b->m[s];
+    derive_member(h, p);
+    // a fresh simulation in the slot: zero state and registers, seeded field and
+    // particles, clock at step 1 (all in the batch's stream order)
+    PD_CK(cudaMemsetAsync(h->fbuf, 0, h->celem * 6 * (size_t)h->g.S, h->st));
+    PD_CK(cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st));
+    PD_CK(cudaMemsetAsync(h->clock, 0, sizeof(Clock), h->st));
+    rc = pandora_init_fluid(h);
+    if (rc) return rc;
+    if (h->particles_on && h->P.np > 0) {
+        rc = pandora_init_particles(h);
+        if (rc) return rc;
+    }
+    rc = set_clock(h, 1, 0.0);
+    if (rc) return rc;
+    set_slot(b, s, 1);
+    b->active[s] = 1;
+    *slot = s;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_release(pandora_batch* b, int32_t slot) {
+    if (!b || slot < 0 || slot >= b->cap || !b->active[slot]) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(b->dev);
+    set_slot(b, slot, 0);
+    b->active[slot] = 0;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_step(pandora_batch* b, int32_t nsteps) {
+    if (!b || nsteps < 0) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(b->dev);
+    if (b->dirty) {
+        // the slot descriptors are kernel parameters: capture the step again and
+        // update the executable graph (same topology) once earlier launches are done
+        PD_CK(cudaStreamSynchronize(b->st));
+        PD_CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        int n = 0;
+        int rc = b->mixed ? batch_enqueue_step<float>(b, &n) : batch_enqueue_step<double>(b, &n);
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+        if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        bool updated = false;
+        if (b->exec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(b->exec, gr, &info) == cudaSuccess;
+            if (!updated) { cudaGetLastError(); cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        }
+        if (!updated && (e = cudaGraphInstantiate(&b->exec, gr, 0)) != cudaSuccess) {
+            cudaGraphDestroy(gr);
+            return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        if (b->graph) cudaGraphDestroy(b->graph);
+        b->graph = gr;
+        b->launches_per_step = n;
+        b->dirty = false;
+    }
+    for (int i = 0; i < nsteps; i++) PD_CK(cudaGraphLaunch(b->exec, b->st));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_sync(pandora_batch* b) {
+    if (!b) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(b->dev);
+    PD_CK(cudaStreamSynchronize(b->st));
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_launches_per_step(pandora_batch* b, int32_t* n) {
+    if (!b || !n) return PANDORA_ERR_INVALID_ARG;
+    *n = b->launches_per_step;
+    return PANDORA_OK;
+}
+
+static int batch_slot(pandora_batch* b, int32_t slot, pandora_handle** h) {
+    if (!b || slot < 0 || slot >= b->cap) return PANDORA_ERR_INVALID_ARG;
+    *h = b->m[slot];
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_member_time(pandora_batch* b, int32_t slot, int32_t* tstep, double* simtime,
+                                         double* dt) {
+    pandora_handle* h;
+    int rc = batch_slot(b, slot, &h);
+    if (rc) return rc;
+    cudaSetDevice(b->dev);
+    PD_CK(cudaMemcpyAsync(h->clock_host, h->clock, sizeof(Clock), cudaMemcpyDeviceToHost, b->st));
+    PD_CK(cudaStreamSynchronize(b->st));
+    if (tstep) *tstep = h->clock_host->tstep;
+    if (simtime) *simtime = h->clock_host->simtime;
+    if (dt) *dt = h->clock_host->dt;
+    return status_to_rc(h->clock_host->status);
+}
+
+extern "C" int pandora_batch_get_state(pandora_batch* b, int32_t slot, double* u1, double* u2, double* u3) {
+    pandora_handle* h;
+    int rc = batch_slot(b, slot, &h);
+    if (rc) return rc;
+    return pandora_get_state(h, u1, u2, u3);
+}
+
+extern "C" int pandora_batch_get_particles(pandora_batch* b, int32_t slot, int64_t np, double* xp, double* up,
+                                           double* up_rk3, double* rk3, double* dp) {
+    pandora_handle* h;
+    int rc = batch_slot(b, slot, &h);
+    if (rc) return rc;
+    return pandora_get_particles(h, np, xp, up, up_rk3, rk3, dp);
+}
+
+extern "C" int pandora_batch_last_step_stats(pandora_batch* b, int32_t slot, double* ek, int32_t kkmax, double* tke,
+                                             double* eps) {
+    pandora_handle* h;
+    int rc = batch_slot(b, slot, &h);
+    if (rc) return rc;
+    cudaSetDevice(b->dev);
+    PD_CK(cudaMemcpyAsync(h->shell_host, b->shell + (size_t)slot * b->nsh, sizeof(double) * b->nsh,
+                          cudaMemcpyDeviceToHost, b->st));
+    PD_CK(cudaStreamSynchronize(b->st));
+    finish_stats(h, h->shell_host, ek, kkmax, tke, eps);
     return PANDORA_OK;
 }

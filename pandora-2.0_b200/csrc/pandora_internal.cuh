@@ -156,32 +156,83 @@ struct InitParams {
     uint64_t key;
 };
 
+// One simulation as the step kernels see it.  Every kernel of the step takes a
+// set of these as a __grid_constant__ parameter (constant bank: read at CTA start
+// without a trip to memory) and finds its member from a grid dimension, so one
+// launch serves up to kBatchChunk members of a batch (same grid size, precision and
+// flow type); a single simulation is a set of one.  A member with active == 0 (a
+// free slot) returns at once in every kernel.
+template <class T> struct Member {
+    FieldsT<T> F;
+    Geo g;
+    Particles P;
+    StepParams sp;
+    ForceParams fp;
+    PartParams pp;
+    int active;
+};
+constexpr int kBatchChunk = 32;   // members per launch of a batch (about 18 KB of parameters)
+template <class T, int CAP> struct MemberSet {
+    static constexpr int cap = CAP;
+    Member<T> m[CAP];
+};
+
 bool supported_length(int n);
 
-template <class T> cudaError_t launch_zpass_inv(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st);
-template <class T> cudaError_t launch_ypass_inv(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+// Calls f(set, n) for each chunk of at most kBatchChunk members of the B in M: a
+// MemberSet<T, 1> for a single simulation, MemberSet<T, kBatchChunk> (unused
+// entries inactive) otherwise.  f launches one kernel with the set as parameter
+// and n as the member extent of its grid.
+template <class T, class Fn> inline cudaError_t for_member_sets(const Member<T>* M, int B, Fn f) {
+    if (B == 1) {
+        MemberSet<T, 1> one;
+        one.m[0] = M[0];
+        f(one, 1);
+        return cudaGetLastError();
+    }
+    static thread_local MemberSet<T, kBatchChunk> set;   // 18 KB, copied into the launch
+    for (int c0 = 0; c0 < B; c0 += kBatchChunk) {
+        const int n = (B - c0) < kBatchChunk ? (B - c0) : kBatchChunk;
+        for (int i = 0; i < kBatchChunk; i++) {
+            if (i < n) set.m[i] = M[c0 + i];
+            else set.m[i].active = 0;
+        }
+        f(set, n);
+        cudaError_t e = cudaGetLastError();
+        if (e) return e;
+    }
+    return cudaSuccess;
+}
+
+// Launchers of the step kernels: g is the batch's geometry (grid sizes and flow
+// type, common to its members), M a host array of its B member descriptors
+// (passed by value to the kernels, kBatchChunk members per launch).
+template <class T> cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st);
+template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 template <class T>
-cudaError_t launch_xpass(const Geo& g, const FieldsT<T>& f, int want_phys, int want_cfl, cudaStream_t st);
-template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys, int want_cfl, cudaStream_t st);
+template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 template <class T>
-cudaError_t launch_zpass_fwd_update(const Geo& g, const FieldsT<T>& f, int stage, int mode, cudaStream_t st);
-template <class T> cudaError_t launch_stats(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
+cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int stage, int mode, cudaStream_t st);
 template <class T>
-cudaError_t launch_stage_scalars(const Geo& g, const FieldsT<T>& f, const StepParams& sp,
-                                 const ForceParams& fp, int stage, cudaStream_t st);
-template <class T> cudaError_t launch_advance_time(const Geo& g, const FieldsT<T>& f, int stage, cudaStream_t st);
-// The initial field is generated in FP64 (the FP32-mixed form converts it).
+cudaError_t launch_stats(const Geo& g, const Member<T>* M, int B, double* shell, cudaStream_t st);
+template <class T>
+cudaError_t launch_stage_scalars(const Geo& g, const Member<T>* M, int B, const ForceParams& fp, int stage,
+                                 cudaStream_t st);
+template <class T> cudaError_t launch_advance_time(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st);
+template <class T>
+cudaError_t launch_particles(const Geo& g, const Member<T>* M, int B, long long np, int order, int stage,
+                             cudaStream_t st);
+template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
+template <class T>
+cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np, cudaStream_t st);
+// Per simulation (not batched): initial field (generated in FP64; the FP32-mixed
+// form converts it), particle initialisation and the per-step spatial sort.
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);
-template <class T>
-cudaError_t launch_particles(const Geo& g, const FieldsT<T>& f, const Particles& p, const PartParams& pp,
-                             int stage, cudaStream_t st);
 cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia,
                                   cudaStream_t st);
 cudaError_t launch_particle_sort(const Geo& g, const Particles& p, const PartSort& s, cudaStream_t st,
                                  int* nlaunch);
-template <class T> cudaError_t launch_check_finite(const Geo& g, const FieldsT<T>& f, cudaStream_t st);
-template <class T>
-cudaError_t launch_remesh(const Geo& g, const FieldsT<T>& f, const Particles& p, cudaStream_t st);
 // n complex values from one precision to the other (FP64 <-> FP32 at the boundary).
 cudaError_t launch_convert(const double2* in, float2* out, long long n, cudaStream_t st);
 cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStream_t st);

@@ -124,10 +124,15 @@ extern "C" int pandora_nonlinear_static(const pandora_params* p, const double* u
     F.yb = sp->yb;
     F.tw_x = sp->tw; F.tw_y = sp->tw + nx; F.tw_z = sp->tw + nx + ny;
     F.clock = sp->clock;
+    pd::Member<double> m{};
+    m.F = F;
+    m.g = g;
+    m.active = 1;
+    const pd::Member<double>* M = &m;   // passed to the kernels by value
     // the same five passes as the step, with the last one storing NL-hat instead of updating
-    if (pd::launch_zpass_inv(g, F, 0, st) != cudaSuccess || pd::launch_ypass_inv(g, F, st) != cudaSuccess ||
-        pd::launch_xpass(g, F, 0, 0, st) != cudaSuccess || pd::launch_ypass_fwd(g, F, st) != cudaSuccess ||
-        pd::launch_zpass_fwd_update(g, F, 1, 1, st) != cudaSuccess) {
+    if (pd::launch_zpass_inv(g, M, 1, 0, st) != cudaSuccess || pd::launch_ypass_inv(g, M, 1, st) != cudaSuccess ||
+        pd::launch_xpass(g, M, 1, 0, 0, st) != cudaSuccess || pd::launch_ypass_fwd(g, M, 1, st) != cudaSuccess ||
+        pd::launch_zpass_fwd_update(g, M, 1, 1, 1, st) != cudaSuccess) {
         cudaGetLastError();
         return PANDORA_ERR_CUDA;
     }

@@ -4,3 +4,4 @@ from .params import (PREC_FP32_MIXED, PREC_FP64, Params, default_params, read_na
                      workload_params)
 from .rk3 import (Simulation, ProgramInit, f_FluidstatsFs, f_InitialiseInit, f_RK3Stage1,  # noqa: F401
                   f_RK3Stage2, f_RK3Stage3, g_RK3Calc, p_ControlInitialiseParticles)
+from .batch import Batch, batch_bytes, class_key  # noqa: F401

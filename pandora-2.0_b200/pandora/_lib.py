@@ -77,6 +77,19 @@ SIGNATURES = {
     "pandora_pass_times": [_vp, ctypes.POINTER(ctypes.c_float)],
     "pandora_frame": [_vp, _dp, _dp],
     "pandora_nonlinear_static": [ctypes.POINTER(Params), _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pandora_batch_bytes": [ctypes.POINTER(Params), _i32, ctypes.POINTER(_i64)],
+    "pandora_batch_create": [ctypes.POINTER(Params), _i32, ctypes.POINTER(_vp)],
+    "pandora_batch_destroy": [_vp],
+    "pandora_batch_capacity": [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)],
+    "pandora_batch_admit": [_vp, ctypes.POINTER(Params), ctypes.POINTER(_i32)],
+    "pandora_batch_release": [_vp, _i32],
+    "pandora_batch_step": [_vp, _i32],
+    "pandora_batch_sync": [_vp],
+    "pandora_batch_launches_per_step": [_vp, ctypes.POINTER(_i32)],
+    "pandora_batch_member_time": [_vp, _i32, ctypes.POINTER(_i32), _dp, _dp],
+    "pandora_batch_get_state": [_vp, _i32, _dp, _dp, _dp],
+    "pandora_batch_get_particles": [_vp, _i32, _i64, _dp, _dp, _dp, _dp, _dp],
+    "pandora_batch_last_step_stats": [_vp, _i32, _dp, _i32, _dp, _dp],
 }
 _RESTYPES = {"pandora_strerror": ctypes.c_char_p}
 

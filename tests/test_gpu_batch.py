@@ -1,0 +1,104 @@
+"""Batches (pandora_batch_*): every member's result equals the same simulation run
+alone, bit for bit -- whatever else shares its launches, and whenever it was
+admitted (continuous batching: members at different step numbers advance in the
+same launches)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(pandora, p, nsteps):
+    with pandora.Simulation(p) as s:
+        s.init_fluid()
+        if p.p_track_part and p.p_np_global > 0:
+            s.init_particles()
+        for k in range(1, nsteps + 1):
+            s.step(k)
+        u = s.get_state()
+        xp = s.get_particles()[0] if p.p_track_part and p.p_np_global > 0 else None
+    return u, xp
+
+
+def _member(base, seed, nu=None):
+    q = base.copy()
+    q.seed_fluid, q.seed_force, q.seed_particles = seed, 1000 + seed, 2000 + seed
+    if nu is not None:
+        q.f_nu = nu
+    return q
+
+
+def _same(a, b):
+    return all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_batch_members_equal_alone_runs(gpu_lib):
+    base = gpu_lib.workload_params("iso_decay", 32)
+    members = [_member(base, 11, 0.01), _member(base, 12, 0.02), _member(base, 13, 0.005)]
+    late = _member(base, 14, 0.015)
+    with gpu_lib.Batch(base, 5) as b:
+        slots = [b.admit(q) for q in members]
+        b.step(4)
+        sl = b.admit(late)                # joins while the others are at step 5
+        b.step(6)
+        b.sync()
+        assert b.member_time(slots[0])[0] == 11 and b.member_time(sl)[0] == 7
+        for q, s in zip(members, slots):
+            assert _same(b.get_state(s), _alone(gpu_lib, q, 10)[0])
+        assert _same(b.get_state(sl), _alone(gpu_lib, late, 6)[0])
+
+
+def test_batch_two_launch_chunks_particles(gpu_lib):
+    """34 slots (two launches of up to 32 members), forced flow with 256 tracers."""
+    base = gpu_lib.workload_params("iso_forced_particles", 32)
+    base.p_np_global = 256
+    with gpu_lib.Batch(base, 34) as b:
+        slots = [b.admit(_member(base, 100 + k)) for k in range(34)]
+        b.step(3)
+        b.sync()
+        for k in (0, 31, 32, 33):
+            u, xp = _alone(gpu_lib, _member(base, 100 + k), 3)
+            assert _same(b.get_state(slots[k]), u), k
+            assert np.array_equal(b.get_particles(slots[k])[0], xp), k
+
+
+def test_batch_mixed_precision_and_slot_reuse(gpu_lib):
+    base = gpu_lib.workload_params("iso_decay", 48)
+    base.precision = gpu_lib.PREC_FP32_MIXED
+    with gpu_lib.Batch(base, 2) as b:
+        s0 = b.admit(_member(base, 21))
+        s1 = b.admit(_member(base, 22))
+        b.step(3)
+        b.release(s0)
+        s2 = b.admit(_member(base, 23))      # reuses the slot: a fresh simulation
+        b.step(2)
+        b.sync()
+        assert _same(b.get_state(s1), _alone(gpu_lib, _member(base, 22), 5)[0])
+        assert _same(b.get_state(s2), _alone(gpu_lib, _member(base, 23), 2)[0])
+
+
+def test_batch_shear_across_remesh(gpu_lib):
+    base = gpu_lib.workload_params("shear", 32)
+    base.p_track_part = 0
+    base.f_remesh_t = 2                      # remesh at step 5
+    with gpu_lib.Batch(base, 2) as b:
+        s0 = b.admit(_member(base, 31))
+        b.step(2)
+        s1 = b.admit(_member(base, 32))
+        b.step(5)
+        b.sync()
+        assert _same(b.get_state(s0), _alone(gpu_lib, _member(base, 31), 7)[0])
+        assert _same(b.get_state(s1), _alone(gpu_lib, _member(base, 32), 5)[0])
+        ek, tke, eps = b.last_step_stats(s0)
+        assert tke > 0 and eps > 0 and np.all(np.isfinite(ek))
+
+
+def test_batch_rejects_other_class_and_full(gpu_lib):
+    base = gpu_lib.workload_params("iso_decay", 32)
+    with gpu_lib.Batch(base, 1) as b:
+        other = gpu_lib.workload_params("iso_decay", 48)
+        with pytest.raises(gpu_lib.PandoraError):
+            b.admit(other)
+        b.admit(_member(base, 1))
+        with pytest.raises(gpu_lib.PandoraError):
+            b.admit(_member(base, 2))
