@@ -248,7 +248,9 @@ int pandora_pass_times(pandora_handle* h, float* ms);
  * launch serves up to 32 members, and members admitted at different times advance
  * side by side, each with its own step counter and time.  Results are those of
  * the same simulation run alone (the kernels do the same arithmetic per member).
- * All calls on one batch run in its stream order; the batch is not re-entrant.
+ * All calls on one batch run in its stream order and, except the readers
+ * (member_time, get_state, get_particles, last_step_stats, sync), none waits on
+ * the host; the batch is not re-entrant.
  */
 typedef struct pandora_batch pandora_batch;
 /* Device bytes a batch of this class and capacity allocates (for admission control). */
@@ -257,12 +259,23 @@ int pandora_batch_create(const pandora_params* cls, int32_t capacity, pandora_ba
 int pandora_batch_destroy(pandora_batch* b);
 int pandora_batch_capacity(pandora_batch* b, int32_t* capacity, int32_t* free_slots);
 /* Start a member in a free slot: seeded initial field (and particles), step 1 at
- * time 0.  PANDORA_ERR_BAD_LAYOUT if `member` is not of the batch's class,
- * PANDORA_ERR_OOM if no slot is free. */
+ * time 0.  *slot < 0 on entry: any free slot; else that slot (it must be free).
+ * PANDORA_ERR_BAD_LAYOUT if `member` is not of the batch's class, PANDORA_ERR_OOM
+ * if no slot is free. */
 int pandora_batch_admit(pandora_batch* b, const pandora_params* member, int32_t* slot);
+/* Free a slot (in stream order; its member stops after the work already enqueued). */
 int pandora_batch_release(pandora_batch* b, int32_t slot);
-/* Enqueue nsteps RK3 steps of every occupied slot (asynchronous). */
-int pandora_batch_step(pandora_batch* b, int32_t nsteps);
+/* Free a slot and keep its member's last-step statistics: enqueues the copy of its
+ * shell sums to pinned host memory, then marks the slot free; *ticket completes
+ * when both are done (pandora_batch_ticket_done), after which
+ * pandora_batch_result_stats reads them without waiting.  Never waits itself. */
+int pandora_batch_finish(pandora_batch* b, int32_t slot, int64_t* ticket);
+int pandora_batch_result_stats(pandora_batch* b, int32_t slot, double* ek, int32_t kkmax, double* tke,
+                               double* eps);
+/* Enqueue nsteps RK3 steps of every occupied slot (asynchronous); *ticket (may be
+ * null) completes when they are done. */
+int pandora_batch_step(pandora_batch* b, int32_t nsteps, int64_t* ticket);
+int pandora_batch_ticket_done(pandora_batch* b, int64_t ticket, int32_t* done);
 int pandora_batch_sync(pandora_batch* b);
 int pandora_batch_launches_per_step(pandora_batch* b, int32_t* n);
 /* Next step number, time and dt of a slot's member (waits for the batch). */

@@ -29,6 +29,9 @@ template <class T, int CAP>
 __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet<T, CAP> ms) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     extern __shared__ double sh[];
@@ -122,6 +125,9 @@ template <class T, int CAP>
 __global__ void __launch_bounds__(256) k_stage_scalars(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     const StepParams sp = mm.sp;
@@ -229,6 +235,9 @@ template <class T, int CAP>
 __global__ void k_advance_time(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
 
@@ -241,6 +250,28 @@ __global__ void k_advance_time(const __grid_constant__ MemberSet<T, CAP> ms, int
         ck->t0 = ck->simtime;
         ck->tstep += 1;
     }
+}
+
+// A fresh clock (step tstep at time t, frame tensors b13 / bi13), set on the
+// device in stream order with the values as launch parameters.
+__global__ void k_reset_clock(Clock* ck, int tstep, double t, double b13, double bi13) {
+    Clock c{};
+    c.tstep = tstep;
+    c.simtime = t;
+    c.t0 = t;
+    c.b13 = b13;
+    c.bi13 = bi13;
+    *ck = c;
+}
+cudaError_t launch_reset_clock(Clock* ck, int tstep, double t, double b13, double bi13, cudaStream_t st) {
+    k_reset_clock<<<1, 1, 0, st>>>(ck, tstep, t, b13, bi13);
+    return cudaGetLastError();
+}
+// Marks a batch slot free (batched kernels skip it from the next launch on).
+__global__ void k_set_idle(Clock* ck) { ck->status |= PD_ST_IDLE; }
+cudaError_t launch_set_idle(Clock* ck, cudaStream_t st) {
+    k_set_idle<<<1, 1, 0, st>>>(ck);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -366,6 +397,9 @@ template <class T, int CAP>
 __global__ void __launch_bounds__(256) k_remesh(const __grid_constant__ MemberSet<T, CAP> ms) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
 
@@ -405,6 +439,9 @@ template <class T, int CAP>
 __global__ void k_remesh_particles(const __grid_constant__ MemberSet<T, CAP> ms) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const Particles P = mm.P;
     const Geo g = mm.g;
     const Clock* ck = mm.F.clock;
@@ -434,6 +471,9 @@ template <class T, int CAP>
 __global__ void k_check_finite(const __grid_constant__ MemberSet<T, CAP> ms) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
 

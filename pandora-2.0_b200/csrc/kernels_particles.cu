@@ -50,7 +50,10 @@ template <int ORD, class T, int CAP>
 __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     constexpr int G = part_group<ORD>();
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
-    if (!mm.active) return;                             // uniform over the CTA
+    if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }                             // uniform over the CTA
     const Particles P = mm.P;
     const Geo g = mm.g;
     const T* __restrict__ phys = mm.F.phys;

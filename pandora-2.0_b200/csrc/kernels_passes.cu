@@ -88,6 +88,9 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
@@ -202,6 +205,9 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_c
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     const C* __restrict__ nlh = F.yb;   // NL-hat from K5a
@@ -295,6 +301,9 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / 6];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
@@ -349,6 +358,9 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 6];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
@@ -373,6 +385,9 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
@@ -396,6 +411,9 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();

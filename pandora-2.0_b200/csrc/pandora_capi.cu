@@ -488,9 +488,8 @@ extern "C" int pandora_state_device_ptrs(pandora_handle* h, void** u1, void** u2
     return PANDORA_OK;
 }
 
-extern "C" int pandora_init_fluid(pandora_handle* h) {
-    if (!h) return PANDORA_ERR_INVALID_ARG;
-    cudaSetDevice(h->dev);
+// The seeded initial field, enqueued on the handle's stream (no host wait).
+static int init_fluid_async(pandora_handle* h) {
     InitParams ip{};
     ip.type = h->p.f_init_type; ip.u0 = h->p.f_init_u0; ip.kp = h->p.f_init_kp; ip.kv = h->p.f_init_kv;
     ip.kstart = h->p.f_init_kstart; ip.kend = h->p.f_init_kend; ip.epsilon = h->p.f_init_epsilon;
@@ -505,6 +504,14 @@ extern "C" int pandora_init_fluid(pandora_handle* h) {
     } else {
         PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
     }
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_init_fluid(pandora_handle* h) {
+    if (!h) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    int rc = init_fluid_async(h);
+    if (rc) return rc;
     PD_CK(cudaStreamSynchronize(h->st));
     return PANDORA_OK;
 }
@@ -1022,11 +1029,15 @@ extern "C" int pandora_frame(pandora_handle* h, double* bmat13, double* binv13) 
 // what may differ between members is everything else: seeds, viscosity, dt, the
 // forcing amplitude and time scale, the shear rate.  One step of the batch is a
 // CUDA graph captured once over all slots: every kernel launch of the step
-// serves every active member (the member index is a grid dimension), free slots
-// return at once, and members at different step numbers advance side by side
-// because each carries its own device clock.  Admitting or releasing a member
-// rewrites its slot's descriptor; the next step re-captures the graph with the new
-// descriptors (same topology: cudaGraphExecUpdate).
+// serves every member (the member index is a grid dimension), and members at
+// different step numbers advance side by side because each carries its own device
+// clock.  Free slots carry an idle bit in their device clock and return at once.
+// Admitting a member (seeding, clock reset) and finishing one (idle bit, copy of
+// its statistics to pinned host memory) are enqueued in the batch's stream order
+// and never wait on the host; the slot descriptors (kernel parameters) change, and
+// the graph is re-captured, only when a member's constant parameters differ from
+// those of its slot.  Every step and finish call records a ticket (an event) the
+// host can poll.
 // ===========================================================================
 struct pandora_batch {
     pandora_params cls{};
@@ -1039,6 +1050,11 @@ struct pandora_batch {
     std::vector<Member<double>> md;        // slot descriptors (FP64 form)
     std::vector<Member<float>> mf;         // slot descriptors (FP32-mixed form)
     bool dirty = true;                     // descriptors changed since the graph was captured
+    std::vector<pandora_params> slot_p;    // the parameters each slot's descriptor was built from
+    double* shell_host = nullptr;          // pinned [cap][shell_words]: statistics of finished members
+    static constexpr int kTickets = 512;
+    cudaEvent_t ev[kTickets] = {};
+    long long ticket = 0;                  // number of tickets recorded
     double* shell = nullptr;               // [cap][shell_words]
     size_t nsh = 0;
     cudaStream_t st = nullptr, side = nullptr;
@@ -1055,6 +1071,9 @@ static void batch_release(pandora_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (pandora_handle* h : b->m) release(h);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->shell_host) cudaFreeHost(b->shell_host);
     cudaFree(b->shell);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
@@ -1098,10 +1117,31 @@ template <class T> static Member<T> slot_member(pandora_batch* b, int slot, int 
     mm.active = on;
     return mm;
 }
-static void set_slot(pandora_batch* b, int slot, int on) {
-    if (b->mixed) b->mf[slot] = slot_member<float>(b, slot, on);
-    else b->md[slot] = slot_member<double>(b, slot, on);
+// Do two members of a class give the same slot descriptor?  (The descriptor holds
+// the slot's buffers and the member's constant parameters: viscosity, time step,
+// shear rate, forcing -- its random key only where forcing runs -- and particle
+// properties; seeds of the initial field and particles are not in it.)
+static bool same_descriptor(const pandora_params& a, const pandora_params& b) {
+    const bool fa = a.force_stop > 0, fb = b.force_stop > 0;
+    return a.f_nu == b.f_nu && a.f_deform_s == b.f_deform_s && a.f_remesh_t == b.f_remesh_t &&
+           a.rk3_timestep == b.rk3_timestep && a.rk3_dt == b.rk3_dt && a.rk3_cfl == b.rk3_cfl &&
+           a.force_stop == b.force_stop && (!fa || (a.force_tf == b.force_tf && a.force_sigma == b.force_sigma &&
+                                                     a.seed_force == b.seed_force)) &&
+           fa == fb && a.p_ts_release == b.p_ts_release && a.p_rho == b.p_rho && a.f_rho == b.f_rho;
+}
+// The slot's descriptor for the member now in it (re-capture only if it changed).
+static void set_slot(pandora_batch* b, int slot, bool force = false) {
+    pandora_handle* h = b->m[slot];
+    if (!force && same_descriptor(b->slot_p[slot], h->p)) return;
+    b->slot_p[slot] = h->p;
+    if (b->mixed) b->mf[slot] = slot_member<float>(b, slot, 1);
+    else b->md[slot] = slot_member<double>(b, slot, 1);
     b->dirty = true;
+}
+static cudaError_t record_ticket(pandora_batch* b) {
+    const cudaError_t e = cudaEventRecord(b->ev[b->ticket % pandora_batch::kTickets], b->st);
+    if (e == cudaSuccess) b->ticket++;
+    return e;
 }
 
 template <class T> static int batch_enqueue_step(pandora_batch* b, int* nlaunch) {
@@ -1167,12 +1207,21 @@ extern "C" int pandora_batch_create(const pandora_params* cls, int32_t capacity,
     }
     b->g = b->m[0]->g;
     b->nsh = shell_words(b->g);
-    if (cudaMalloc((void**)&b->shell, sizeof(double) * b->nsh * capacity) != cudaSuccess) {
+    if (cudaMalloc((void**)&b->shell, sizeof(double) * b->nsh * capacity) != cudaSuccess ||
+        cudaMallocHost((void**)&b->shell_host, sizeof(double) * b->nsh * capacity) != cudaSuccess) {
         cudaGetLastError(); batch_release(b); return PANDORA_ERR_OOM;
     }
+    for (cudaEvent_t& ev : b->ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) {
+            batch_release(b); return cuda_fail(e, "batch events");
+        }
     b->md.resize(b->mixed ? 0 : capacity);
     b->mf.resize(b->mixed ? capacity : 0);
-    for (int i = 0; i < capacity; i++) set_slot(b, i, 0);
+    b->slot_p.assign(capacity, *cls);
+    for (int i = 0; i < capacity; i++) {
+        set_slot(b, i, true);
+        if ((e = launch_set_idle(b->m[i]->clock, b->st)) != cudaSuccess) { batch_release(b); return cuda_fail(e, "idle"); }
+    }
     if ((e = cudaStreamSynchronize(b->st)) != cudaSuccess) { batch_release(b); return cuda_fail(e, "batch"); }
     *out = b;
     return PANDORA_OK;
@@ -1199,26 +1248,30 @@ extern "C" int pandora_batch_admit(pandora_batch* b, const pandora_params* p, in
     if (rc) return rc;
     if (!same_class(p, &b->cls)) return PANDORA_ERR_BAD_LAYOUT;
     int s = -1;
-    for (int i = 0; i < b->cap; i++)
-        if (!b->active[i]) { s = i; break; }
+    if (*slot >= 0) {              // the caller's choice of a free slot
+        if (*slot >= b->cap || b->active[*slot]) return PANDORA_ERR_INVALID_ARG;
+        s = *slot;
+    } else {
+        for (int i = 0; i < b->cap; i++)
+            if (!b->active[i]) { s = i; break; }
+    }
     if (s < 0) return PANDORA_ERR_OOM;
     cudaSetDevice(b->dev);
     pandora_handle* h = b->m[s];
     derive_member(h, p);
     // a fresh simulation in the slot: zero state and registers, seeded field and
-    // particles, clock at step 1 (all in the batch's stream order)
+    // particles, clock at step 1 (all in the batch's stream order, no host wait)
     PD_CK(cudaMemsetAsync(h->fbuf, 0, h->celem * 6 * (size_t)h->g.S, h->st));
     PD_CK(cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st));
-    PD_CK(cudaMemsetAsync(h->clock, 0, sizeof(Clock), h->st));
-    rc = pandora_init_fluid(h);
+    rc = init_fluid_async(h);
     if (rc) return rc;
-    if (h->particles_on && h->P.np > 0) {
-        rc = pandora_init_particles(h);
-        if (rc) return rc;
-    }
-    rc = set_clock(h, 1, 0.0);
-    if (rc) return rc;
-    set_slot(b, s, 1);
+    if (h->particles_on && h->P.np > 0)
+        PD_CK(launch_init_particles(h->g, h->P, stream_key(p->seed_particles, TAG_PART), p->p_dia_vals, h->st));
+    // clock of step 1 at time 0 (frame of the initial state for shear)
+    double b13 = 0.0, bi13 = 0.0;
+    if (h->g.shear) update_b(h->g, 0, 0.0, b13, bi13);
+    PD_CK(launch_reset_clock(h->clock, 1, 0.0, b13, bi13, h->st));
+    set_slot(b, s);
     b->active[s] = 1;
     *slot = s;
     return PANDORA_OK;
@@ -1227,12 +1280,41 @@ extern "C" int pandora_batch_admit(pandora_batch* b, const pandora_params* p, in
 extern "C" int pandora_batch_release(pandora_batch* b, int32_t slot) {
     if (!b || slot < 0 || slot >= b->cap || !b->active[slot]) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(b->dev);
-    set_slot(b, slot, 0);
+    PD_CK(launch_set_idle(b->m[slot]->clock, b->st));
     b->active[slot] = 0;
     return PANDORA_OK;
 }
 
-extern "C" int pandora_batch_step(pandora_batch* b, int32_t nsteps) {
+extern "C" int pandora_batch_finish(pandora_batch* b, int32_t slot, int64_t* ticket) {
+    if (!b || slot < 0 || slot >= b->cap || !b->active[slot]) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(b->dev);
+    PD_CK(cudaMemcpyAsync(b->shell_host + (size_t)slot * b->nsh, b->shell + (size_t)slot * b->nsh,
+                          sizeof(double) * b->nsh, cudaMemcpyDeviceToHost, b->st));
+    PD_CK(launch_set_idle(b->m[slot]->clock, b->st));
+    PD_CK(record_ticket(b));
+    b->active[slot] = 0;
+    if (ticket) *ticket = b->ticket - 1;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_ticket_done(pandora_batch* b, int64_t ticket, int32_t* done) {
+    if (!b || !done || ticket < 0 || ticket >= b->ticket) return PANDORA_ERR_INVALID_ARG;
+    if (b->ticket - ticket > pandora_batch::kTickets) { *done = 1; return PANDORA_OK; }   // long retired
+    const cudaError_t e = cudaEventQuery(b->ev[ticket % pandora_batch::kTickets]);
+    if (e == cudaErrorNotReady) { cudaGetLastError(); *done = 0; return PANDORA_OK; }
+    PD_CK(e);
+    *done = 1;
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_result_stats(pandora_batch* b, int32_t slot, double* ek, int32_t kkmax, double* tke,
+                                          double* eps) {
+    if (!b || slot < 0 || slot >= b->cap) return PANDORA_ERR_INVALID_ARG;
+    finish_stats(b->m[slot], b->shell_host + (size_t)slot * b->nsh, ek, kkmax, tke, eps);
+    return PANDORA_OK;
+}
+
+extern "C" int pandora_batch_step(pandora_batch* b, int32_t nsteps, int64_t* ticket) {
     if (!b || nsteps < 0) return PANDORA_ERR_INVALID_ARG;
     cudaSetDevice(b->dev);
     if (b->dirty) {
@@ -1262,6 +1344,8 @@ extern "C" int pandora_batch_step(pandora_batch* b, int32_t nsteps) {
         b->dirty = false;
     }
     for (int i = 0; i < nsteps; i++) PD_CK(cudaGraphLaunch(b->exec, b->st));
+    PD_CK(record_ticket(b));
+    if (ticket) *ticket = b->ticket - 1;
     return PANDORA_OK;
 }
 

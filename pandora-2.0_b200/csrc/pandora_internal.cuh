@@ -50,6 +50,7 @@ enum : unsigned int {
     PD_ST_POLAR = 2u,       // bounded polar rejection loop gave up
     PD_ST_LOST = 4u,        // particle outside the domain after the wrap
     PD_ST_TIMEOUT = 8u,
+    PD_ST_IDLE = 16u,       // batch slot without a member: batched kernels return at once
 };
 
 // ---- project RNG (SplitMix64 finaliser over a stream index; the oracle
@@ -229,6 +230,8 @@ cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np,
 // Per simulation (not batched): initial field (generated in FP64; the FP32-mixed
 // form converts it), particle initialisation and the per-step spatial sort.
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);
+cudaError_t launch_reset_clock(Clock* ck, int tstep, double t, double b13, double bi13, cudaStream_t st);
+cudaError_t launch_set_idle(Clock* ck, cudaStream_t st);
 cudaError_t launch_init_particles(const Geo& g, const Particles& p, uint64_t key, double dia,
                                   cudaStream_t st);
 cudaError_t launch_particle_sort(const Geo& g, const Particles& p, const PartSort& s, cudaStream_t st,

@@ -83,7 +83,10 @@ SIGNATURES = {
     "pandora_batch_capacity": [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i32)],
     "pandora_batch_admit": [_vp, ctypes.POINTER(Params), ctypes.POINTER(_i32)],
     "pandora_batch_release": [_vp, _i32],
-    "pandora_batch_step": [_vp, _i32],
+    "pandora_batch_step": [_vp, _i32, ctypes.POINTER(_i64)],
+    "pandora_batch_finish": [_vp, _i32, ctypes.POINTER(_i64)],
+    "pandora_batch_ticket_done": [_vp, _i64, ctypes.POINTER(_i32)],
+    "pandora_batch_result_stats": [_vp, _i32, _dp, _i32, _dp, _dp],
     "pandora_batch_sync": [_vp],
     "pandora_batch_launches_per_step": [_vp, ctypes.POINTER(_i32)],
     "pandora_batch_member_time": [_vp, _i32, ctypes.POINTER(_i32), _dp, _dp],

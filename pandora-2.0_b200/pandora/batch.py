@@ -71,19 +71,46 @@ class Batch:
         except Exception:
             pass
 
-    def admit(self, p: Params) -> int:
+    def admit(self, p: Params, slot: int | None = None) -> int:
+        """Start a member (in `slot`, or the first free slot); returns the slot."""
         q = p.copy()
-        s = ctypes.c_int32()
+        s = ctypes.c_int32(-1 if slot is None else slot)
         _lib.check(self.L.pandora_batch_admit(self.h, ctypes.byref(q), ctypes.byref(s)), "pandora_batch_admit")
-        self.free.remove(s.value)
+        if s.value in self.free:
+            self.free.remove(s.value)
         return s.value
 
     def release(self, slot: int) -> None:
         _lib.check(self.L.pandora_batch_release(self.h, slot), "pandora_batch_release")
         self.free.append(slot)
 
-    def step(self, n: int = 1) -> None:
-        _lib.check(self.L.pandora_batch_step(self.h, n), "pandora_batch_step")
+    def step(self, n: int = 1) -> int:
+        """Enqueue n steps of every member; returns a ticket (see ``done``)."""
+        t = ctypes.c_int64()
+        _lib.check(self.L.pandora_batch_step(self.h, n, ctypes.byref(t)), "pandora_batch_step")
+        return t.value
+
+    def finish(self, slot: int) -> int:
+        """Free the slot, keeping its member's last-step statistics (``result_stats``
+        once the returned ticket is done).  Does not wait."""
+        t = ctypes.c_int64()
+        _lib.check(self.L.pandora_batch_finish(self.h, slot, ctypes.byref(t)), "pandora_batch_finish")
+        return t.value      # the slot rejoins ``free`` through ``reuse`` once its result is read
+
+    def reuse(self, slot: int) -> None:
+        self.free.append(slot)
+
+    def done(self, ticket: int) -> bool:
+        d = ctypes.c_int32()
+        _lib.check(self.L.pandora_batch_ticket_done(self.h, ticket, ctypes.byref(d)), "pandora_batch_ticket_done")
+        return bool(d.value)
+
+    def result_stats(self, slot: int):
+        ek = np.zeros(self.kkmax)
+        tke, eps = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.L.pandora_batch_result_stats(self.h, slot, _ptr(ek), self.kkmax, ctypes.byref(tke),
+                                                     ctypes.byref(eps)), "pandora_batch_result_stats")
+        return ek, tke.value, eps.value
 
     def sync(self) -> None:
         _lib.check(self.L.pandora_batch_sync(self.h), "pandora_batch_sync")

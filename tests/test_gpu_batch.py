@@ -102,3 +102,21 @@ def test_batch_rejects_other_class_and_full(gpu_lib):
         b.admit(_member(base, 1))
         with pytest.raises(gpu_lib.PandoraError):
             b.admit(_member(base, 2))
+
+
+def test_ensemble_server_results_same_alone(gpu_lib):
+    """A small trace through the ensemble server (continuous batching, both precisions,
+    isotropic and sheared, with and without tracers): every run's final state equals
+    the same request run alone."""
+    from pandora import ensemble
+    trace = ensemble.make_trace(6, seed=3, rate=None, steps=10, particles=64, sizes=(32, 48))
+    for k, r in enumerate(trace):
+        r.arrival = 0.0 if k < 6 else 0.001 * k     # the later half joins running batches
+    caps = {f"{n}/{p}": {"best": 2} for n in (32, 48) for p in (0, 1)}
+    srv = ensemble.Server(8 << 30, caps, chunk=3, keep_state=True)
+    res = srv.run(trace, realtime=False)
+    srv.close()
+    assert res["requests"] == len(trace) and res["p99_ms"] > 0
+    for r in trace:
+        u, _ = _alone(gpu_lib, r.params, r.steps)
+        assert _same(r.result["u"], u), r.rid
