@@ -124,11 +124,19 @@ def tune_capacity(n: int, precision: int, caps=(1, 2, 4, 8, 16, 32, 64), steps: 
     return {"best": best, "rates": rates}
 
 
-def autotune(sizes=SIZES, precisions=(PREC_FP64, PREC_FP32_MIXED), cache: str | None = None) -> dict:
-    """Batch capacity per (N, precision); cached in `cache` (JSON) when given."""
+# Capacities measured on a B200 by tune_capacity (the starting table of autotune).
+MEASURED_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_b200.json")
+
+
+def autotune(sizes=SIZES, precisions=(PREC_FP64, PREC_FP32_MIXED), cache: str | None = None,
+             start: str | None = MEASURED_TABLE) -> dict:
+    """Batch capacity per (N, precision): from `cache` (JSON) if it exists, else from
+    the measured table `start`; classes missing from both are measured now, and the
+    table is written to `cache` when given."""
     table = {}
-    if cache and os.path.exists(cache):
-        with open(cache) as fh:
+    src = cache if (cache and os.path.exists(cache)) else start
+    if src and os.path.exists(src):
+        with open(src) as fh:
             table = json.load(fh)
     changed = False
     for n in sizes:
