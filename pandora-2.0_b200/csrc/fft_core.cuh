@@ -106,6 +106,31 @@ template <int S, class C> PD_HD void dft16(C* v) {
 #pragma unroll
     for (int r = 0; r < 8; r++) { v[r] = add(e[r], o[r]); v[r + 8] = sub(e[r], o[r]); }
 }
+// 12 = 3 x 4 (Cooley-Tukey): n = 4 n1 + n2, k = k1 + 3 k2.  Length-3 DFTs over n1
+// for each n2, twiddles W12^(S n2 k1) (multiples of 30 degrees), length-4 DFTs over
+// n2 for each k1.
+template <int S, class C> PD_HD void dft12(C* v) {
+    C y[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+        y[n2][0] = v[n2]; y[n2][1] = v[4 + n2]; y[n2][2] = v[8 + n2];
+        dft3<S>(y[n2]);
+    }
+    // W12^m = cos(30 m deg) + S i sin(30 m deg) for m = n2 k1 in 1..6
+    y[1][1] = mul_cs<S>(y[1][1], kSin60, 0.5);            // m = 1
+    y[1][2] = mul_cs<S>(y[1][2], 0.5, kSin60);            // m = 2
+    y[2][1] = mul_cs<S>(y[2][1], 0.5, kSin60);            // m = 2
+    y[2][2] = mul_cs<S>(y[2][2], -0.5, kSin60);           // m = 4
+    y[3][1] = mul_si<S>(y[3][1]);                          // m = 3
+    y[3][2] = mk(-y[3][2].x, -y[3][2].y);                  // m = 6
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        C z[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+        dft4<S>(z);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) v[k1 + 3 * k2] = z[k2];
+    }
+}
 // odd prime R (5, 7): X_r = v0 + sum_{q=1}^{(R-1)/2} [C(qr)(v_q + v_{R-q}) + S i S(qr)(v_q - v_{R-q})]
 template <int R> struct PrimeTab;
 template <> struct PrimeTab<5> {
@@ -155,12 +180,14 @@ template <int R, int S, class C> PD_HD void dft(C* v) {
     else if constexpr (R == 4) dft4<S>(v);
     else if constexpr (R == 8) dft8<S>(v);
     else if constexpr (R == 16) dft16<S>(v);
+    else if constexpr (R == 12) dft12<S>(v);
     else if constexpr (R == 5 || R == 7) dft_prime<R, S>(v);
     else static_assert(R == 2, "unsupported radix");
 }
 
 // Radix schedule per transform length.  Supported N: 2^a * {1,3,5,7} up to 1024 that
-// factor into the radices below in at most three passes.
+// factor into the radices below (2, 3, 4, 5, 7, 8, 12, 16) in at most three passes;
+// lengths with a factor 3 take a radix-12 pass where that saves a pass.
 template <int N> struct Plan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
 #define PD_PLAN(N_, A, B, C) \
     template <> struct Plan<N_> { static constexpr int r0 = A, r1 = B, r2 = C; };
@@ -172,11 +199,11 @@ PD_PLAN(48, 3, 16, 0)
 PD_PLAN(56, 7, 8, 0)
 PD_PLAN(64, 8, 8, 0)
 PD_PLAN(80, 5, 16, 0)
-PD_PLAN(96, 3, 4, 8)
+PD_PLAN(96, 8, 12, 0)
 PD_PLAN(112, 7, 16, 0)
 PD_PLAN(128, 8, 16, 0)
 PD_PLAN(160, 5, 4, 8)
-PD_PLAN(192, 3, 8, 8)
+PD_PLAN(192, 16, 12, 0)
 PD_PLAN(224, 7, 4, 8)
 PD_PLAN(256, 16, 16, 0)
 PD_PLAN(320, 5, 8, 8)
@@ -292,11 +319,11 @@ template <int N> struct WPlan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
 PD_WPLAN(16, 4, 4, 0)
 PD_WPLAN(24, 3, 8, 0)
 PD_WPLAN(32, 4, 8, 0)
-PD_WPLAN(48, 3, 4, 4)
+PD_WPLAN(48, 4, 12, 0)
 PD_WPLAN(64, 8, 8, 0)
-PD_WPLAN(96, 3, 4, 8)
+PD_WPLAN(96, 8, 12, 0)
 PD_WPLAN(128, 4, 4, 8)
-PD_WPLAN(192, 3, 8, 8)
+PD_WPLAN(192, 16, 12, 0)
 PD_WPLAN(256, 4, 8, 8)
 PD_WPLAN(384, 3, 8, 16)
 PD_WPLAN(512, 8, 8, 8)
@@ -313,7 +340,6 @@ template <int N> constexpr bool wplan_ok() {
 template <int N> struct WPlanL : WPlan<N> {};
 template <> struct WPlanL<128> { static constexpr int r0 = 16, r1 = 8, r2 = 0; };
 template <> struct WPlanL<256> { static constexpr int r0 = 16, r1 = 16, r2 = 0; };
-template <> struct WPlanL<48> { static constexpr int r0 = 3, r1 = 16, r2 = 0; };
 
 template <int N> constexpr bool wplanl_ok() {
     return WPlanL<N>::r0 * (WPlanL<N>::r1 ? WPlanL<N>::r1 : 1) * (WPlanL<N>::r2 ? WPlanL<N>::r2 : 1) == N;

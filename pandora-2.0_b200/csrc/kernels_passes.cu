@@ -76,7 +76,7 @@ bool supported_length(int n) {
 // arrays and XPS chosen per length, those passes are free of bank conflicts.
 // ---------------------------------------------------------------------------
 template <int N> constexpr int xps() {
-    return (N == 16 || N == 32) ? 2 : ((N == 24 || N == 64 || N == 192 || N == 384 || N == 512) ? 3 : 4);
+    return (N == 16 || N == 32 || N == 48) ? 2 : ((N == 24 || N == 64 || N == 96 || N == 384 || N == 512) ? 3 : 4);
 }
 template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
 template <int N> constexpr int xna() { return N <= 256 ? 2 : 1; }
@@ -284,7 +284,8 @@ template <int N> struct TCfg {
     // resident CTAs per SM asked of the register allocator: FP32 tiles need half the
     // registers and shared memory of FP64 ones
     template <class T> static constexpr int minb() {
-        return sizeof(T) == 8 ? (NT <= 128 ? 5 : (NT <= 256 ? 2 : 1)) : (NT <= 128 ? 8 : (NT <= 256 ? 4 : 2));
+        return sizeof(T) == 8 ? (NT <= 128 ? (N == 192 ? 4 : 5) : (NT <= 256 ? 2 : (N == 512 ? 2 : 1)))
+                              : (NT <= 128 ? (N == 192 ? 6 : 8) : (NT <= 256 ? 4 : 2));
     }
     template <class T> static constexpr size_t smem() { return sizeof(typename Cplx<T>::type) * (size_t)N * L; }
 };
