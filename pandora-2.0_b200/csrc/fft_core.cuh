@@ -106,6 +106,34 @@ template <int S, class C> PD_HD void dft16(C* v) {
 #pragma unroll
     for (int r = 0; r < 8; r++) { v[r] = add(e[r], o[r]); v[r + 8] = sub(e[r], o[r]); }
 }
+// 32 = 2 x 16: radix-2 decimation in time over two length-16 DFTs, twiddles
+// W32^(S r) = cos(pi r / 16) + S i sin(pi r / 16) for r = 1..15.
+template <int S, class C> PD_HD void dft32(C* v) {
+    C e[16], o[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) { e[q] = v[2 * q]; o[q] = v[2 * q + 1]; }
+    dft16<S>(e); dft16<S>(o);
+    constexpr double c1 = 0.9807852804032304491261822, s1 = 0.1950903220161282678482849;
+    constexpr double c2 = 0.9238795325112867561281832, s2 = 0.38268343236508977172846;
+    constexpr double c3 = 0.8314696123025452370787884, s3 = 0.5555702330196022247428308;
+    o[1] = mul_cs<S>(o[1], c1, s1);
+    o[2] = mul_cs<S>(o[2], c2, s2);
+    o[3] = mul_cs<S>(o[3], c3, s3);
+    o[4] = mul_cs<S>(o[4], kSqrtHalf, kSqrtHalf);
+    o[5] = mul_cs<S>(o[5], s3, c3);
+    o[6] = mul_cs<S>(o[6], s2, c2);
+    o[7] = mul_cs<S>(o[7], s1, c1);
+    o[8] = mul_si<S>(o[8]);
+    o[9] = mul_cs<S>(o[9], -s1, c1);
+    o[10] = mul_cs<S>(o[10], -s2, c2);
+    o[11] = mul_cs<S>(o[11], -s3, c3);
+    o[12] = mul_cs<S>(o[12], -kSqrtHalf, kSqrtHalf);
+    o[13] = mul_cs<S>(o[13], -c3, s3);
+    o[14] = mul_cs<S>(o[14], -c2, s2);
+    o[15] = mul_cs<S>(o[15], -c1, s1);
+#pragma unroll
+    for (int r = 0; r < 16; r++) { v[r] = add(e[r], o[r]); v[r + 16] = sub(e[r], o[r]); }
+}
 // 12 = 3 x 4 (Cooley-Tukey): n = 4 n1 + n2, k = k1 + 3 k2.  Length-3 DFTs over n1
 // for each n2, twiddles W12^(S n2 k1) (multiples of 30 degrees), length-4 DFTs over
 // n2 for each k1.
@@ -181,12 +209,13 @@ template <int R, int S, class C> PD_HD void dft(C* v) {
     else if constexpr (R == 8) dft8<S>(v);
     else if constexpr (R == 16) dft16<S>(v);
     else if constexpr (R == 12) dft12<S>(v);
+    else if constexpr (R == 32) dft32<S>(v);
     else if constexpr (R == 5 || R == 7) dft_prime<R, S>(v);
     else static_assert(R == 2, "unsupported radix");
 }
 
 // Radix schedule per transform length.  Supported N: 2^a * {1,3,5,7} up to 1024 that
-// factor into the radices below (2, 3, 4, 5, 7, 8, 12, 16) in at most three passes;
+// factor into the radices below (2, 3, 4, 5, 7, 8, 12, 16; 32 in warp plans) in at most three passes;
 // lengths with a factor 3 take a radix-12 pass where that saves a pass.
 template <int N> struct Plan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
 #define PD_PLAN(N_, A, B, C) \
@@ -340,6 +369,8 @@ template <int N> constexpr bool wplan_ok() {
 template <int N> struct WPlanL : WPlan<N> {};
 template <> struct WPlanL<128> { static constexpr int r0 = 16, r1 = 8, r2 = 0; };
 template <> struct WPlanL<256> { static constexpr int r0 = 16, r1 = 16, r2 = 0; };
+template <> struct WPlanL<512> { static constexpr int r0 = 32, r1 = 16, r2 = 0; };
+template <> struct WPlanL<1024> { static constexpr int r0 = 32, r1 = 32, r2 = 0; };
 
 template <int N> constexpr bool wplanl_ok() {
     return WPlanL<N>::r0 * (WPlanL<N>::r1 ? WPlanL<N>::r1 : 1) * (WPlanL<N>::r2 ? WPlanL<N>::r2 : 1) == N;

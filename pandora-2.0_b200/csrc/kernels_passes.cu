@@ -70,16 +70,20 @@ bool supported_length(int n) {
 // the same line.  Optionally writes the physical velocity (arr_u*_3r,
 // src/pf_rk3.f90:1108-1115) and the CFL maximum (src/pf_fluidstats.f90:913-917).
 // Warp shared region: three arrays XAS elements apart (XAS = 4 mod 8 in 16-byte
-// units), element n of array p at s[p*XAS + prow<XPS>(n)].  Up to N = 256 the
-// warp transforms arrays 0 and 1 in lockstep (a radix-16 pass of one array
-// leaves half the lanes idle); with the offset of 4 bank groups between the two
+// units), element n of array p at s[p*XAS + prow<XPS>(n)].  Up to N = 512 the
+// warp transforms arrays 0 and 1 in lockstep (a radix-16 or radix-32 pass of one
+// array leaves lanes idle); with the offset of 4 bank groups between the two
 // arrays and XPS chosen per length, those passes are free of bank conflicts.
+// The warp plans are two passes up to N = 1024 (radix 32 at 512 and 1024): the
+// kernel is bound by shared-memory wavefronts, and each pass is a full read and
+// write of the three arrays.
 // ---------------------------------------------------------------------------
 template <int N> constexpr int xps() {
-    return (N == 16 || N == 32 || N == 48) ? 2 : ((N == 24 || N == 64 || N == 96 || N == 384 || N == 512) ? 3 : 4);
+    return (N == 16 || N == 32 || N == 48) ? 2 : ((N == 24 || N == 64 || N == 96 || N == 384) ? 3 : (N >= 512 ? 5 : 4));
 }
 template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
-template <int N> constexpr int xna() { return N <= 256 ? 2 : 1; }
+// arrays transformed in lockstep: 2 while a lane's items of a pass fit its registers
+template <int N> constexpr int xna() { return N <= 512 ? 2 : 1; }
 
 template <int NX, class T, int CAP>
 __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,

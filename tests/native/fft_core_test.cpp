@@ -152,7 +152,7 @@ int main() {
         printf("warp low-pass N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                       \
         if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                             \
     } while (0)
-    RUNL(48); RUNL(128); RUNL(256); RUNL(512);
+    RUNL(48); RUNL(128); RUNL(256); RUNL(512); RUNL(1024);
 #define RUND(N)                                                                                      \
     do {                                                                                             \
         double e1 = check<N, -1, 8, 9, false, false, true>(), e2 = check<N, +1, 8, 9, false, false, true>(); \
@@ -168,7 +168,7 @@ int main() {
         if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                              \
     } while (0)
     RUNP(16, 2); RUNP(24, 3); RUNP(32, 2); RUNP(48, 2); RUNP(64, 3); RUNP(96, 3); RUNP(128, 4);
-    RUNP(192, 4); RUNP(256, 4);
+    RUNP(192, 4); RUNP(256, 4); RUNP(512, 5);
     printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }

@@ -58,6 +58,21 @@ def test_nonlinear_anisotropic_grid(gpu_lib):
     assert e < 1e-13
 
 
+@pytest.mark.parametrize("axis", [0, 1, 2])
+@pytest.mark.parametrize("n", [96, 128, 192, 256, 384, 512, 768, 1024])
+def test_nonlinear_every_length(gpu_lib, n, axis):
+    """Every supported transform length along each axis (x pass, y passes, z passes),
+    the other two axes 16 points long."""
+    p = gpu_lib.workload_params("iso_decay", 32)
+    dims = [16, 16, 16]
+    dims[axis] = n
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    o, s = _pair(gpu_lib, p)
+    e = rel_l2_fields(s.nonlinear(), o.nonlinear())
+    s.close()
+    assert e < 1e-13
+
+
 def test_init_fluid_matches_oracle(gpu_lib):
     import oracle as O
     p = gpu_lib.workload_params("iso_decay", 64)
