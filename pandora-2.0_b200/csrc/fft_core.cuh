@@ -264,12 +264,23 @@ template <int LP, int PS, int AS> PD_HD int tidx(int n, int l) {
     return AS ? l * AS + prow<PS>(n) : prow<PS>(n) * LP + l;
 }
 
-template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0, class C>
+// The band of a 2/3-truncated spectrum on a length-N line: n <= KB or n >= N - KB
+// (KB = 0: the whole line).  A pass_load with KB > 0 reads the elements outside
+// the band as zero without touching shared memory (first pass of a transform of a
+// truncated spectrum); a pass_store with KB > 0 writes only the band (last pass of
+// a transform whose outputs outside it are discarded).
+template <int N, int KB> PD_HD bool in_band(int n) { return KB == 0 || n <= KB || n >= N - KB; }
+
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0, int KB = 0, class C>
 PD_HD void pass_load(const C* s, const C* tw, int w, C* v) {
+    using T = real_of<C>;
     constexpr int NR = N / R;
     const int l = w % L, j = w / L;
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = s[tidx<LP, PS, AS>(j + r * NR, l)];
+    for (int r = 0; r < R; r++) {
+        if constexpr (KB > 0) v[r] = in_band<N, KB>(j + r * NR) ? s[tidx<LP, PS, AS>(j + r * NR, l)] : mk(T(0), T(0));
+        else v[r] = s[tidx<LP, PS, AS>(j + r * NR, l)];
+    }
     if constexpr (NS > 1) {
         const int k = j % NS;
         constexpr int step = N / (NS * R);
@@ -278,13 +289,14 @@ PD_HD void pass_load(const C* s, const C* tw, int w, C* v) {
     }
     dft<R, S>(v);
 }
-template <int N, int R, int NS, int L, int LP, int PS = 0, int AS = 0, class C>
+template <int N, int R, int NS, int L, int LP, int PS = 0, int AS = 0, int KB = 0, class C>
 PD_HD void pass_store(C* s, int w, const C* v) {
     const int l = w % L, j = w / L;
     const int k = j % NS;
     const int d = (j / NS) * NS * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) s[tidx<LP, PS, AS>(d + r * NS, l)] = v[r];
+    for (int r = 0; r < R; r++)
+        if (in_band<N, KB>(d + r * NS)) s[tidx<LP, PS, AS>(d + r * NS, l)] = v[r];
 }
 
 // Transforms whose first pass reads global memory and whose last pass writes it
@@ -369,8 +381,28 @@ template <int N> constexpr bool wplan_ok() {
 template <int N> struct WPlanL : WPlan<N> {};
 template <> struct WPlanL<128> { static constexpr int r0 = 16, r1 = 8, r2 = 0; };
 template <> struct WPlanL<256> { static constexpr int r0 = 16, r1 = 16, r2 = 0; };
+template <> struct WPlanL<384> { static constexpr int r0 = 32, r1 = 12, r2 = 0; };
 template <> struct WPlanL<512> { static constexpr int r0 = 32, r1 = 16, r2 = 0; };
 template <> struct WPlanL<1024> { static constexpr int r0 = 32, r1 = 32, r2 = 0; };
+
+// Plan of a backward transform, a pointwise product and a forward transform run
+// by one warp (the x pass): backward (r0, r1[, r2]) = WPlanL; with `fused` the
+// forward transform runs the reversed plan, so that the last backward pass and
+// the first forward pass see the same elements n = j + r * (N / rl) in item j, and
+// the last backward pass of one array, the product and the first forward pass run
+// in registers, one item per lane (nrl = N / rl items, 16..32 of them).  Lines
+// shorter than 256 keep separate passes and the same plan both ways (measured
+// faster at 192: the fused step leaves half the lanes idle there).
+template <int N> struct FusedPlan {
+    static constexpr int r0 = WPlanL<N>::r0, r1 = WPlanL<N>::r1, r2 = WPlanL<N>::r2;
+    static constexpr int np = r2 ? 3 : 2;
+    static constexpr int rl = r2 ? r2 : r1;
+    static constexpr int nrl = N / rl;
+    static constexpr bool fused = N >= 256 && nrl >= 16 && nrl <= 32;
+    static constexpr int f0 = fused ? rl : r0;
+    static constexpr int f1 = fused ? (r2 ? r1 : r0) : r1;
+    static constexpr int f2 = fused ? (r2 ? r0 : 0) : r2;
+};
 
 template <int N> constexpr bool wplanl_ok() {
     return WPlanL<N>::r0 * (WPlanL<N>::r1 ? WPlanL<N>::r1 : 1) * (WPlanL<N>::r2 ? WPlanL<N>::r2 : 1) == N;
@@ -402,7 +434,8 @@ __device__ __forceinline__ void wpass(C* s, const C* __restrict__ tw, int lane) 
 // AS = 0, else separate arrays AS elements apart): each pass has NA times the
 // independent work of a single line, which fills the lanes a radix-16 pass of
 // one line leaves idle.
-template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0, class C>
+// KL / KS: band of the loads / stores (see in_band).
+template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0, int KL = 0, int KS = 0, class C>
 __device__ __forceinline__ void wpass_n(C* s, const C* __restrict__ tw, int lane) {
     constexpr int WORK = (N / R) * NA;
     constexpr int IT = (WORK + 31) / 32;
@@ -410,15 +443,27 @@ __device__ __forceinline__ void wpass_n(C* s, const C* __restrict__ tw, int lane
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS, AS>(s, tw, w, v[it]);
+        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS, AS, KL>(s, tw, w, v[it]);
     }
     __syncwarp();
 #pragma unroll
     for (int it = 0; it < IT; it++) {
         const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS, AS>(s, w, v[it]);
+        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS, AS, KS>(s, w, v[it]);
     }
     __syncwarp();
+}
+
+// Passes P0..P1-1 of the radix plan (R0, R1, R2) over NA arrays owned by one
+// warp: pass p has radix Rp and NS = the product of the radices before it.  The
+// plan's first pass reads the band KL, its last pass writes the band KS.
+template <int N, int S, int LP, int PS, int NA, int AS, int R0, int R1, int R2, int P0, int P1,
+          int KL = 0, int KS = 0, class C>
+__device__ __forceinline__ void wpasses(C* s, const C* __restrict__ tw, int lane) {
+    constexpr int NP = R2 ? 3 : (R1 ? 2 : 1);
+    if constexpr (P0 <= 0 && 0 < P1) wpass_n<N, R0, 1, S, LP, PS, NA, AS, KL, NP == 1 ? KS : 0>(s, tw, lane);
+    if constexpr (P0 <= 1 && 1 < P1 && NP > 1) wpass_n<N, R1, R0, S, LP, PS, NA, AS, 0, NP == 2 ? KS : 0>(s, tw, lane);
+    if constexpr (P0 <= 2 && 2 < P1 && NP > 2) wpass_n<N, R2, R0 * R1, S, LP, PS, NA, AS, 0, KS>(s, tw, lane);
 }
 
 template <int N, int S, int LP, int PS, int NA, bool LOWPASS = false, int AS = 0, class C>

@@ -25,7 +25,6 @@
 
 namespace pd {
 
-using pdfft::fft_warp;
 using pdfft::mk;
 using pdfft::prow;
 using pdfft::tile_rows;
@@ -79,17 +78,33 @@ bool supported_length(int n) {
 // write of the three arrays.
 // ---------------------------------------------------------------------------
 template <int N> constexpr int xps() {
-    return (N == 16 || N == 32 || N == 48) ? 2 : ((N == 24 || N == 64 || N == 96 || N == 384) ? 3 : (N >= 512 ? 5 : 4));
+    return (N == 16 || N == 32 || N == 48) ? 2
+         : ((N == 24 || N == 64 || N == 96) ? 3 : ((N == 384 || N == 512 || N == 1024) ? 5 : 4));
 }
 template <int N> constexpr int xas() { return (tile_rows<N, xps<N>()>() + 7) / 8 * 8 + 4; }
 // arrays transformed in lockstep: 2 while a lane's items of a pass fit its registers
 template <int N> constexpr int xna() { return N <= 512 ? 2 : 1; }
+
+// NL = omega x u at one point (isotropic or BF-rot); returns (n1, n2) and n3.
+template <class T, class C>
+__device__ __forceinline__ C nl_point(const BF& bf, bool shear, T u1, T u2, T u3, T w1, T w2, T w3, T& n3) {
+    if (shear) {   // f_RK3ComputeNonlinearBFRot (FP64 registers in both forms)
+        const double uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
+        double nl[3];
+        nl_bf(bf, uu, om, nl);
+        n3 = T(nl[2]);
+        return mk(T(nl[0]), T(nl[1]));
+    }
+    n3 = u2 * w1 - u1 * w2;
+    return mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
+}
 
 template <int NX, class T, int CAP>
 __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                         int want_phys,
                                                                                         int want_cfl) {
     using C = typename FieldsT<T>::C;
+    using XP = pdfft::FusedPlan<NX>;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
@@ -98,6 +113,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
+    constexpr int KB = NX / 3;   // the kept band of the x spectrum, i <= KI
     C* smem = smem_as<C>();
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const long long lines = (long long)g.ny * g.nz;
@@ -106,10 +122,11 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     if (q >= lines) return;                       // whole warp; no block barrier follows
     C* s = smem + (size_t)w * 3 * XAS;
     const long long fstride = lines * g.nkip;     // distance between fields in yb
-    const int KI = g.ki, NKI = g.nki;
+    const int NKI = g.nki;
     C* b = F.yb + q * g.nkip;
     BF bf;
     if (g.shear) bf = make_bf(g, F.clock);
+    // the band of each array; the first backward pass reads nothing outside it
     for (int m = lane; m < NKI; m += 32) {
 #pragma unroll
         for (int p = 0; p < 3; p++) {
@@ -119,50 +136,78 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
             if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
         }
     }
-    for (int n = KI + 1 + lane; n < NX - KI; n += 32) {
-#pragma unroll
-        for (int p = 0; p < 3; p++) s[p * XAS + prow<XPS>(n)] = mk(T(0), T(0));
-    }
     __syncwarp();
+    constexpr int R0 = XP::r0, R1 = XP::r1, R2 = XP::r2, NP = XP::np;
     if constexpr (NA == 2) {
-        pdfft::fft_warp_n<NX, +1, 1, XPS, 2, true, XAS>(s, tw, lane);
+        pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB>(s, tw, lane);
     } else {
-        fft_warp<NX, +1, 1, XPS, true>(s, tw, lane);
-        fft_warp<NX, +1, 1, XPS, true>(s + XAS, tw, lane);
+        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s, tw, lane);
+        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + XAS, tw, lane);
     }
-    fft_warp<NX, +1, 1, XPS, true>(s + 2 * XAS, tw, lane);
     T umax = T(0);
-    for (int n = lane; n < NX; n += 32) {
-        C* e = s + prow<XPS>(n);
-        const C a = e[0], bb = e[XAS], c = e[2 * XAS];
-        const T u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
-        if (want_phys) {
-            F.phys[q * NX + n] = u1;
-            F.phys[g.R + q * NX + n] = u2;
-            F.phys[2 * g.R + q * NX + n] = u3;
+    if constexpr (XP::fused) {
+        constexpr int RL = XP::rl, NRL = XP::nrl;
+        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP - 1, KB>(s + 2 * XAS, tw, lane);
+        C v[RL];
+        T n3[RL];
+        if (lane < NRL) {
+            // last backward pass of array 2: (w2, w3) at n = lane + r * NRL
+            pdfft::pass_load<NX, RL, NRL, +1, 1, 1, XPS, 0>(s + 2 * XAS, tw, lane, v);
+#pragma unroll
+            for (int r = 0; r < RL; r++) {
+                const int n = lane + r * NRL;
+                const C* e = s + prow<XPS>(n);
+                const C a = e[0], bb = e[XAS];
+                const T u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = v[r].x, w3 = v[r].y;
+                if (want_phys) {
+                    F.phys[q * NX + n] = u1;
+                    F.phys[g.R + q * NX + n] = u2;
+                    F.phys[2 * g.R + q * NX + n] = u3;
+                }
+                if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
+                v[r] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3[r]);
+            }
         }
-        if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
-        if (g.shear) {   // f_RK3ComputeNonlinearBFRot (FP64 registers in both forms)
-            const double uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
-            double nl[3];
-            nl_bf(bf, uu, om, nl);
-            e[0] = mk(T(nl[0]), T(nl[1]));
-            e[XAS] = mk(T(nl[2]), T(0));
-        } else {
-            e[0] = mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
-            e[XAS] = mk(u2 * w1 - u1 * w2, T(0));
+        __syncwarp();   // every lane has read arrays 0 and 1
+        if (lane < NRL) {
+            // first forward pass (NS = 1) of the two product arrays, one at a time
+            pdfft::dft<RL, -1>(v);
+            pdfft::pass_store<NX, RL, 1, 1, 1, XPS, 0>(s, lane, v);
+#pragma unroll
+            for (int r = 0; r < RL; r++) v[r] = mk(n3[r], T(0));
+            pdfft::dft<RL, -1>(v);
+            pdfft::pass_store<NX, RL, 1, 1, 1, XPS, 0>(s + XAS, lane, v);
         }
+        __syncwarp();
+    } else {
+        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + 2 * XAS, tw, lane);
+        for (int n = lane; n < NX; n += 32) {
+            C* e = s + prow<XPS>(n);
+            const C a = e[0], bb = e[XAS], c = e[2 * XAS];
+            const T u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
+            if (want_phys) {
+                F.phys[q * NX + n] = u1;
+                F.phys[g.R + q * NX + n] = u2;
+                F.phys[2 * g.R + q * NX + n] = u3;
+            }
+            if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
+            T n3;
+            e[0] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3);
+            e[XAS] = mk(n3, T(0));
+        }
+        __syncwarp();
     }
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
         if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
     }
-    __syncwarp();
+    // forward transforms of the product arrays; only the band is written
+    constexpr int F0 = XP::f0, F1 = XP::f1, F2 = XP::f2, P0 = XP::fused ? 1 : 0;
     if constexpr (NA == 2) {
-        pdfft::fft_warp_n<NX, -1, 1, XPS, 2, true, XAS>(s, tw, lane);
+        pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, F0, F1, F2, P0, NP, 0, KB>(s, tw, lane);
     } else {
-        fft_warp<NX, -1, 1, XPS, true>(s, tw, lane);
-        fft_warp<NX, -1, 1, XPS, true>(s + XAS, tw, lane);
+        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s, tw, lane);
+        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s + XAS, tw, lane);
     }
     const T half = T(0.5);
     for (int m = lane; m < g.nkip; m += 32) {

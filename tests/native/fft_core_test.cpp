@@ -10,12 +10,119 @@
 
 using namespace pdfft;
 
-template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0>
+template <int N, int R, int NS, int S, int L, int LP, int PS = 0, int AS = 0, int KL = 0, int KS = 0>
 static void emu_pass(std::vector<double2>& s, const std::vector<double2>& tw) {
     constexpr int WORK = (N / R) * L;
     std::vector<double2> v((size_t)WORK * R);
-    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP, PS, AS>(s.data(), tw.data(), w, &v[(size_t)w * R]);
-    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP, PS, AS>(s.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_load<N, R, NS, S, L, LP, PS, AS, KL>(s.data(), tw.data(), w, &v[(size_t)w * R]);
+    for (int w = 0; w < WORK; w++) pass_store<N, R, NS, L, LP, PS, AS, KS>(s.data(), w, &v[(size_t)w * R]);
+}
+
+// Passes P0..P1-1 of the plan (R0, R1, R2) on NA arrays AS apart (wpasses on the GPU).
+template <int N, int S, int PS, int NA, int AS, int R0, int R1, int R2, int P0, int P1, int KL = 0, int KS = 0>
+static void emu_passes(std::vector<double2>& s, const std::vector<double2>& tw) {
+    constexpr int NP = R2 ? 3 : (R1 ? 2 : 1);
+    if constexpr (P0 <= 0 && 0 < P1) emu_pass<N, R0, 1, S, NA, 1, PS, AS, KL, NP == 1 ? KS : 0>(s, tw);
+    if constexpr (P0 <= 1 && 1 < P1 && NP > 1) emu_pass<N, R1, R0, S, NA, 1, PS, AS, 0, NP == 2 ? KS : 0>(s, tw);
+    if constexpr (P0 <= 2 && 2 < P1 && NP > 2) emu_pass<N, R2, R0 * R1, S, NA, 1, PS, AS, 0, KS>(s, tw);
+}
+
+// The x pass's transform chain on one line (three arrays AS apart, band KB = N/3):
+// backward transforms of band-limited arrays (first pass reading only the band),
+// NL = omega x u at every point, forward transforms of (n1 + i n2) and n3 written
+// only in the band; with FusedPlan::fused the third array's last backward pass,
+// the product and the first forward pass run per item as the kernel runs them.
+// Checked against direct long-double DFTs and the product.
+template <int N, int PS>
+static double check_xchain() {
+    using FP = FusedPlan<N>;
+    constexpr int KB = N / 3, AS = (N + (N >> PS) + 7) / 8 * 8 + 4;
+    constexpr int R0 = FP::r0, R1 = FP::r1, R2 = FP::r2, NP = FP::np;
+    std::vector<double2> tw(N);
+    for (int e = 0; e < N; e++) {
+        long double a = 6.283185307179586476925286766559005768L * e / N;
+        tw[e] = mk((double)cosl(a), -(double)sinl(a));
+    }
+    std::vector<double2> s((size_t)3 * AS, mk(1e30, 1e30)), x((size_t)3 * N, mk(0.0, 0.0));
+    srand(N * 13 + PS);
+    for (int p = 0; p < 3; p++)
+        for (int n = 0; n < N; n++)
+            if (in_band<N, KB>(n)) {
+                double2 v = mk(rand() / (double)RAND_MAX - 0.5, rand() / (double)RAND_MAX - 0.5);
+                x[(size_t)p * N + n] = v;
+                s[(size_t)p * AS + prow<PS>(n)] = v;
+            }
+    emu_passes<N, +1, PS, 2, AS, R0, R1, R2, 0, NP, KB>(s, tw);
+    auto nl = [](double u1, double u2, double u3, double w1, double w2, double w3, double& n3) {
+        n3 = u2 * w1 - u1 * w2;
+        return mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
+    };
+    std::vector<double2> a2(s.begin() + 2 * AS, s.begin() + 3 * AS);
+    if constexpr (FP::fused) {
+        constexpr int RL = FP::rl, NRL = FP::nrl;
+        emu_passes<N, +1, PS, 1, 0, R0, R1, R2, 0, NP - 1, KB>(a2, tw);
+        std::vector<double2> v((size_t)NRL * RL), xx((size_t)NRL * RL);
+        for (int j = 0; j < NRL; j++) {
+            double2* vj = &v[(size_t)j * RL];
+            double2* xj = &xx[(size_t)j * RL];
+            pass_load<N, RL, NRL, +1, 1, 1, PS, 0>(a2.data(), tw.data(), j, vj);
+            for (int r = 0; r < RL; r++) {
+                const int n = j + r * NRL;
+                const double2 a = s[prow<PS>(n)], b = s[AS + prow<PS>(n)];
+                double n3;
+                vj[r] = nl(a.x, a.y, b.x, b.y, vj[r].x, vj[r].y, n3);
+                xj[r] = mk(n3, 0.0);
+            }
+            dft<RL, -1>(vj);
+            dft<RL, -1>(xj);
+        }
+        for (int j = 0; j < NRL; j++) {
+            pass_store<N, RL, 1, 1, 1, PS, 0>(s.data(), j, &v[(size_t)j * RL]);
+            pass_store<N, RL, 1, 1, 1, PS, 0>(s.data() + AS, j, &xx[(size_t)j * RL]);
+        }
+    } else {
+        emu_passes<N, +1, PS, 1, 0, R0, R1, R2, 0, NP, KB>(a2, tw);
+        for (int n = 0; n < N; n++) {
+            const double2 a = s[prow<PS>(n)], b = s[AS + prow<PS>(n)], c = a2[prow<PS>(n)];
+            double n3;
+            s[prow<PS>(n)] = nl(a.x, a.y, b.x, b.y, c.x, c.y, n3);
+            s[AS + prow<PS>(n)] = mk(n3, 0.0);
+        }
+    }
+    emu_passes<N, -1, PS, 2, AS, FP::f0, FP::f1, FP::f2, FP::fused ? 1 : 0, NP, 0, KB>(s, tw);
+    // direct: backward DFTs, product, forward DFTs
+    std::vector<long double> ph((size_t)6 * N);
+    for (int p = 0; p < 3; p++)
+        for (int n = 0; n < N; n++) {
+            long double re = 0, im = 0;
+            for (int m = 0; m < N; m++) {
+                long double ang = 6.283185307179586476925286766559005768L * (long double)((long)m * n % N) / N;
+                double2 v = x[(size_t)p * N + m];
+                re += v.x * cosl(ang) - v.y * sinl(ang);
+                im += v.x * sinl(ang) + v.y * cosl(ang);
+            }
+            ph[(size_t)(2 * p) * N + n] = re;
+            ph[(size_t)(2 * p + 1) * N + n] = im;
+        }
+    double err = 0, mag = 0;
+    for (int k = 0; k < N; k++) {
+        if (!in_band<N, KB>(k)) continue;
+        long double r0 = 0, i0 = 0, r1 = 0, i1 = 0;
+        for (int n = 0; n < N; n++) {
+            const long double u1 = ph[n], u2 = ph[N + n], u3 = ph[2 * N + n];
+            const long double w1 = ph[3 * N + n], w2 = ph[4 * N + n], w3 = ph[5 * N + n];
+            const long double n1 = u3 * w2 - u2 * w3, n2 = u1 * w3 - u3 * w1, n3 = u2 * w1 - u1 * w2;
+            long double ang = -6.283185307179586476925286766559005768L * (long double)((long)k * n % N) / N;
+            const long double c = cosl(ang), sn = sinl(ang);
+            r0 += n1 * c - n2 * sn; i0 += n1 * sn + n2 * c;
+            r1 += n3 * c; i1 += n3 * sn;
+        }
+        const double2 g0 = s[prow<PS>(k)], g1 = s[AS + prow<PS>(k)];
+        err = fmax(err, fabs((double)(g0.x - r0)) + fabs((double)(g0.y - i0)));
+        err = fmax(err, fabs((double)(g1.x - r1)) + fabs((double)(g1.y - i1)));
+        mag = fmax(mag, fabs((double)r0) + fabs((double)i0));
+    }
+    return err / mag;
 }
 
 // Two lines in separate arrays AS elements apart, transformed in lockstep with the
@@ -169,6 +276,14 @@ int main() {
     } while (0)
     RUNP(16, 2); RUNP(24, 3); RUNP(32, 2); RUNP(48, 2); RUNP(64, 3); RUNP(96, 3); RUNP(128, 4);
     RUNP(192, 4); RUNP(256, 4); RUNP(512, 5);
+#define RUNX(N, PS)                                                              \
+    do {                                                                         \
+        double e = check_xchain<N, PS>();                                        \
+        printf("x chain N=%4d PS=%d fused=%d err %.2e\n", N, PS, (int)FusedPlan<N>::fused, e); \
+        if (!(e < 1e-13)) bad++;                                                 \
+    } while (0)
+    RUNX(16, 2); RUNX(24, 3); RUNX(32, 2); RUNX(48, 2); RUNX(64, 3); RUNX(96, 3); RUNX(128, 4);
+    RUNX(192, 4); RUNX(256, 4); RUNX(384, 5); RUNX(512, 5); RUNX(768, 4); RUNX(1024, 5);
     printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }
