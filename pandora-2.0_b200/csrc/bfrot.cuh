@@ -11,11 +11,14 @@
 
 namespace pd {
 
-struct BF {
-    double bm[3][3];
-    double bi[3][3];
-    double a13;     // amat(1,3) = F_DEFORM_S
+// The frame's tensors in real type R: FP64 as computed, or rounded once to FP32 for
+// the pointwise products of the FP32-mixed form (bf_as).
+template <class R> struct BFT {
+    R bm[3][3];
+    R bi[3][3];
+    R a13;     // amat(1,3) = F_DEFORM_S
 };
+using BF = BFT<double>;
 
 __host__ __device__ __forceinline__ constexpr bool bex(int a, int b) { return a == b || (a == 0 && b == 2); }
 
@@ -33,34 +36,48 @@ __device__ __forceinline__ BF make_bf(const Geo& g, const Clock* ck) {
     return f;
 }
 
+template <class R> __device__ __forceinline__ BFT<R> bf_as(const BF& f) {
+    BFT<R> r;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) { r.bm[a][b] = (R)f.bm[a][b]; r.bi[a][b] = (R)f.bi[a][b]; }
+    r.a13 = (R)f.a13;
+    return r;
+}
+
 // f_RK3VorticityBFRot (src/pf_rk3.f90:3786-3843), summed over the three velocity
-// components: w = sum_n omega(u_n).
-__device__ __forceinline__ void vort_bf(const BF& f, const double2* u, const double* k, double2* w) {
-    w[0] = make_double2(0.0, 0.0); w[1] = w[0]; w[2] = w[0];
+// components: w = sum_n omega(u_n).  Structurally w[0] has no term in u[0] and
+// w[1] none in u[1] (bex), so a caller that needs only w[0] or w[1] may pass zero
+// for that component.
+template <class R, class C>
+__device__ __forceinline__ void vort_bf(const BFT<R>& f, const C* u, const R* k, C* w) {
+    w[0].x = R(0); w[0].y = R(0); w[1] = w[0]; w[2] = w[0];
 #pragma unroll
     for (int n = 0; n < 3; n++) {
-        const double2 un = u[n];
+        const C un = u[n];
 #pragma unroll
         for (int m = 0; m < 3; m++) {
             if (bex(m, 0)) {
-                if (bex(2, n)) { const double c = f.bm[m][0] * f.bi[2][n] * k[m]; w[1].y -= c * un.x; w[1].x += c * un.y; }
-                if (bex(1, n)) { const double c = f.bm[m][0] * f.bi[1][n] * k[m]; w[2].y += c * un.x; w[2].x -= c * un.y; }
+                if (bex(2, n)) { const R c = f.bm[m][0] * f.bi[2][n] * k[m]; w[1].y -= c * un.x; w[1].x += c * un.y; }
+                if (bex(1, n)) { const R c = f.bm[m][0] * f.bi[1][n] * k[m]; w[2].y += c * un.x; w[2].x -= c * un.y; }
             }
             if (bex(m, 1)) {
-                if (bex(2, n)) { const double c = f.bm[m][1] * f.bi[2][n] * k[m]; w[0].y += c * un.x; w[0].x -= c * un.y; }
-                if (bex(0, n)) { const double c = f.bm[m][1] * f.bi[0][n] * k[m]; w[2].y -= c * un.x; w[2].x += c * un.y; }
+                if (bex(2, n)) { const R c = f.bm[m][1] * f.bi[2][n] * k[m]; w[0].y += c * un.x; w[0].x -= c * un.y; }
+                if (bex(0, n)) { const R c = f.bm[m][1] * f.bi[0][n] * k[m]; w[2].y -= c * un.x; w[2].x += c * un.y; }
             }
             if (bex(m, 2)) {
-                if (bex(1, n)) { const double c = f.bm[m][2] * f.bi[1][n] * k[m]; w[0].y -= c * un.x; w[0].x += c * un.y; }
-                if (bex(0, n)) { const double c = f.bm[m][2] * f.bi[0][n] * k[m]; w[1].y += c * un.x; w[1].x -= c * un.y; }
+                if (bex(1, n)) { const R c = f.bm[m][2] * f.bi[1][n] * k[m]; w[0].y -= c * un.x; w[0].x += c * un.y; }
+                if (bex(0, n)) { const R c = f.bm[m][2] * f.bi[0][n] * k[m]; w[1].y += c * un.x; w[1].x -= c * un.y; }
             }
         }
     }
 }
 
 // f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711), pointwise in physical space.
-__device__ __forceinline__ void nl_bf(const BF& f, const double* u, const double* om, double* nl) {
-    double n1 = 0.0, n2 = 0.0, n3 = 0.0;
+template <class R>
+__device__ __forceinline__ void nl_bf(const BFT<R>& f, const R* u, const R* om, R* nl) {
+    R n1 = R(0), n2 = R(0), n3 = R(0);
 #pragma unroll
     for (int m = 0; m < 3; m++) {
         if (bex(0, m)) { n3 -= om[1] * f.bi[0][m] * u[m]; n2 += om[2] * f.bi[0][m] * u[m]; }

@@ -87,13 +87,13 @@ template <int N> constexpr int xna() { return N <= 512 ? 2 : 1; }
 
 // NL = omega x u at one point (isotropic or BF-rot); returns (n1, n2) and n3.
 template <class T, class C>
-__device__ __forceinline__ C nl_point(const BF& bf, bool shear, T u1, T u2, T u3, T w1, T w2, T w3, T& n3) {
-    if (shear) {   // f_RK3ComputeNonlinearBFRot (FP64 registers in both forms)
-        const double uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
-        double nl[3];
+__device__ __forceinline__ C nl_point(const BFT<T>& bf, bool shear, T u1, T u2, T u3, T w1, T w2, T w3, T& n3) {
+    if (shear) {   // f_RK3ComputeNonlinearBFRot, in the fields' real type
+        const T uu[3] = {u1, u2, u3}, om[3] = {w1, w2, w3};
+        T nl[3];
         nl_bf(bf, uu, om, nl);
-        n3 = T(nl[2]);
-        return mk(T(nl[0]), T(nl[1]));
+        n3 = nl[2];
+        return mk(nl[0], nl[1]);
     }
     n3 = u2 * w1 - u1 * w2;
     return mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
@@ -124,8 +124,8 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int NKI = g.nki;
     C* b = F.yb + q * g.nkip;
-    BF bf;
-    if (g.shear) bf = make_bf(g, F.clock);
+    BFT<T> bf;
+    if (g.shear) bf = bf_as<T>(make_bf(g, F.clock));
     // the band of each array; the first backward pass reads nothing outside it
     for (int m = lane; m < NKI; m += 32) {
 #pragma unroll
@@ -368,9 +368,9 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1)
     const C* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
     const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
-    BF bf;
+    BFT<T> bf;
     if constexpr (SHEAR) {
-        if (f >= 3) bf = make_bf(g, F.clock);
+        if (f >= 3) bf = bf_as<T>(make_bf(g, F.clock));
     }
     auto ld = [&](int z, int l) -> C {
         const int i = i0 + l;
@@ -381,12 +381,14 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
         if (i >= nki) return mk(T(0), T(0));
         const long long m = row0 + l * istride + k;
         if (f < 3) return pa[m];
-        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot), FP64 registers
-            const double kv[3] = {(double)i, k2, wvn(k, KK)};
-            const double2 uv[3] = {to_d(F.u[0][m]), to_d(F.u[1][m]), to_d(F.u[2][m])};
-            double2 w3[3];
+        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot), in T
+            const T kv[3] = {(T)i, k2t, (T)wvn(k, KK)};
+            const C zero = mk(T(0), T(0));
+            // omega1 has no term in u1 and omega2 none in u2: those loads are skipped
+            const C uv[3] = {f != 3 ? F.u[0][m] : zero, f != 4 ? F.u[1][m] : zero, F.u[2][m]};
+            C w3[3];
             vort_bf(bf, uv, kv, w3);
-            return from_d<C>(f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]));
+            return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
         } else {
             const T k1 = (T)i, k3 = (T)wvn(k, KK);
             const T ka = (f == 3) ? k2t : ((f == 4) ? k3 : k1);
