@@ -33,7 +33,6 @@ using pdfft::tile_rows;
 extern __shared__ __align__(16) unsigned char pd_smem[];
 template <class C> __device__ __forceinline__ C* smem_as() { return reinterpret_cast<C*>(pd_smem); }
 
-constexpr int L = 8;              // lines per tile of the z and y passes (one 128-byte row)
 
 // K3 holds three complex arrays per warp, so long lines get fewer warps per CTA.
 template <int N> struct Cfg {
@@ -324,25 +323,39 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_c
 
 // ---------------------------------------------------------------------------
 // z and y passes: direct-I/O tile transforms (pdfft::fft_tile_io), one field
-// per CTA, 8 interleaved lines, the first radix pass reading its butterfly
+// per CTA, TCfg::lines interleaved lines, the first radix pass reading its butterfly
 // inputs straight from HBM and the last pass writing its outputs straight to
 // HBM, so a 256-point line crosses shared memory once (one block barrier).
 // ---------------------------------------------------------------------------
 template <int N> struct TCfg {
+    // threads per CTA: one butterfly per thread and pass for a tile of 8 lines
     static constexpr int NT = pdfft::tile_threads<N>();
-    // resident CTAs per SM asked of the register allocator: FP32 tiles need half the
-    // registers and shared memory of FP64 ones
+    // Lines per tile: 8 (FP64: one 128-byte row of complex values, so the quarter
+    // warp of a shared-memory wavefront owns the lines of one butterfly and every
+    // access of a pass is whole rows).  FP32 tiles of 512-point lines take 16 lines,
+    // again a 128-byte row per half-warp wavefront (with 8 the stores of a pass have
+    // two-way bank conflicts and global rows are 64 bytes); elsewhere the doubled
+    // tile costs occupancy (1024) or a half-empty last tile (nkip = 88 at 256) and
+    // measured slower.
+    template <class T> static constexpr int lines() { return (sizeof(T) == 4 && N == 512) ? 16 : 8; }
+    // resident CTAs per SM asked of the register allocator: an FP32 tile of 16 lines
+    // holds the registers and shared memory of an FP64 one, of 8 lines half of them
     template <class T> static constexpr int minb() {
-        return sizeof(T) == 8 ? (NT <= 128 ? (N == 192 ? 4 : 5) : (NT <= 256 ? 2 : (N == 512 ? 2 : 1)))
-                              : (NT <= 128 ? (N == 192 ? 6 : 8) : (NT <= 256 ? 4 : 2));
+        return (sizeof(T) == 8 || lines<T>() == 16) ? (NT <= 128 ? (N == 192 ? 4 : 5) : (NT <= 256 ? 2 : (N == 512 ? 2 : 1)))
+                                                    : (NT <= 128 ? (N == 192 ? 6 : 8) : (NT <= 256 ? 4 : 2));
     }
-    template <class T> static constexpr size_t smem() { return sizeof(typename Cplx<T>::type) * (size_t)N * L; }
+    template <class T> static constexpr size_t smem() { return sizeof(typename Cplx<T>::type) * (size_t)N * lines<T>(); }
+    // tiles along i; with 16 lines the last one may be partial (nkip is a multiple
+    // of 8), and its loads and stores stop at nkip
+    template <class T> static unsigned tiles(const Geo& g) {
+        return (unsigned)((g.nkip + lines<T>() - 1) / lines<T>());
+    }
 };
 
 // K1: spectral velocity and vorticity, backward z transforms.  Field f =
 // blockIdx.x: 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
 // f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
-// f_RK3Derivative 3735-3743), or the BF-rot vorticity; lines i0..i0+7 at one j;
+// f_RK3Derivative 3735-3743), or the BF-rot vorticity; the tile's lines from i0 at one j;
 // k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.
@@ -357,7 +370,9 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int f = blockIdx.x % 6, i0 = blockIdx.y * L, j = blockIdx.z;
+    constexpr int LT = TCfg<NZ>::template lines<T>();
+    const int f = blockIdx.x % 6, i0 = blockIdx.y * LT, j = blockIdx.z;
+    const int lmax = g.nkip - i0;   // lines of this tile inside the i padding
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const double k2 = wvn(j, g.kj);
@@ -399,8 +414,11 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     };
     C* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
     const long long zs = (long long)g.nkj * g.nkip;
-    auto st = [&](int z, int l, C v) { dst[z * zs + l] = v; };
-    pdfft::fft_tile_io<NZ, +1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+    auto st = [&](int z, int l, C v) {
+        if (LT > 8 && l >= lmax) return;
+        dst[z * zs + l] = v;
+    };
+    pdfft::fft_tile_io<NZ, +1, LT, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
@@ -416,18 +434,24 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z % 6;
+    constexpr int LT = TCfg<NY>::template lines<T>();
+    const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % 6;
+    const int lmax = g.nkip - i0;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
     C* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
     auto ld = [&](int y, int l) -> C {
+        if (LT > 8 && l >= lmax) return mk(T(0), T(0));
         if (y <= KJ) return src[y * rs + l];
         if (y >= NY - KJ) return src[(y - NY + NKJ) * rs + l];
         return mk(T(0), T(0));
     };
-    auto st = [&](int y, int l, C v) { dst[y * rs + l] = v; };
-    pdfft::fft_tile_io<NY, +1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+    auto st = [&](int y, int l, C v) {
+        if (LT > 8 && l >= lmax) return;
+        dst[y * rs + l] = v;
+    };
+    pdfft::fft_tile_io<NY, +1, LT, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
 }
 
 // K4: forward y transforms of NL field f = blockIdx.z, truncated to j
@@ -443,17 +467,23 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, z = blockIdx.y, f = blockIdx.z % 3;
+    constexpr int LT = TCfg<NY>::template lines<T>();
+    const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % 3;
+    const int lmax = g.nkip - i0;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
     const C* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
     C* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
-    auto ld = [&](int y, int l) -> C { return src[y * rs + l]; };
+    auto ld = [&](int y, int l) -> C {
+        if (LT > 8 && l >= lmax) return mk(T(0), T(0));
+        return src[y * rs + l];
+    };
     auto st = [&](int y, int l, C v) {
+        if (LT > 8 && l >= lmax) return;
         if (y <= KJ) dst[y * rs + l] = v;
         else if (y >= NY - KJ) dst[(y - NY + NKJ) * rs + l] = v;
     };
-    pdfft::fft_tile_io<NY, -1, L, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+    pdfft::fft_tile_io<NY, -1, LT, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
 }
 
 // K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
@@ -469,7 +499,9 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     C* s = smem_as<C>();
-    const int i0 = blockIdx.x * L, j = blockIdx.y, f = blockIdx.z % 3;
+    constexpr int LT = TCfg<NZ>::template lines<T>();
+    const int i0 = blockIdx.x * LT, j = blockIdx.y, f = blockIdx.z % 3;
+    const int lmax = g.nkip - i0;
     // NL-hat into the y-pencil buffer, or (mode 1) into rk
     Out3<C> nlh;
     for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? F.rk[c] : F.yb + c * g.S;
@@ -479,7 +511,10 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
     C* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
     const long long istride = (long long)g.nkj * NKK;
     const T norm = (T)g.norm;
-    auto ld = [&](int z, int l) -> C { return src[z * zs + l]; };
+    auto ld = [&](int z, int l) -> C {
+        if (LT > 8 && l >= lmax) return mk(T(0), T(0));
+        return src[z * zs + l];
+    };
     auto st = [&](int z, int l, C v) {
         if (i0 + l >= nki) return;
         int k;
@@ -488,7 +523,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
         else return;
         dst[l * istride + k] = mk(v.x * norm, v.y * norm);
     };
-    pdfft::fft_tile_io<NZ, -1, L, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+    pdfft::fft_tile_io<NZ, -1, LT, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -542,7 +577,7 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
-                const dim3 grid(6 * nb, g.nkip / L, g.nkj);                                       \
+                const dim3 grid(6 * nb, TCfg<N>::template tiles<T>(g), g.nkj);                                       \
                 if (g.shear)                                                                      \
                     k_zpass_inv<N, true, T, CAP><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, stage); \
                 else                                                                              \
@@ -562,7 +597,7 @@ template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_inv<N, T, CAP><<<dim3(g.nkip / L, g.nz, 6 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nz, 6 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -596,7 +631,7 @@ template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_fwd<N, T, CAP><<<dim3(g.nkip / L, g.nz, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+                k_ypass_fwd<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nz, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -613,7 +648,7 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int
         e = for_member_sets(M, B, [&](const auto& ms, int nb) {                                   \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_zpass_fwd<N, T, CAP><<<dim3(g.nkip / L, g.nkj, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, mode); \
+                k_zpass_fwd<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nkj, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, mode); \
         });                                                                                       \
         break;
         PD_FOR_EACH_N(PD_L)

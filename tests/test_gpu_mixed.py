@@ -44,6 +44,19 @@ def test_mixed_nonlinear(gpu_lib, n):
     assert e < 1e-5, e
 
 
+@pytest.mark.parametrize("dims", [(64, 512, 16), (64, 16, 512), (512, 16, 16), (16, 1024, 16),
+                                  (16, 16, 1024), (1024, 16, 16), (256, 16, 32), (48, 192, 96)])
+def test_mixed_nonlinear_every_tile_shape(gpu_lib, dims):
+    """Long lines in each direction of the FP32 form, including tiles of 16 lines
+    whose last tile is partial (nkip = 24 at nx = 64)."""
+    p = gpu_lib.workload_params("iso_decay", 32)
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    o, s = _mixed(gpu_lib, p)
+    e = rel_l2_fields(s.nonlinear(), o.nonlinear())
+    s.close()
+    assert e < 1e-5, e
+
+
 def test_mixed_decay_10_steps(gpu_lib):
     p = gpu_lib.workload_params("iso_decay", 64)
     o, s = _mixed(gpu_lib, p)
