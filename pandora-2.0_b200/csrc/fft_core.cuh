@@ -313,6 +313,24 @@ template <int LP, int PS, int AS> PD_HD int tidx(int n, int l) {
     return AS ? l * AS + prow<PS>(n) : prow<PS>(n) * LP + l;
 }
 
+// Twiddles w[r] = tw[r e] (r = 1..R-1) of one butterfly: the entries at power-of-two
+// multiples r = 2^a are read from the table (log2 R loads), the others are products
+// w[2^a] w[r - 2^a] of those (at most log2(R) - 1 roundings on a correctly rounded
+// entry).  The kernels are bound by load instructions and shared/L1 wavefronts, so
+// the table reads are what is saved; the FP arithmetic has room.
+template <int R, class C> PD_HD void twiddles(const C* tw, int e, C* w) {
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+        if ((r & (r - 1)) == 0) {
+            w[r] = tw[r * e];
+        } else {
+            int hb = 1;
+            while (hb * 2 <= r) hb *= 2;
+            w[r] = cmul(w[hb], w[r - hb]);
+        }
+    }
+}
+
 // The band of a 2/3-truncated spectrum on a length-N line: n <= KB or n >= N - KB
 // (KB = 0: the whole line).  A pass_load with KB > 0 reads the elements outside
 // the band as zero without touching shared memory (first pass of a transform of a
@@ -333,8 +351,10 @@ PD_HD void pass_load(const C* s, const C* tw, int w, C* v) {
     if constexpr (NS > 1) {
         const int k = j % NS;
         constexpr int step = N / (NS * R);
+        C wt[R];
+        twiddles<R>(tw, k * step, wt);
 #pragma unroll
-        for (int r = 1; r < R; r++) v[r] = twmul<S>(v[r], tw[r * k * step]);
+        for (int r = 1; r < R; r++) v[r] = twmul<S>(v[r], wt[r]);
     }
     dft<R, S>(v);
 }
