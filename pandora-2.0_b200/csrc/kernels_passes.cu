@@ -125,14 +125,37 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     C* b = F.yb + q * g.nkip;
     BFT<T> bf;
     if (g.shear) bf = bf_as<T>(make_bf(g, F.clock));
-    // the band of each array; the first backward pass reads nothing outside it
-    for (int m = lane; m < NKI; m += 32) {
+    // the band of each array; the first backward pass reads nothing outside it.
+    // From 384 points on (registers to spare at one or two CTAs per SM) the loads
+    // of up to IB rounds of m are issued before any of their stores, so a line waits
+    // on HBM about twice rather than once per round.
+    {
+        constexpr int ITM = (NX / 3 + 1 + 31) / 32;       // rounds of m (NKI = NX/3 + 1)
+        constexpr int IB = NX >= 384 ? (ITM + 1) / 2 : 1;
 #pragma unroll
-        for (int p = 0; p < 3; p++) {
-            C X = b[(2 * p) * fstride + m], Y = b[(2 * p + 1) * fstride + m];
-            if (m == 0) { X.y = T(0); Y.y = T(0); }
-            s[p * XAS + prow<XPS>(m)] = mk(X.x - Y.y, X.y + Y.x);
-            if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
+        for (int i0 = 0; i0 < ITM; i0 += IB) {
+            C X[IB][6];
+#pragma unroll
+            for (int it = 0; it < IB; it++) {
+                const int m = lane + 32 * (i0 + it);
+                if (i0 + it < ITM && m < NKI) {
+#pragma unroll
+                    for (int c = 0; c < 6; c++) X[it][c] = b[c * fstride + m];
+                }
+            }
+#pragma unroll
+            for (int it = 0; it < IB; it++) {
+                const int m = lane + 32 * (i0 + it);
+                if (i0 + it < ITM && m < NKI) {
+#pragma unroll
+                    for (int p = 0; p < 3; p++) {
+                        C Xp = X[it][2 * p], Yp = X[it][2 * p + 1];
+                        if (m == 0) { Xp.y = T(0); Yp.y = T(0); }
+                        s[p * XAS + prow<XPS>(m)] = mk(Xp.x - Yp.y, Xp.y + Yp.x);
+                        if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(Xp.x + Yp.y, -Xp.y + Yp.x);
+                    }
+                }
+            }
         }
     }
     __syncwarp();
