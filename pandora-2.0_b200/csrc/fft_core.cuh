@@ -411,15 +411,16 @@ PD_HD void pass_only(int l, Ld& ld, St& st) {
 
 // Threads per CTA of a direct tile transform of L = 8 lines: one item per thread
 // in the widest pass, at most 512.
-template <int N> constexpr int tile_items_max() {
-    constexpr int a = N / Plan<N>::r0;
-    constexpr int b = Plan<N>::r1 ? N / Plan<N>::r1 : 0;
-    constexpr int c = Plan<N>::r2 ? N / Plan<N>::r2 : 0;
-    return 8 * (a > b ? (a > c ? a : c) : (b > c ? b : c));
+// Threads of a tile transform of 8 lines with the radix plan (R0, R1, R2): one
+// butterfly per thread in the pass with the most, 64..512.
+template <int N, int R0, int R1, int R2> constexpr int tile_threads_for() {
+    constexpr int a = N / R0;
+    constexpr int b = R1 ? N / R1 : 0;
+    constexpr int c = R2 ? N / R2 : 0;
+    constexpr int m = 8 * (a > b ? (a > c ? a : c) : (b > c ? b : c));
+    return m < 64 ? 64 : (m > 512 ? 512 : m);
 }
-template <int N> constexpr int tile_threads() {
-    return tile_items_max<N>() < 64 ? 64 : (tile_items_max<N>() > 512 ? 512 : tile_items_max<N>());
-}
+template <int N> constexpr int tile_threads() { return tile_threads_for<N, Plan<N>::r0, Plan<N>::r1, Plan<N>::r2>(); }
 
 // Radix schedule of the warp-level transforms (one line per warp): radix 8 where
 // possible so that a pass has N/8 items, about one per lane.
@@ -579,13 +580,14 @@ __device__ __forceinline__ void pass(C* s, const C* __restrict__ tw, int tid) {
     __syncthreads();
 }
 
-// Direct tile transform of L interleaved lines by NT threads (see pass_first).
-// The caller makes `s` free before the call (a barrier after any earlier use);
-// on return other threads may still read `s`.
-template <int N, int S, int L, int NT, class C, class Ld, class St>
+// Direct tile transform of L interleaved lines by NT threads (see pass_first) with
+// the radix plan (R0, R1, R2), by default Plan<N>.  The caller makes `s` free
+// before the call (a barrier after any earlier use); on return other threads may
+// still read `s`.
+template <int N, int S, int L, int NT, int R0 = Plan<N>::r0, int R1 = Plan<N>::r1, int R2 = Plan<N>::r2,
+          class C, class Ld, class St>
 __device__ __forceinline__ void fft_tile_io(C* s, const C* __restrict__ tw, int tid, Ld& ld, St& st) {
-    static_assert(plan_ok<N>(), "no radix plan for this length");
-    constexpr int R0 = Plan<N>::r0, R1 = Plan<N>::r1, R2 = Plan<N>::r2;
+    static_assert(R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) == N, "radix plan does not factor N");
     if constexpr (R1 == 0) {
         for (int l = tid; l < L; l += NT) pass_only<N, S, L>(l, ld, st);
     } else {

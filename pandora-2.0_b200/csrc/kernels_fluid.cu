@@ -46,44 +46,72 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
     BF bf;
     if (g.shear) bf = make_bf(g, F.clock);
     double p11 = 0, p22 = 0, p33 = 0;
-    const long long total = g.S;
-    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < total;
-         m += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(m % g.nkk);
-        const long long ij = m / g.nkk;
-        const int jj = (int)(ij % g.nkj), i = (int)(ij / g.nkj);
-        double kv[3] = {(double)i, wvn(jj, g.kj), wvn(k, g.kk)};
-        double2 uv[3] = {to_d(F.u[0][m]), to_d(F.u[1][m]), to_d(F.u[2][m])};
-        if (g.shear) {
-            double kl[3] = {0.0, 0.0, 0.0};
-            double2 ul[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    // one warp per (i, j) row of k; lanes take 32 consecutive k at a time.  Along a
+    // row the shell index is monotone on each half of k, so the lanes of a shell
+    // form runs: a segmented sum over the runs leaves one shared-memory update per
+    // run instead of one per mode.
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int NKK = g.nkk;
+    const long long rows = (long long)g.nki * g.nkj;
+    for (long long r = (long long)blockIdx.x * nw + wib; r < rows; r += (long long)gridDim.x * nw) {
+        const int i = (int)(r / g.nkj), jj = (int)(r - (long long)i * g.nkj);
+        const double k1 = (double)i, k2 = wvn(jj, g.kj);
+        const double wgt = (i != 0) ? 2.0 : 1.0;
+        for (int k0 = 0; k0 < NKK; k0 += 32) {
+            const int k = k0 + lane;
+            double e = 0.0, d = 0.0;
+            int q = -1;   // shell, -1: none
+            if (k < NKK) {
+                const long long m = r * NKK + k;
+                double kv[3] = {k1, k2, wvn(k, g.kk)};
+                double2 uv[3] = {to_d(F.u[0][m]), to_d(F.u[1][m]), to_d(F.u[2][m])};
+                if (g.shear) {
+                    double kl[3] = {0.0, 0.0, 0.0};
+                    double2 ul[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
 #pragma unroll
-            for (int a = 0; a < 3; a++)
+                    for (int a = 0; a < 3; a++)
 #pragma unroll
-                for (int b = 0; b < 3; b++)
-                    if (bex(a, b)) {
-                        kl[b] += bf.bm[a][b] * kv[a];
-                        ul[a].x += bf.bi[a][b] * uv[b].x;
-                        ul[a].y += bf.bi[a][b] * uv[b].y;
-                    }
+                        for (int b = 0; b < 3; b++)
+                            if (bex(a, b)) {
+                                kl[b] += bf.bm[a][b] * kv[a];
+                                ul[a].x += bf.bi[a][b] * uv[b].x;
+                                ul[a].y += bf.bi[a][b] * uv[b].y;
+                            }
 #pragma unroll
-            for (int a = 0; a < 3; a++) { kv[a] = kl[a]; uv[a] = ul[a]; }
-        }
-        const double km = sqrt((kv[0] * kv[0]) + (kv[1] * kv[1]) + (kv[2] * kv[2]));
-        double q11 = uv[0].x * uv[0].x + uv[0].y * uv[0].y, q22 = uv[1].x * uv[1].x + uv[1].y * uv[1].y;
-        double q33 = uv[2].x * uv[2].x + uv[2].y * uv[2].y;
-        if (i != 0) { q11 *= 2.0; q22 *= 2.0; q33 *= 2.0; }
-        p11 += q11; p22 += q22; p33 += q33;
-        const double e = 0.5 * (q11 + q22 + q33);
-        if (!isfinite(e)) atomicOr(&F.clock->status, PD_ST_NAN);
-        const double d = 2.0 * km * km * g.nu * e;
-        const int kc = (int)floor(km + 0.5);
-        for (int q = kc - 1; q <= kc + 1; q++) {
-            if (q < 1 || q > K) continue;
-            if (km >= (double)q - 0.5 && km < (double)q + 0.5) {
+                    for (int a = 0; a < 3; a++) { kv[a] = kl[a]; uv[a] = ul[a]; }
+                }
+                const double km = sqrt((kv[0] * kv[0]) + (kv[1] * kv[1]) + (kv[2] * kv[2]));
+                double q11 = uv[0].x * uv[0].x + uv[0].y * uv[0].y, q22 = uv[1].x * uv[1].x + uv[1].y * uv[1].y;
+                double q33 = uv[2].x * uv[2].x + uv[2].y * uv[2].y;
+                if (i != 0) { q11 *= 2.0; q22 *= 2.0; q33 *= 2.0; }
+                p11 += q11; p22 += q22; p33 += q33;
+                e = 0.5 * (q11 + q22 + q33);
+                if (!isfinite(e)) atomicOr(&F.clock->status, PD_ST_NAN);
+                d = 2.0 * km * km * g.nu * e;
+                // bin [q - 1/2, q + 1/2), q = 1..K
+                int qc = (int)floor(km + 0.5);
+                if (km < (double)qc - 0.5) qc--;
+                else if (km >= (double)qc + 0.5) qc++;
+                if (qc >= 1 && qc <= K) q = qc;
+            }
+            // runs of equal q in lane order: start lane of this lane's run
+            const int prevq = __shfl_up_sync(0xffffffffu, q, 1);
+            int start = (lane == 0 || prevq != q) ? lane : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) start = max(start, __shfl_up_sync(0xffffffffu, start, o));
+            double c = (q >= 0) ? wgt : 0.0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double e2 = __shfl_up_sync(0xffffffffu, e, o), d2 = __shfl_up_sync(0xffffffffu, d, o);
+                const double c2 = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane - o >= start) { e += e2; d += d2; c += c2; }
+            }
+            const int nextq = __shfl_down_sync(0xffffffffu, q, 1);
+            const bool last = (lane == 31) || (nextq != q);
+            if (last && q >= 1) {
                 atomicAdd(&se[q], e);
                 atomicAdd(&sd[q], d);
-                if (g.shear) atomicAdd(&sc[q], (i != 0) ? 2.0 : 1.0);
+                if (g.shear) atomicAdd(&sc[q], c);
             }
         }
     }

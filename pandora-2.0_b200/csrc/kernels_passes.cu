@@ -350,9 +350,17 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_c
 // inputs straight from HBM and the last pass writing its outputs straight to
 // HBM, so a 256-point line crosses shared memory once (one block barrier).
 // ---------------------------------------------------------------------------
-template <int N> struct TCfg {
-    // threads per CTA: one butterfly per thread and pass for a tile of 8 lines
-    static constexpr int NT = pdfft::tile_threads<N>();
+template <int N, bool TWO = false> struct TCfg {
+    // Radix plan: Plan<N>, or with TWO (the y passes and K5a) for FP32 512-point
+    // lines the two-pass (32, 16): one shared-memory round trip instead of two.  An
+    // FP64 item of radix 32 does not fit the registers of two CTAs per SM, and K1
+    // (vorticity loads in its first pass) measured slower with it.
+    template <class T> static constexpr bool two() { return TWO && sizeof(T) == 4 && N == 512; }
+    template <class T> static constexpr int r0() { return two<T>() ? 32 : pdfft::Plan<N>::r0; }
+    template <class T> static constexpr int r1() { return two<T>() ? 16 : pdfft::Plan<N>::r1; }
+    template <class T> static constexpr int r2() { return two<T>() ? 0 : pdfft::Plan<N>::r2; }
+    // threads per CTA: one butterfly per thread in the widest pass of a tile of 8 lines
+    template <class T> static constexpr int nt() { return pdfft::tile_threads_for<N, r0<T>(), r1<T>(), r2<T>()>(); }
     // Lines per tile: 8 (FP64: one 128-byte row of complex values, so the quarter
     // warp of a shared-memory wavefront owns the lines of one butterfly and every
     // access of a pass is whole rows).  FP32 tiles of 512-point lines take 16 lines,
@@ -364,6 +372,7 @@ template <int N> struct TCfg {
     // resident CTAs per SM asked of the register allocator: an FP32 tile of 16 lines
     // holds the registers and shared memory of an FP64 one, of 8 lines half of them
     template <class T> static constexpr int minb() {
+        constexpr int NT = nt<T>();
         return (sizeof(T) == 8 || lines<T>() == 16) ? (NT <= 128 ? (N == 192 ? 4 : 5) : (NT <= 256 ? 2 : (N == 512 ? 2 : 1)))
                                                     : (NT <= 128 ? (N == 192 ? 6 : 8) : (NT <= 256 ? 4 : 2));
     }
@@ -372,6 +381,11 @@ template <int N> struct TCfg {
     // of 8), and its loads and stores stop at nkip
     template <class T> static unsigned tiles(const Geo& g) {
         return (unsigned)((g.nkip + lines<T>() - 1) / lines<T>());
+    }
+    template <int S, int L, class C, class Ld, class St>
+    static __device__ __forceinline__ void transform(C* s, const C* tw, Ld& ld, St& st) {
+        using T = pdfft::real_of<C>;
+        pdfft::fft_tile_io<N, S, L, nt<T>(), r0<T>(), r1<T>(), r2<T>()>(s, tw, threadIdx.x, ld, st);
     }
 };
 
@@ -383,7 +397,7 @@ template <int N> struct TCfg {
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.
 template <int NZ, bool SHEAR, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+__global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / 6];
     if (!mm.active) return;
@@ -441,13 +455,13 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
         if (LT > 8 && l >= lmax) return;
         dst[z * zs + l] = v;
     };
-    pdfft::fft_tile_io<NZ, +1, LT, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+    TCfg<NZ>::template transform<+1, LT>(s, F.tw_z, ld, st);
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
 // [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).
 template <int NY, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
+__global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 6];
     if (!mm.active) return;
@@ -474,13 +488,13 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
         if (LT > 8 && l >= lmax) return;
         dst[y * rs + l] = v;
     };
-    pdfft::fft_tile_io<NY, +1, LT, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+    TCfg<NY, true>::template transform<+1, LT>(s, F.tw_y, ld, st);
 }
 
 // K4: forward y transforms of NL field f = blockIdx.z, truncated to j
 // (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
 template <int NY, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_ypass_fwd(const __grid_constant__ MemberSet<T, CAP> ms) {
+__global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_fwd(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
     if (!mm.active) return;
@@ -506,13 +520,13 @@ __global__ void __launch_bounds__(TCfg<NY>::NT, TCfg<NY>::template minb<T>()) k_
         if (y <= KJ) dst[y * rs + l] = v;
         else if (y >= NY - KJ) dst[(y - NY + NKJ) * rs + l] = v;
     };
-    pdfft::fft_tile_io<NY, -1, LT, TCfg<NY>::NT>(s, F.tw_y, threadIdx.x, ld, st);
+    TCfg<NY, true>::template transform<-1, LT>(s, F.tw_y, ld, st);
 }
 
 // K5a: forward z transforms of NL field f = blockIdx.z, x 1/(NX NY NZ), truncated
 // to k, stored as rows of NL-hat [c][i][j][k].
 template <int NZ, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_zpass_fwd(const __grid_constant__ MemberSet<T, CAP> ms, int mode) {
+__global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, true>::template minb<T>()) k_zpass_fwd(const __grid_constant__ MemberSet<T, CAP> ms, int mode) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
     if (!mm.active) return;
@@ -546,7 +560,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::NT, TCfg<NZ>::template minb<T>()) k_
         else return;
         dst[l * istride + k] = mk(v.x * norm, v.y * norm);
     };
-    pdfft::fft_tile_io<NZ, -1, LT, TCfg<NZ>::NT>(s, F.tw_z, threadIdx.x, ld, st);
+    TCfg<NZ, true>::template transform<-1, LT>(s, F.tw_z, ld, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -569,11 +583,11 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
     if (g.nz == N) {                                                                           \
         if ((e = set_smem(k_zpass_inv<N, false, T, CAP>, TCfg<N>::template smem<T>()))) return e; \
         if ((e = set_smem(k_zpass_inv<N, true, T, CAP>, TCfg<N>::template smem<T>()))) return e;  \
-        if ((e = set_smem(k_zpass_fwd<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
+        if ((e = set_smem(k_zpass_fwd<N, T, CAP>, TCfg<N, true>::template smem<T>()))) return e;        \
     }                                                                                          \
     if (g.ny == N) {                                                                           \
-        if ((e = set_smem(k_ypass_inv<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
-        if ((e = set_smem(k_ypass_fwd<N, T, CAP>, TCfg<N>::template smem<T>()))) return e;        \
+        if ((e = set_smem(k_ypass_inv<N, T, CAP>, TCfg<N, true>::template smem<T>()))) return e;        \
+        if ((e = set_smem(k_ypass_fwd<N, T, CAP>, TCfg<N, true>::template smem<T>()))) return e;        \
     }                                                                                          \
     if (g.nx == N) {                                                                           \
         if ((e = set_smem(k_xpass<N, T, CAP>, smem_kx<N, T>()))) return e;                     \
@@ -602,9 +616,9 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
                 const dim3 grid(6 * nb, TCfg<N>::template tiles<T>(g), g.nkj);                                       \
                 if (g.shear)                                                                      \
-                    k_zpass_inv<N, true, T, CAP><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, stage); \
+                    k_zpass_inv<N, true, T, CAP><<<grid, TCfg<N>::template nt<T>(), TCfg<N>::template smem<T>(), st>>>(ms, stage); \
                 else                                                                              \
-                    k_zpass_inv<N, false, T, CAP><<<grid, TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, stage); \
+                    k_zpass_inv<N, false, T, CAP><<<grid, TCfg<N>::template nt<T>(), TCfg<N>::template smem<T>(), st>>>(ms, stage); \
             }                                                                                     \
         });
         PD_FOR_EACH_N(PD_L)
@@ -620,7 +634,7 @@ template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nz, 6 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, 6 * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -654,7 +668,7 @@ template <class T> cudaError_t launch_ypass_fwd(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_fwd<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nz, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms); \
+                k_ypass_fwd<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, 3 * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -671,7 +685,7 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int
         e = for_member_sets(M, B, [&](const auto& ms, int nb) {                                   \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_zpass_fwd<N, T, CAP><<<dim3(TCfg<N>::template tiles<T>(g), g.nkj, 3 * nb), TCfg<N>::NT, TCfg<N>::template smem<T>(), st>>>(ms, mode); \
+                k_zpass_fwd<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nkj, 3 * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms, mode); \
         });                                                                                       \
         break;
         PD_FOR_EACH_N(PD_L)
