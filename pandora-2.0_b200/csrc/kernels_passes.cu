@@ -101,7 +101,8 @@ __device__ __forceinline__ C nl_point(const BFT<T>& bf, bool shear, T u1, T u2, 
 template <int NX, class T, int CAP>
 __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                         int want_phys,
-                                                                                        int want_cfl) {
+                                                                                        int want_cfl,
+                                                                                        long long pf_lines) {
     using C = typename FieldsT<T>::C;
     using XP = pdfft::FusedPlan<NX>;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
@@ -222,6 +223,15 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
         if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
+    }
+    // The six input rows of line q + pf_lines (a wave of resident CTAs later, so
+    // the CTA that takes it starts about when this one ends) are prefetched into
+    // L2, one bulk prefetch per row, while this line's forward transforms run:
+    // that CTA's loads then wait on L2 rather than HBM.
+    if (pf_lines > 0 && q + pf_lines < lines && lane < 6) {
+        const C* row = F.yb + lane * fstride + (q + pf_lines) * g.nkip;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"((unsigned)(NKI * sizeof(C)))
+                     : "memory");
     }
     // forward transforms of the product arrays; only the band is written
     constexpr int F0 = XP::f0, F1 = XP::f1, F2 = XP::f2, P0 = XP::fused ? 1 : 0;
@@ -570,6 +580,18 @@ template <int N, class T> static size_t smem_kx() {
     return sizeof(typename Cplx<T>::type) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
 }
 
+// CTAs of `kernel` resident on the whole device at once.
+template <typename K> static long long resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0, nsm = 1, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        per = 1;
+    }
+    return (long long)nsm * per;
+}
+
 template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
@@ -652,7 +674,9 @@ cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys,
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
                 const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                     \
-                k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl); \
+                /* L2 prefetch distance: one wave of resident CTAs (single simulations) */      \
+                const long long pf = CAP == 1 ? Cfg<N>::NWX * resident_ctas(k_xpass<N, T, CAP>, 32 * Cfg<N>::NWX, smem_kx<N, T>()) : 0; \
+                k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl, pf); \
             }                                                                                     \
         });
         PD_FOR_EACH_N(PD_L)
