@@ -583,18 +583,25 @@ __device__ __forceinline__ void pass(C* s, const C* __restrict__ tw, int tid) {
 // Direct tile transform of L interleaved lines by NT threads (see pass_first) with
 // the radix plan (R0, R1, R2), by default Plan<N>.  The caller makes `s` free
 // before the call (a barrier after any earlier use); on return other threads may
-// still read `s`.
+// still read `s`.  `mid()` runs once per thread after the first pass (the loads
+// of the tile are done and the remaining passes are shared-memory work).
+struct NoMid {
+    __device__ void operator()() const {}
+};
 template <int N, int S, int L, int NT, int R0 = Plan<N>::r0, int R1 = Plan<N>::r1, int R2 = Plan<N>::r2,
-          class C, class Ld, class St>
-__device__ __forceinline__ void fft_tile_io(C* s, const C* __restrict__ tw, int tid, Ld& ld, St& st) {
+          class C, class Ld, class St, class Mid = NoMid>
+__device__ __forceinline__ void fft_tile_io(C* s, const C* __restrict__ tw, int tid, Ld& ld, St& st,
+                                            const Mid& mid = Mid()) {
     static_assert(R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) == N, "radix plan does not factor N");
     if constexpr (R1 == 0) {
+        mid();
         for (int l = tid; l < L; l += NT) pass_only<N, S, L>(l, ld, st);
     } else {
         constexpr int W0 = (N / R0) * L;
 #pragma unroll
         for (int w = tid; w < W0; w += NT) pass_first<N, R0, S, L>(s, w, ld);
         __syncthreads();
+        mid();
         if constexpr (R2 != 0) pass<N, R1, R0, S, L, L, NT>(s, tw, tid);   // in place, ends with a barrier
         constexpr int RL = R2 ? R2 : R1;
         constexpr int WL = (N / RL) * L;

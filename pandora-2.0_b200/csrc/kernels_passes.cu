@@ -76,6 +76,15 @@ bool supported_length(int n) {
 // kernel is bound by shared-memory wavefronts, and each pass is a full read and
 // write of the three arrays.
 // ---------------------------------------------------------------------------
+// Bulk prefetch of [p, p + bytes) into L2 (a hint: no data moves to the SM),
+// trimmed inward to the 16-byte boundaries the bulk copy requires.
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+    unsigned long long a = (unsigned long long)p, e = a + bytes;
+    a = (a + 15) & ~15ull;
+    e &= ~15ull;
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+
 template <int N> constexpr int xps() {
     return (N == 16 || N == 32 || N == 48) ? 2
          : ((N == 24 || N == 64 || N == 96) ? 3 : ((N == 384 || N == 512 || N == 1024) ? 5 : 4));
@@ -228,11 +237,8 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     // the CTA that takes it starts about when this one ends) are prefetched into
     // L2, one bulk prefetch per row, while this line's forward transforms run:
     // that CTA's loads then wait on L2 rather than HBM.
-    if (pf_lines > 0 && q + pf_lines < lines && lane < 6) {
-        const C* row = F.yb + lane * fstride + (q + pf_lines) * g.nkip;
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"((unsigned)(NKI * sizeof(C)))
-                     : "memory");
-    }
+    if (pf_lines > 0 && q + pf_lines < lines && lane < 6)
+        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
     // forward transforms of the product arrays; only the band is written
     constexpr int F0 = XP::f0, F1 = XP::f1, F2 = XP::f2, P0 = XP::fused ? 1 : 0;
     if constexpr (NA == 2) {
@@ -392,10 +398,10 @@ template <int N, bool TWO = false> struct TCfg {
     template <class T> static unsigned tiles(const Geo& g) {
         return (unsigned)((g.nkip + lines<T>() - 1) / lines<T>());
     }
-    template <int S, int L, class C, class Ld, class St>
-    static __device__ __forceinline__ void transform(C* s, const C* tw, Ld& ld, St& st) {
+    template <int S, int L, class C, class Ld, class St, class Mid = pdfft::NoMid>
+    static __device__ __forceinline__ void transform(C* s, const C* tw, Ld& ld, St& st, const Mid& mid = Mid()) {
         using T = pdfft::real_of<C>;
-        pdfft::fft_tile_io<N, S, L, nt<T>(), r0<T>(), r1<T>(), r2<T>()>(s, tw, threadIdx.x, ld, st);
+        pdfft::fft_tile_io<N, S, L, nt<T>(), r0<T>(), r1<T>(), r2<T>()>(s, tw, threadIdx.x, ld, st, mid);
     }
 };
 
@@ -407,7 +413,8 @@ template <int N, bool TWO = false> struct TCfg {
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.
 template <int NZ, bool SHEAR, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+__global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
+                                                                                                   long long pf_ctas) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / 6];
     if (!mm.active) return;
@@ -465,7 +472,27 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
         if (LT > 8 && l >= lmax) return;
         dst[z * zs + l] = v;
     };
-    TCfg<NZ>::template transform<+1, LT>(s, F.tw_z, ld, st);
+    // After the first pass: prefetch into L2 the velocity rows of the CTA a wave of
+    // resident CTAs later (single simulations: blocks (f, tile, j) in launch order),
+    // so that its loads wait on L2 rather than HBM.  A vorticity CTA's rows are all
+    // three components.
+    const C* const u0 = F.u[0];
+    const C* const u1 = F.u[1];
+    const C* const u2 = F.u[2];
+    const int nkj = g.nkj;
+    auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2]() {
+        if (pf_ctas <= 0) return;
+        const long long nblk = 6LL * gridDim.y * gridDim.z;
+        const long long nxt = blockIdx.x + 6LL * (blockIdx.y + (long long)gridDim.y * blockIdx.z) + pf_ctas;
+        if (nxt >= nblk) return;
+        const int f2 = (int)(nxt % 6), ti = (int)((nxt / 6) % gridDim.y), j2 = (int)(nxt / (6LL * gridDim.y));
+        const int nc = f2 < 3 ? 1 : 3, t = threadIdx.x;
+        if (t >= LT * nc) return;
+        const int c = f2 < 3 ? f2 : t / LT, i = ti * LT + t % LT;
+        const C* uc = c == 0 ? u0 : (c == 1 ? u1 : u2);
+        if (i < nki) prefetch_l2(uc + ((long long)i * nkj + j2) * NKK, NKK * sizeof(C));
+    };
+    TCfg<NZ>::template transform<+1, LT>(s, F.tw_z, ld, st, mid);
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
@@ -637,10 +664,15 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
                 const dim3 grid(6 * nb, TCfg<N>::template tiles<T>(g), g.nkj);                                       \
-                if (g.shear)                                                                      \
-                    k_zpass_inv<N, true, T, CAP><<<grid, TCfg<N>::template nt<T>(), TCfg<N>::template smem<T>(), st>>>(ms, stage); \
-                else                                                                              \
-                    k_zpass_inv<N, false, T, CAP><<<grid, TCfg<N>::template nt<T>(), TCfg<N>::template smem<T>(), st>>>(ms, stage); \
+                constexpr int NT = TCfg<N>::template nt<T>();                                      \
+                const size_t sm = TCfg<N>::template smem<T>();                                     \
+                if (g.shear) {                                                                    \
+                    const long long pf = CAP == 1 ? resident_ctas(k_zpass_inv<N, true, T, CAP>, NT, sm) : 0; \
+                    k_zpass_inv<N, true, T, CAP><<<grid, NT, sm, st>>>(ms, stage, pf);            \
+                } else {                                                                          \
+                    const long long pf = CAP == 1 ? resident_ctas(k_zpass_inv<N, false, T, CAP>, NT, sm) : 0; \
+                    k_zpass_inv<N, false, T, CAP><<<grid, NT, sm, st>>>(ms, stage, pf);           \
+                }                                                                                 \
             }                                                                                     \
         });
         PD_FOR_EACH_N(PD_L)
