@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 #include <math.h>
+#include <algorithm>
+#include <atomic>
 #include <type_traits>
 #include "fft_core.cuh"
 #include "pandora_internal.cuh"
@@ -21,12 +23,30 @@ using pdfft::mk;
 // ---------------------------------------------------------------------------
 size_t shell_words(const Geo& g) { return (size_t)3 * (g.kkmax + 1) + 3; }
 
+// Compensated (Neumaier) accumulation: s + c carries the sum of the added terms
+// to about one rounding, whatever their count and order of magnitude.
+__device__ __forceinline__ void neumaier(double& s, double& c, double x) {
+    const double t = s + x;
+    c += (fabs(s) >= fabs(x)) ? ((s - t) + x) : ((x - t) + s);
+    s = t;
+}
+
 // Shear flow: the same sums in the laboratory frame, k_lab = B^T k and
 // u_lab = B^-1 u (f_FluidstatsFsPrimaryQuantsBFRot, src/pf_fluidstats.f90:1586-1960),
 // with the per-shell mode counts of f_FluidstatsModeDensityBFRot
 // (src/pf_fluidstats.f90:1977-2229), which change with B every step.
+//
+// Two launches.  k_stats: G CTAs of 8 warps, CTA b owning the contiguous rows
+// [b R / G, (b+1) R / G) of (i, j), one warp per row, 32 consecutive k at a time.
+// Along a row the shell index is monotone on each half of k, so the lanes of a shell
+// form runs; a segmented sum over the runs (a fixed shuffle tree) leaves one
+// shared-memory update per run.  Each CTA writes its sums to the free y-pencil
+// buffer (G x nsh doubles).  k_stats_reduce adds the G partial sums of every output
+// word in CTA order with Neumaier compensation: the cross-CTA sum, where the terms
+// are many and of every size, carries about one rounding, and the result does not
+// depend on the order in which CTAs finish.
 template <class T, int CAP>
-__global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet<T, CAP> ms) {
+__global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet<T, CAP> ms, int G) {
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
@@ -46,14 +66,11 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
     BF bf;
     if (g.shear) bf = make_bf(g, F.clock);
     double p11 = 0, p22 = 0, p33 = 0;
-    // one warp per (i, j) row of k; lanes take 32 consecutive k at a time.  Along a
-    // row the shell index is monotone on each half of k, so the lanes of a shell
-    // form runs: a segmented sum over the runs leaves one shared-memory update per
-    // run instead of one per mode.
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int NKK = g.nkk;
     const long long rows = (long long)g.nki * g.nkj;
-    for (long long r = (long long)blockIdx.x * nw + wib; r < rows; r += (long long)gridDim.x * nw) {
+    const long long r0 = rows * blockIdx.x / G, r1 = rows * (blockIdx.x + 1) / G;
+    for (long long r = r0 + wib; r < r1; r += nw) {
         const int i = (int)(r / g.nkj), jj = (int)(r - (long long)i * g.nkj);
         const double k1 = (double)i, k2 = wvn(jj, g.kj);
         const double wgt = (i != 0) ? 2.0 : 1.0;
@@ -107,8 +124,7 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
                 if (lane - o >= start) { e += e2; d += d2; c += c2; }
             }
             const int nextq = __shfl_down_sync(0xffffffffu, q, 1);
-            const bool last = (lane == 31) || (nextq != q);
-            if (last && q >= 1) {
+            if (((lane == 31) || (nextq != q)) && q >= 1) {
                 atomicAdd(&se[q], e);
                 atomicAdd(&sd[q], d);
                 if (g.shear) atomicAdd(&sc[q], c);
@@ -119,8 +135,37 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
     atomicAdd(&sp[1], p22);
     atomicAdd(&sp[2], p33);
     __syncthreads();
-    for (int q = threadIdx.x; q < nsh; q += blockDim.x)
-        if (sh[q] != 0.0) atomicAdd(&F.shell[q], sh[q]);
+    double* part = reinterpret_cast<double*>(F.yb) + (size_t)blockIdx.x * nsh;
+    for (int q = threadIdx.x; q < nsh; q += blockDim.x) part[q] = sh[q];
+}
+
+// One CTA per 32 output words: lane l of warp v adds, compensated, the partials of
+// word w0 + l from CTAs v, v + 8, v + 16, ...; the 8 pairs of a word then fold in warp
+// order.
+template <class T, int CAP>
+__global__ void __launch_bounds__(256) k_stats_reduce(const __grid_constant__ MemberSet<T, CAP> ms, int G) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
+    const FieldsT<T> F = mm.F;
+    const int nsh = 3 * (mm.g.kkmax + 1) + 3;
+    __shared__ double ps[8][32], pc[8][32];
+    const int lane = threadIdx.x & 31, v = threadIdx.x >> 5;
+    const int w = blockIdx.x * 32 + lane;
+    const double* part = reinterpret_cast<const double*>(F.yb);
+    double s = 0.0, c = 0.0;
+    if (w < nsh)
+        for (int b = v; b < G; b += 8) neumaier(s, c, part[(size_t)b * nsh + w]);
+    ps[v][lane] = s;
+    pc[v][lane] = c;
+    __syncthreads();
+    if (v == 0 && w < nsh) {
+        double S = 0.0, Cc = 0.0;
+        for (int u = 0; u < 8; u++) { neumaier(S, Cc, ps[u][lane]); Cc += pc[u][lane]; }
+        F.shell[w] = S + Cc;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -530,20 +575,25 @@ static int sm_count() {
     return n;
 }
 
-// The shell sums of every member start at zero: `shell` is the first member's
-// buffer, members' buffers are contiguous (B x shell_words).
+// Statistics of every member into its own F.shell (shell_words doubles); the
+// per-CTA partial sums live in the member's y-pencil buffer, free at stage 1 and
+// between steps.
 template <class T>
 cudaError_t launch_stats(const Geo& g, const Member<T>* M, int B, double* shell, cudaStream_t st) {
+    (void)shell;
     const size_t nsh = shell_words(g);
-    cudaError_t e = cudaMemsetAsync(shell, 0, sizeof(double) * nsh * B, st);
+    const long long rows = (long long)g.nki * g.nkj;
+    const size_t yb_bytes = sizeof(typename Cplx<T>::type) * 6 * (size_t)g.nz * g.ny * g.nkip;
+    long long G = std::min<long long>(4LL * sm_count(), std::max<long long>(1, rows / 8));
+    G = std::min<long long>(G, (long long)(yb_bytes / (sizeof(double) * nsh)));
+    if (G < 1) return cudaErrorInvalidValue;
+    const int gi = (int)G;
+    cudaError_t e = for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_stats<T, PD_CAP(ms)><<<dim3((unsigned)gi, nm), 256, sizeof(double) * nsh, st>>>(ms, gi);
+    });
     if (e) return e;
-    long long nb = (g.S + 255) / 256;
-    const long long cap = 4LL * sm_count();
-    if (nb > cap) nb = cap;
-    // each launch's members take consecutive shell blocks (member i of a chunk uses its
-    // own F.shell, which the batch points into `shell`)
     return for_member_sets(M, B, [&](const auto& ms, int nm) {
-        k_stats<T, PD_CAP(ms)><<<dim3((unsigned)nb, nm), 256, sizeof(double) * nsh, st>>>(ms);
+        k_stats_reduce<T, PD_CAP(ms)><<<dim3((unsigned)((nsh + 31) / 32), nm), 256, 0, st>>>(ms, gi);
     });
 }
 
@@ -554,14 +604,28 @@ static size_t stage_scalars_smem(const Geo& g, const ForceParams& fp) {
     return sizeof(double) * 2 * (size_t)fp.calls_per_stage + sizeof(double2) * 3 * (size_t)fw * fw;
 }
 
+// The dynamic shared memory limits only ever grow: the attribute is per function for
+// the whole process, and handles of several geometries live side by side.
+template <typename K> static cudaError_t raise_smem(K kernel, int bytes, std::atomic<int>& have) {
+    int cur = have.load();
+    if (bytes <= cur) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        while (cur < bytes && !have.compare_exchange_weak(cur, bytes)) {}
+    return e;
+}
+
 cudaError_t configure_fluid_kernels(const Geo& g, const ForceParams& fp) {
+    static std::atomic<int> ss[4], st[4];   // zero-initialised (static storage)
     const int b = (int)stage_scalars_smem(g, fp);
+    const int bs = (int)(sizeof(double) * shell_words(g));   // statistics' shell sums
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_stage_scalars<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)) ||
-        (e = cudaFuncSetAttribute(k_stage_scalars<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)) ||
-        (e = cudaFuncSetAttribute(k_stage_scalars<double, kBatchChunk>, cudaFuncAttributeMaxDynamicSharedMemorySize, b)))
+    if ((e = raise_smem(k_stage_scalars<double, 1>, b, ss[0])) || (e = raise_smem(k_stage_scalars<float, 1>, b, ss[1])) ||
+        (e = raise_smem(k_stage_scalars<double, kBatchChunk>, b, ss[2])) ||
+        (e = raise_smem(k_stage_scalars<float, kBatchChunk>, b, ss[3])) || (e = raise_smem(k_stats<double, 1>, bs, st[0])) ||
+        (e = raise_smem(k_stats<float, 1>, bs, st[1])) || (e = raise_smem(k_stats<double, kBatchChunk>, bs, st[2])))
         return e;
-    return cudaFuncSetAttribute(k_stage_scalars<float, kBatchChunk>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return raise_smem(k_stats<float, kBatchChunk>, bs, st[3]);
 }
 
 template <class T>

@@ -304,8 +304,12 @@ def serial_baseline(requests: list[Request]) -> dict:
             per_class[k] = _plain_run(r)
     secs = sum(per_class[class_key(r.params) + (r.steps,)] for r in requests)
     pts = sum(r.points * r.steps for r in requests)
+    by_size: dict[int, float] = collections.defaultdict(float)   # serial seconds per grid size
+    for r in requests:
+        by_size[r.params.nodes_x] += per_class[class_key(r.params) + (r.steps,)]
     return {"requests": len(requests), "classes_timed": len(per_class), "seconds": secs,
-            "member_steps_per_s": sum(r.steps for r in requests) / secs, "mpts_rk3steps_per_s": pts / secs / 1e6}
+            "member_steps_per_s": sum(r.steps for r in requests) / secs, "mpts_rk3steps_per_s": pts / secs / 1e6,
+            "seconds_by_size": {str(n): by_size[n] for n in sorted(by_size)}}
 
 
 def main(argv=None) -> int:

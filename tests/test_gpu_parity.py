@@ -326,3 +326,11 @@ def test_pass_timing_instrumentation(gpu_lib):
     assert (b.pass_times() == -1).all()
     a.close()
     b.close()
+
+
+def test_run_module(gpu_lib):
+    """The profiling driver `python -m pandora.run` on a small anisotropic case."""
+    from pandora import run
+    assert run.main(["--workload", "shear", "--nodes", "64", "32", "48", "--steps", "2"]) == 0
+    assert run.main(["--workload", "iso_forced_particles", "--nodes", "32", "32", "32", "--steps", "1",
+                     "--np", "256", "--precision", "fp32_mixed"]) == 0
