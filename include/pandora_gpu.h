@@ -48,7 +48,9 @@ extern "C" {
 #define PANDORA_RK3_TIMESTEP_FIXED   2   /* pg_parameters.f90:212 */
 #define PANDORA_RK3_TIMESTEP_CFL     3   /* pg_parameters.f90:213 */
 #define PANDORA_NS_BF_ROT            1   /* pg_parameters.f90:219 */
-#define PANDORA_DEALIASING_23        1   /* 2/3 rule (cube truncation)  */
+#define PANDORA_DEALIASING_23        1   /* 2/3 rule (cube truncation), pg_parameters.f90:224 */
+#define PANDORA_DEALIASING_SPHERICAL 2   /* 2/3 sphere |k_lab| <= KMAX, pg_parameters.f90:225 */
+#define PANDORA_DEALIASING_LES       3   /* |k_lab| <= LES_CUTOFF * KMAX, pg_parameters.f90:226 */
 #define PANDORA_F_INIT_NULL          0   /* pg_parameters.f90:150 */
 #define PANDORA_F_INIT_GAUSS         3
 #define PANDORA_F_INIT_KERR          4
@@ -109,7 +111,10 @@ typedef struct pandora_params {
     uint64_t seed_fluid, seed_force, seed_particles;
     /* arithmetic of the step: PANDORA_PREC_FP64 or PANDORA_PREC_FP32_MIXED */
     int32_t precision;
-    int32_t reserved[7];
+    int32_t reserved0;
+    /* nl_numerics LES_CUTOFF: cutoff of DEALIASING = 3 as a multiple of KMAX */
+    double  les_cutoff;
+    int32_t reserved[4];
 } pandora_params;
 
 typedef struct pandora_handle pandora_handle;

@@ -664,8 +664,40 @@ void oracle_get_b(const oracle* o, double* b13, double* bi13) {
     *bi13 = o->binv[0][2];
 }
 
-/* transforms + nonlinear term of the current state -> o->nl (normalised) */
+/* f_ArraysDealiasSpherical / f_ArraysLESCutoff (src/pf_arrays.f90:1865-1987):
+ * DEALIASING 2 zeroes every mode whose laboratory-frame wave vector
+ * k_lab(n) = sum_m bmat(m,n) k(m) is longer than KMAX = min(KI, KJ, KK)
+ * (src/pg_domain.f90:231), DEALIASING 3 those longer than LES_CUTOFF * KMAX. */
+static void dealias(oracle* o) {
+    const int mode = o->p.dealiasing;
+    if (mode != PANDORA_DEALIASING_SPHERICAL && mode != PANDORA_DEALIASING_LES) return;
+    int kmin = o->ki < o->kj ? o->ki : o->kj;
+    kmin = kmin < o->kk ? kmin : o->kk;
+    const double kmax = (double)kmin;
+    const double cutoff = mode == PANDORA_DEALIASING_SPHERICAL ? kmax : o->p.les_cutoff * kmax;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < o->nki; i++)
+        for (int j = 0; j < o->nkj; j++)
+            for (int k = 0; k < o->nkk; k++) {
+                const double mov[3] = {(double)i, wvn(j, o->kj), wvn(k, o->kk)};
+                double lab[3] = {0.0, 0.0, 0.0};
+                for (int m = 0; m < 3; m++)
+                    for (int n = 0; n < 3; n++)
+                        if (o->bexist[m][n]) lab[n] = lab[n] + o->bmat[m][n] * mov[m];
+                const double kmag = sqrt((lab[0] * lab[0]) + (lab[1] * lab[1]) + (lab[2] * lab[2]));
+                if (kmag > cutoff) {
+                    const long m = ((long)i * o->nkj + j) * o->nkk + k;
+                    for (int c = 0; c < 3; c++) { o->u[c][m].re = 0.0; o->u[c][m].im = 0.0; }
+                }
+            }
+}
+
+/* transforms + nonlinear term of the current state -> o->nl (normalised); with
+ * DEALIASING 2/3 the state is first truncated (f_RK3PrepareRealSpace,
+ * src/pf_rk3.f90:269-277; the second truncation after the nonlinear term,
+ * src/pf_rk3.f90:2101-2109, finds the state unchanged) */
 static void compute_nonlinear(oracle* o, int want_cfl) {
+    dealias(o);
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};   /* spectral omega held in nl */
     if (o->shear) vorticity_bf(o, om);
     else vorticity_iso(o, om);
@@ -1300,6 +1332,7 @@ void oracle_init_fluid(oracle* o) {
         }
     }
 #undef U
+    dealias(o);   /* src/pf_initialise.f90:75-83 */
 }
 
 /* tf_RK3InitTaylorGreenReverse (src/ptf_rk3.f90:1030-1105) */
@@ -1350,9 +1383,11 @@ static double tstep_dt(const oracle* o, double ucfl) {
 /* f_RK3Stage{1,2,3} (src/pf_rk3.f90:40-200); *dt in/out */
 int oracle_stage(oracle* o, int stage, int tstep, double* dt) {
     if (o->p.f_type != PANDORA_F_ISOTROPIC && o->p.f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
-    if (stage == 1 && o->shear && oracle_remesh_due(o, tstep)) {
+    if (stage == 1 && o->shear && oracle_remesh_due(o, tstep)) {   /* src/pf_rk3.f90:3990-4025 */
+        dealias(o);
         particles_remesh(o);
         remesh_wave_space(o);
+        dealias(o);
     }
     compute_nonlinear(o, stage == 1);
     if (stage == 1) *dt = tstep_dt(o, o->ucfl);

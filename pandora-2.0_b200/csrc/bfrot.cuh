@@ -74,6 +74,22 @@ __device__ __forceinline__ void vort_bf(const BFT<R>& f, const C* u, const R* k,
     }
 }
 
+// f_ArraysDealiasSpherical / f_ArraysLESCutoff (src/pf_arrays.f90:1865-1987): a mode
+// whose laboratory-frame wave vector k_lab(n) = sum_m bmat(m,n) k(m) is longer than
+// g.dealias_cut is dropped.  Unfused, correctly rounded products and sums in the
+// reference's order, so that the decision at the cutoff is the reference's.
+__device__ __forceinline__ bool dealias_drop(const Geo& g, const BF& f, double k1, double k2, double k3) {
+    const double kv[3] = {k1, k2, k3};
+    double kl[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int n = 0; n < 3; n++)
+            if (bex(m, n)) kl[n] = __dadd_rn(kl[n], __dmul_rn(f.bm[m][n], kv[m]));
+    const double km = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(kl[0], kl[0]), __dmul_rn(kl[1], kl[1])), __dmul_rn(kl[2], kl[2])));
+    return km > g.dealias_cut;
+}
+
 // f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711), pointwise in physical space.
 template <class R>
 __device__ __forceinline__ void nl_bf(const BFT<R>& f, const R* u, const R* om, R* nl) {

@@ -481,8 +481,19 @@ __global__ void __launch_bounds__(256) k_remesh(const __grid_constant__ MemberSe
     if (!remesh_due(g, ck->tstep)) return;
     extern __shared__ double2 rowbuf[];   // [3][NKK]
     const long long ij = blockIdx.x;
-    const int i = (int)(ij / g.nkj);
+    const int i = (int)(ij / g.nkj), jj = (int)(ij - (long long)i * g.nkj);
     const int KK = g.kk, NKK = g.nkk, nodes = 2 * KK + 1;
+    // DEALIASING 2/3: modes outside the cutoff are dropped in the frame before the
+    // remesh and again in the frame after it (src/pf_rk3.f90:3999-4025); the frame
+    // itself is reset by k_remesh_frame after this kernel
+    const bool dealias = g.dealias_cut > 0.0;
+    BF fold, fnew;
+    if (dealias) {
+        fold = make_bf(g, ck);
+        fnew = fold;
+        fnew.bm[0][2] = -g.bdiag[0] * (-(double)g.b110 * 0.5);
+    }
+    const double k1 = (double)i, k2 = wvn(jj, g.kj);
     for (int q = threadIdx.x; q < 3 * NKK; q += blockDim.x) rowbuf[q] = mk(0.0, 0.0);
     __syncthreads();
     for (int k = threadIdx.x; k < NKK; k += blockDim.x) {
@@ -490,20 +501,57 @@ __global__ void __launch_bounds__(256) k_remesh(const __grid_constant__ MemberSe
         int knew = actualk - i;
         if (knew >= -KK) {
             if (knew < 0) knew += nodes;
-            for (int c = 0; c < 3; c++) rowbuf[c * NKK + knew] = to_d(F.u[c][ij * NKK + k]);
+            const bool drop = dealias && dealias_drop(g, fold, k1, k2, (double)actualk);
+            for (int c = 0; c < 3; c++)
+                rowbuf[c * NKK + knew] = drop ? mk(0.0, 0.0) : to_d(F.u[c][ij * NKK + k]);
         }
     }
     __syncthreads();
     for (int k = threadIdx.x; k < NKK; k += blockDim.x) {
         const double2 a = rowbuf[k], b3 = rowbuf[2 * NKK + k];
+        if (dealias && dealias_drop(g, fnew, k1, k2, wvn(k, KK))) {
+            for (int c = 0; c < 3; c++) F.u[c][ij * NKK + k] = from_d<C>(mk(0.0, 0.0));
+            continue;
+        }
         F.u[0][ij * NKK + k] = from_d<C>(mk(a.x + b3.x, a.y + b3.y));
         F.u[1][ij * NKK + k] = from_d<C>(rowbuf[NKK + k]);
         F.u[2][ij * NKK + k] = from_d<C>(b3);
     }
-    if (ij == 0 && threadIdx.x == 0) {
-        const double half_b = (double)g.b110 * 0.5;
-        ck->b13 = -g.bdiag[0] * (-half_b);
-        ck->bi13 = (-half_b) / g.bdiag[2];
+}
+
+// The frame jump of the remesh (bmat/binv (1,3) to S t = -B110/2), after k_remesh:
+// every CTA of k_remesh reads the frame from before the remesh.
+template <class T, int CAP>
+__global__ void k_remesh_frame(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x];
+    if (!mm.active) return;
+    Clock* ck = mm.F.clock;
+    if constexpr (CAP > 1) {
+        if (ck->status & PD_ST_IDLE) return;
+    }
+    const Geo& g = mm.g;
+    if (!remesh_due(g, ck->tstep)) return;
+    const double half_b = (double)g.b110 * 0.5;
+    ck->b13 = -g.bdiag[0] * (-half_b);
+    ck->bi13 = (-half_b) / g.bdiag[2];
+}
+
+// DEALIASING 2/3 applied to the state in place (after the initial field,
+// src/pf_initialise.f90:75-83).
+template <class T, int CAP>
+__global__ void k_dealias(const __grid_constant__ MemberSet<T, CAP> ms) {
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+    using C = typename FieldsT<T>::C;
+    const BF bf = make_bf(g, F.clock);
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.S; m += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(m % g.nkk);
+        const long long ij = m / g.nkk;
+        const int j = (int)(ij % g.nkj), i = (int)(ij / g.nkj);
+        if (dealias_drop(g, bf, (double)i, wvn(j, g.kj), wvn(k, g.kk)))
+            for (int c = 0; c < 3; c++) F.u[c][m] = C{};
     }
 }
 
@@ -530,12 +578,34 @@ __global__ void k_remesh_particles(const __grid_constant__ MemberSet<T, CAP> ms)
 
 // np: particles per member (0: none)
 #define PD_CAP(S) std::decay_t<decltype(S)>::cap
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
 template <class T>
 cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np, cudaStream_t st) {
     return for_member_sets(M, B, [&](const auto& ms, int nb) {
         constexpr int CAP = PD_CAP(ms);
         if (np > 0) k_remesh_particles<T, CAP><<<dim3((unsigned)((np + 255) / 256), nb), 256, 0, st>>>(ms);
         k_remesh<T, CAP><<<dim3((unsigned)((long long)g.nki * g.nkj), nb), 256, sizeof(double2) * 3 * g.nkk, st>>>(ms);
+        k_remesh_frame<T, CAP><<<nb, 1, 0, st>>>(ms);
+    });
+}
+
+template <class T>
+cudaError_t launch_dealias(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
+    if (!(g.dealias_cut > 0.0)) return cudaSuccess;
+    long long nb = (g.S + 255) / 256;
+    if (nb > 4LL * sm_count()) nb = 4LL * sm_count();
+    return for_member_sets(M, B, [&](const auto& ms, int nm) {
+        k_dealias<T, PD_CAP(ms)><<<dim3((unsigned)nb, nm), 256, 0, st>>>(ms);
     });
 }
 
@@ -564,16 +634,6 @@ __global__ void k_check_finite(const __grid_constant__ MemberSet<T, CAP> ms) {
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-static int sm_count() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
 
 // Statistics of every member into its own F.shell (shell_words doubles); the
 // per-CTA partial sums live in the member's y-pencil buffer, free at stage 1 and
@@ -670,7 +730,8 @@ template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>
                                                  cudaStream_t);                                      \
     template cudaError_t launch_advance_time<T>(const Geo&, const Member<T>*, int, int, cudaStream_t); \
     template cudaError_t launch_check_finite<T>(const Geo&, const Member<T>*, int, cudaStream_t);    \
-    template cudaError_t launch_remesh<T>(const Geo&, const Member<T>*, int, long long, cudaStream_t);
+    template cudaError_t launch_remesh<T>(const Geo&, const Member<T>*, int, long long, cudaStream_t);  \
+    template cudaError_t launch_dealias<T>(const Geo&, const Member<T>*, int, cudaStream_t);
 PD_INST(double)
 PD_INST(float)
 #undef PD_INST

@@ -435,12 +435,18 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
     // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1)
-    const C* pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
+    C* const pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
     const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
     BFT<T> bf;
     if constexpr (SHEAR) {
         if (f >= 3) bf = bf_as<T>(make_bf(g, F.clock));
     }
+    // DEALIASING 2/3: f_RK3PrepareRealSpace first zeroes the modes outside the cutoff
+    // (src/pf_rk3.f90:269-277); each velocity CTA clears its component's dropped modes
+    // in u as it reads them, every CTA reads them as zero
+    const bool dealias = g.dealias_cut > 0.0;
+    BF bfd;
+    if (dealias) bfd = make_bf(g, F.clock);
     auto ld = [&](int z, int l) -> C {
         const int i = i0 + l;
         int k;
@@ -449,6 +455,10 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
         else return mk(T(0), T(0));
         if (i >= nki) return mk(T(0), T(0));
         const long long m = row0 + l * istride + k;
+        if (dealias && dealias_drop(g, bfd, (double)i, k2, wvn(k, KK))) {
+            if (f < 3) pa[m] = mk(T(0), T(0));
+            return mk(T(0), T(0));
+        }
         if (f < 3) return pa[m];
         if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot), in T
             const T kv[3] = {(T)i, k2t, (T)wvn(k, KK)};

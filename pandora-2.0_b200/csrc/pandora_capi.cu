@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <new>
 #include <vector>
 #include "pandora_internal.cuh"
@@ -111,6 +112,7 @@ extern "C" int pandora_params_default(pandora_params* p) {
     p->p_interp_order = 4; p->p_ts_release = 1000; p->p_rho = 1000.0; p->p_dia_vals = 0.01514314;
     p->seed_fluid = 1; p->seed_force = 2; p->seed_particles = 3;
     p->precision = PANDORA_PREC_FP64;
+    p->les_cutoff = 1.0;
     return PANDORA_OK;
 }
 
@@ -195,7 +197,8 @@ static int validate(const pandora_params* p) {
         if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
             return PANDORA_ERR_INVALID_ARG;
     }
-    if (p->dealiasing != 1) return PANDORA_ERR_UNSUPPORTED;
+    if (p->dealiasing < PANDORA_DEALIASING_23 || p->dealiasing > PANDORA_DEALIASING_LES) return PANDORA_ERR_UNSUPPORTED;
+    if (p->dealiasing == PANDORA_DEALIASING_LES && !(p->les_cutoff > 0.0)) return PANDORA_ERR_INVALID_ARG;
     if (!supported_length(p->nodes_x) || !supported_length(p->nodes_y) || !supported_length(p->nodes_z))
         return PANDORA_ERR_BAD_LAYOUT;
     if (p->rk3_cfl >= 1.0) return PANDORA_ERR_CFL;   // g_RK3Check, src/pg_rk3.f90:240-267
@@ -242,6 +245,11 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.b110 = p->b110; g.remesh_t = p->f_remesh_t;
     g.rk3_decide = (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) ? 1 : 0;
     g.bvol = (double)p->b110 * (double)p->b220 * (double)p->b330;
+    {   // KMAX = min(KI_MAX, KJ_MAX, KK_MAX) (src/pg_domain.f90:231)
+        const double kmax = (double)std::min(g.ki, std::min(g.kj, g.kk));
+        g.dealias_cut = p->dealiasing == PANDORA_DEALIASING_SPHERICAL ? kmax
+                      : (p->dealiasing == PANDORA_DEALIASING_LES ? p->les_cutoff * kmax : 0.0);
+    }
     h->nforce = (long long)(g.fnk + 1) * (2 * g.fnk + 1) * (2 * g.fnk + 1);
     h->particles_on = p->p_track_part != 0;
     h->mixed = p->precision == PANDORA_PREC_FP32_MIXED;
@@ -501,8 +509,12 @@ static int init_fluid_async(pandora_handle* h) {
         for (int c = 0; c < 3; c++) Fd.u[c] = h->F.zb + c * h->g.S;
         PD_CK(launch_init_fluid(h->g, Fd, ip, h->st));
         for (int c = 0; c < 3; c++) PD_CK(launch_convert(Fd.u[c], h->Ff.u[c], h->g.S, h->st));
+        const Member<float> m = self_of<float>(h);
+        PD_CK(launch_dealias(h->g, &m, 1, h->st));   // DEALIASING 2/3 after the initial field
     } else {
         PD_CK(launch_init_fluid(h->g, h->F, ip, h->st));
+        const Member<double> m = self_of<double>(h);
+        PD_CK(launch_dealias(h->g, &m, 1, h->st));
     }
     return PANDORA_OK;
 }
@@ -1104,7 +1116,7 @@ static bool same_class(const pandora_params* a, const pandora_params* b) {
     const long long na = a->p_track_part ? a->p_np_global : 0, nb = b->p_track_part ? b->p_np_global : 0;
     return a->nodes_x == b->nodes_x && a->nodes_y == b->nodes_y && a->nodes_z == b->nodes_z &&
            a->precision == b->precision && a->f_type == b->f_type && a->ns_deformed == b->ns_deformed &&
-           a->b110 == b->b110 && a->b220 == b->b220 && a->b330 == b->b330 && a->dealiasing == b->dealiasing &&
+           a->b110 == b->b110 && a->b220 == b->b220 && a->b330 == b->b330 && a->dealiasing == b->dealiasing && a->les_cutoff == b->les_cutoff &&
            na == nb && (na == 0 || a->p_interp_order == b->p_interp_order) &&
            (int)a->force_kf == (int)b->force_kf;
 }

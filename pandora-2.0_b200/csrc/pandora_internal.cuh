@@ -31,6 +31,9 @@ struct Geo {
     double shear_s;       // F_DEFORM_S = amat(1,3)
     int b110, remesh_t, rk3_decide;
     double bvol;          // B110 B220 B330
+    // DEALIASING 2 (2/3 sphere) or 3 (LES cutoff): modes with |k_lab| above this are
+    // zeroed (src/pf_arrays.f90:1865-1987); 0 for the 2/3 rule alone
+    double dealias_cut;
 };
 
 // Scalars of the running step kept in device memory so that a whole step can
@@ -227,6 +230,9 @@ cudaError_t launch_particles(const Geo& g, const Member<T>* M, int B, long long 
 template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 template <class T>
 cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np, cudaStream_t st);
+// DEALIASING 2/3 applied to the members' state in place (no-op for the 2/3 rule)
+template <class T>
+cudaError_t launch_dealias(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 // Per simulation (not batched): initial field (generated in FP64; the FP32-mixed
 // form converts it), particle initialisation and the per-step spatial sort.
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);

@@ -76,7 +76,8 @@ extern "C" int pandora_nonlinear_static(const pandora_params* p, const double* u
                                         const double* u3, double* n1, double* n2, double* n3,
                                         void* cuda_stream) {
     if (!p || !u1 || !u2 || !u3 || !n1 || !n2 || !n3) return PANDORA_ERR_INVALID_ARG;
-    if (p->f_type != PANDORA_F_ISOTROPIC || p->precision != PANDORA_PREC_FP64) return PANDORA_ERR_UNSUPPORTED;
+    if (p->f_type != PANDORA_F_ISOTROPIC || p->precision != PANDORA_PREC_FP64 || p->dealiasing != PANDORA_DEALIASING_23)
+        return PANDORA_ERR_UNSUPPORTED;
     const int nx = p->nodes_x, ny = p->nodes_y, nz = p->nodes_z;
     if (nx > kStaticMaxN || ny > kStaticMaxN || nz > kStaticMaxN) return PANDORA_ERR_BAD_LAYOUT;
     if (!pd::supported_length(nx) || !pd::supported_length(ny) || !pd::supported_length(nz))

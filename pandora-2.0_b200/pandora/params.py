@@ -59,7 +59,9 @@ class Params(ctypes.Structure):
         ("seed_fluid", ctypes.c_uint64), ("seed_force", ctypes.c_uint64),
         ("seed_particles", ctypes.c_uint64),
         ("precision", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("reserved0", ctypes.c_int32),
+        ("les_cutoff", ctypes.c_double),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
     def copy(self) -> "Params":
@@ -68,7 +70,7 @@ class Params(ctypes.Structure):
         return q
 
     def as_dict(self) -> dict:
-        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+        return {n: getattr(self, n) for n, _ in self._fields_ if not n.startswith("reserved")}
 
 
 def default_params(n: int = 32) -> Params:

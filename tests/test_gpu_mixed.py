@@ -115,3 +115,17 @@ def test_mixed_error_module_small(gpu_lib):
     r = mixed_error.compare(p, 6)
     assert r["rel_l2_u"] < 1e-5 and r["rel_l2_ek"] < 1e-4 and r["rel_eps"] < 1e-4, r
     assert r["ms_per_step_fp64"] > 0 and r["ms_per_step_fp32_mixed"] > 0
+
+
+def test_mixed_dealias_spherical(gpu_lib):
+    p = gpu_lib.workload_params("iso_decay", 32)
+    p.dealiasing = 2
+    o, s = _mixed(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 11):
+        t, _ = o.step(step, t)
+        s.step(step)
+    eu = rel_l2_fields(s.get_state(), o.get_state())
+    s.close()
+    assert eu < 1e-5, eu
+

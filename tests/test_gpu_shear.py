@@ -29,9 +29,13 @@ def test_deformed_init_matches_oracle(gpu_lib):
         assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-13
 
 
-def test_shear_steps_across_remesh(gpu_lib):
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_shear_steps_across_remesh(gpu_lib, mode):
+    """mode: DEALIASING 1 (2/3 cube), 2 (2/3 sphere in the laboratory frame, also
+    applied before and after the remesh, src/pf_rk3.f90:3999-4025) or 3 (LES cutoff 0.8)."""
     import oracle as O
     p = _shear(gpu_lib, 32, remesh_t=5)
+    p.dealiasing, p.les_cutoff = mode, 0.8
     o = O.Oracle(p)
     s = gpu_lib.Simulation(p)
     s.init_fluid()
