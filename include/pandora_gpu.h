@@ -207,6 +207,18 @@ int pandora_last_step_stats(pandora_handle* h, double* ek, int32_t kkmax, double
  * transforms (test hook of src/ptf_rk3.f90:1115-1191). */
 int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, double* n3);
 
+/* ---- statistics beyond E(k) ----
+ * Real-space statistics of the current state (f_FluidstatsRs2D, src/pf_fluidstats.f90:
+ * 827-958; the transforms of one stage, no state change): out[0..20] raw sums over the
+ * NX NY NZ points of u1u1 u2u2 u3u3 u1u2 u1u3 u2u3, u1^3 u2^3 u3^3, u1^4 u2^4 u3^4
+ * (laboratory-frame velocity), w1^2 w2^2 w3^2, w1^3.., w1^4..; out[21] max |u1|+|u2|+|u3|,
+ * out[22..24] max |w_i|.  n >= 25.  Normalisation as f_FluidstatsRsCollect
+ * (src/pf_fluidstats.f90:960-1100) is the caller's. */
+int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n);
+/* Particle statistics (p_StatsPrimary, src/pp_stats.f90:119-200): out[0..5] sums of
+ * up_i up_j, out[6] sum of (1/2)(pi/6 dp^3 P_RHO)|up|^2.  n >= 7. */
+int pandora_particle_stats(pandora_handle* h, double* out, int32_t n);
+
 /* Physical-space velocity of the last stage (x fastest, [z][y][x]), as
  * materialised for particle interpolation (arr_u*_3r, src/pf_rk3.f90:1108-1115). */
 int pandora_get_physical_velocity(pandora_handle* h, double* u1, double* u2, double* u3);

@@ -74,6 +74,7 @@ def lib():
         L.oracle_remesh_due.argtypes = [vp, i32]
         L.oracle_force_calls_per_stage.restype = i64
         L.oracle_force_calls_per_stage.argtypes = [vp]
+        L.oracle_realspace_sums.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -141,6 +142,12 @@ class Oracle:
 
     def nonlinear(self):
         return self._three(self.L.oracle_nonlinear, self.shape)
+
+    def realspace_sums(self):
+        """f_FluidstatsRs2D's raw sums and maxima of the current state (25 values)."""
+        out = np.zeros(25)
+        self.L.oracle_realspace_sums(self.h, _ptr(out))
+        return out
 
     def get_forcing(self):
         w = 2 * self.fnk + 1

@@ -709,6 +709,43 @@ static void compute_nonlinear(oracle* o, int want_cfl) {
     for (int c = 0; c < 3; c++) phys_to_spec(o, o->phys[3 + c], o->nl[c]);
 }
 
+/* f_FluidstatsRs2D (src/pf_fluidstats.f90:827-958) over the physical fields of the
+ * current state: out[0..20] raw sums of u1u1 u2u2 u3u3 u1u2 u1u3 u2u3, u^3, u^4
+ * (laboratory frame: u_lab = binv u), w^2, w^3, w^4; out[21] max |u1|+|u2|+|u3|,
+ * out[22..24] max |w_i|.  The state is truncated first as at a stage's start. */
+void oracle_realspace_sums(oracle* o, double* out) {
+    dealias(o);
+    cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};
+    if (o->shear) vorticity_bf(o, om);
+    else vorticity_iso(o, om);
+    for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
+    for (int c = 0; c < 3; c++) spec_to_phys(o, om[c], o->phys[3 + c]);
+    for (int a = 0; a < 25; a++) out[a] = 0.0;
+    for (long x = 0; x < o->R; x++) {
+        double u[3] = {o->phys[0][x], o->phys[1][x], o->phys[2][x]};
+        if (o->p.f_type != PANDORA_F_ISOTROPIC) {
+            double ul[3] = {0.0, 0.0, 0.0};
+            for (int m = 0; m < 3; m++)
+                for (int n = 0; n < 3; n++)
+                    if (o->bexist[m][n]) ul[m] += o->binv[m][n] * u[n];
+            u[0] = ul[0]; u[1] = ul[1]; u[2] = ul[2];
+        }
+        const double w[3] = {o->phys[3][x], o->phys[4][x], o->phys[5][x]};
+        out[0] += u[0] * u[0]; out[1] += u[1] * u[1]; out[2] += u[2] * u[2];
+        out[3] += u[0] * u[1]; out[4] += u[0] * u[2]; out[5] += u[1] * u[2];
+        for (int c = 0; c < 3; c++) {
+            out[6 + c] += u[c] * u[c] * u[c];
+            out[9 + c] += (u[c] * u[c]) * (u[c] * u[c]);
+            out[12 + c] += w[c] * w[c];
+            out[15 + c] += w[c] * w[c] * w[c];
+            out[18 + c] += (w[c] * w[c]) * (w[c] * w[c]);
+            if (fabs(w[c]) > out[22 + c]) out[22 + c] = fabs(w[c]);
+        }
+        const double us = fabs(u[0]) + fabs(u[1]) + fabs(u[2]);
+        if (us > out[21]) out[21] = us;
+    }
+}
+
 int oracle_nonlinear(oracle* o, double* a, double* b, double* c) {
     compute_nonlinear(o, 0);
     oracle_get_nl(o, a, b, c);

@@ -14,6 +14,7 @@
 // so that a wave of threads reads a compact set of velocity rows that stays in
 // L2 instead of gathering at random from a field larger than L2.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <type_traits>
 #include "pandora_internal.cuh"
 #include "bfrot.cuh"
@@ -385,6 +386,41 @@ cudaError_t launch_particle_sort(const Geo& g, const Particles& P, const PartSor
     e = cudaMemcpyAsync(P.xp[0], s.tmp.xp[0], sizeof(double) * 14 * (size_t)P.np, cudaMemcpyDeviceToDevice, st);
     if (nlaunch) *nlaunch += 5;
     return e;
+}
+
+// p_StatsPrimary (src/pp_stats.f90:119-200): the sums over particles of up_i up_j and of
+// the kinetic energy (1/2)(pi/6 dp^3 P_RHO)|up|^2; the caller divides by P_NP_GLOBAL.
+__global__ void __launch_bounds__(256) k_part_stats(Particles p, long long np, double rho_p, double* acc) {
+    double s[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double c = 3.14159265358979323846264338327950288 / 6.0;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+        const double u1 = p.up[0][n], u2 = p.up[1][n], u3 = p.up[2][n], d = p.dp[n];
+        s[0] += u1 * u1; s[1] += u2 * u2; s[2] += u3 * u3;
+        s[3] += u1 * u2; s[4] += u1 * u3; s[5] += u2 * u3;
+        s[6] += 0.5 * ((c * (d * d * d)) * rho_p) * ((u1 * u1) + (u2 * u2) + (u3 * u3));
+    }
+    __shared__ double red[8][7];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int a = 0; a < 7; a++) {
+        double x = s[a];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[w][a] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double x = 0.0;
+        for (int v = 0; v < (int)(blockDim.x >> 5); v++) x += red[v][threadIdx.x];
+        atomicAdd(acc + threadIdx.x, x);
+    }
+}
+
+cudaError_t launch_particle_stats(const Particles& p, long long np, double rho_p, double* acc, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(double) * 7, st);
+    if (e || np <= 0) return e;
+    unsigned nb = (unsigned)std::min<long long>((np + 255) / 256, 1024);
+    k_part_stats<<<nb, 256, 0, st>>>(p, np, rho_p, acc);
+    return cudaGetLastError();
 }
 
 template cudaError_t launch_particles<double>(const Geo&, const Member<double>*, int, long long, int, int,

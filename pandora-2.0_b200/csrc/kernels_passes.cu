@@ -107,11 +107,42 @@ __device__ __forceinline__ C nl_point(const BFT<T>& bf, bool shear, T u1, T u2, 
     return mk(u3 * w2 - u2 * w3, u1 * w3 - u3 * w1);
 }
 
-template <int NX, class T, int CAP>
+// Real-space statistics of f_FluidstatsRs2D (src/pf_fluidstats.f90:827-958) at one
+// point: velocity moments in the laboratory frame (u_lab = binv u for shear), vorticity
+// moments, maxima.  acc: [0..5] u1u1 u2u2 u3u3 u1u2 u1u3 u2u3, [6..8] u^3, [9..11] u^4,
+// [12..14] w^2, [15..17] w^3, [18..20] w^4; mx: [0] max |u1|+|u2|+|u3|, [1..3] max |w|.
+constexpr int kRsSums = 21, kRsMax = 4, kRsSlots = 32, kRsWords = 32;
+__device__ __forceinline__ void rs_point(double* acc, double* mx, bool shear, const BF& f, double u1, double u2,
+                                         double u3, double w1, double w2, double w3) {
+    if (shear) {
+        const double um[3] = {u1, u2, u3};
+        double ul[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int n = 0; n < 3; n++)
+                if (bex(m, n)) ul[m] += f.bi[m][n] * um[n];
+        u1 = ul[0]; u2 = ul[1]; u3 = ul[2];
+    }
+    acc[0] += u1 * u1; acc[1] += u2 * u2; acc[2] += u3 * u3;
+    acc[3] += u1 * u2; acc[4] += u1 * u3; acc[5] += u2 * u3;
+    acc[6] += u1 * u1 * u1; acc[7] += u2 * u2 * u2; acc[8] += u3 * u3 * u3;
+    acc[9] += (u1 * u1) * (u1 * u1); acc[10] += (u2 * u2) * (u2 * u2); acc[11] += (u3 * u3) * (u3 * u3);
+    acc[12] += w1 * w1; acc[13] += w2 * w2; acc[14] += w3 * w3;
+    acc[15] += w1 * w1 * w1; acc[16] += w2 * w2 * w2; acc[17] += w3 * w3 * w3;
+    acc[18] += (w1 * w1) * (w1 * w1); acc[19] += (w2 * w2) * (w2 * w2); acc[20] += (w3 * w3) * (w3 * w3);
+    mx[0] = fmax(mx[0], fabs(u1) + fabs(u2) + fabs(u3));
+    mx[1] = fmax(mx[1], fabs(w1)); mx[2] = fmax(mx[2], fabs(w2)); mx[3] = fmax(mx[3], fabs(w3));
+}
+
+// RS: the real-space statistics pass (the same transforms, plus the moments of every
+// point, reduced per warp into one of kRsSlots copies of the sums in `rs`).
+template <int NX, class T, int CAP, bool RS = false>
 __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                         int want_phys,
                                                                                         int want_cfl,
-                                                                                        long long pf_lines) {
+                                                                                        long long pf_lines,
+                                                                                        double* rs) {
     using C = typename FieldsT<T>::C;
     using XP = pdfft::FusedPlan<NX>;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
@@ -135,6 +166,15 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     C* b = F.yb + q * g.nkip;
     BFT<T> bf;
     if (g.shear) bf = bf_as<T>(make_bf(g, F.clock));
+    double racc[RS ? kRsSums : 1], rmax[RS ? kRsMax : 1];
+    BF brs;
+    if constexpr (RS) {
+#pragma unroll
+        for (int a = 0; a < kRsSums; a++) racc[a] = 0.0;
+#pragma unroll
+        for (int a = 0; a < kRsMax; a++) rmax[a] = 0.0;
+        brs = make_bf(g, F.clock);
+    }
     // the band of each array; the first backward pass reads nothing outside it.
     // From 384 points on (registers to spare at one or two CTAs per SM) the loads
     // of up to IB rounds of m are issued before any of their stores, so a line waits
@@ -197,6 +237,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
                     F.phys[2 * g.R + q * NX + n] = u3;
                 }
                 if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
+                if constexpr (RS) rs_point(racc, rmax, g.shear, brs, u1, u2, u3, w1, w2, w3);
                 v[r] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3[r]);
             }
         }
@@ -223,6 +264,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
                 F.phys[2 * g.R + q * NX + n] = u3;
             }
             if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
+            if constexpr (RS) rs_point(racc, rmax, g.shear, brs, u1, u2, u3, w1, w2, w3);
             T n3;
             e[0] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3);
             e[XAS] = mk(n3, T(0));
@@ -232,6 +274,22 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
         if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
+    }
+    if constexpr (RS) {   // the warp's sums into slot q % kRsSlots
+        double* slot = rs + (size_t)(q % kRsSlots) * kRsWords;
+#pragma unroll
+        for (int a = 0; a < kRsSums; a++) {
+            double x = racc[a];
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) atomicAdd(slot + a, x);
+        }
+#pragma unroll
+        for (int a = 0; a < kRsMax; a++) {
+            double x = rmax[a];
+            for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+            if (lane == 0)
+                atomicMax(reinterpret_cast<unsigned long long*>(slot + kRsSums + a), (unsigned long long)__double_as_longlong(x));
+        }
     }
     // The six input rows of line q + pf_lines (a wave of resident CTAs later, so
     // the CTA that takes it starts about when this one ends) are prefetched into
@@ -718,9 +776,31 @@ cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys,
                 const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                     \
                 /* L2 prefetch distance: one wave of resident CTAs (single simulations) */      \
                 const long long pf = CAP == 1 ? Cfg<N>::NWX * resident_ctas(k_xpass<N, T, CAP>, 32 * Cfg<N>::NWX, smem_kx<N, T>()) : 0; \
-                k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl, pf); \
+                k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl, pf, nullptr); \
             }                                                                                     \
         });
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// The x pass of the real-space statistics (single simulation): the moments of every
+// point into `rs` (kRsSlots x kRsWords doubles, zeroed by the caller).
+template <class T>
+cudaError_t launch_xpass_stats(const Geo& g, const Member<T>* M, double* rs, cudaStream_t st) {
+    const long long lines = (long long)g.ny * g.nz;
+    switch (g.nx) {
+#define PD_L(N)                                                                                   \
+    case N: {                                                                                     \
+        cudaError_t e = set_smem(k_xpass<N, T, 1, true>, smem_kx<N, T>());                        \
+        if (e) return e;                                                                          \
+        MemberSet<T, 1> ms;                                                                       \
+        ms.m[0] = M[0];                                                                           \
+        const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                             \
+        k_xpass<N, T, 1, true><<<dim3((unsigned)nl, 1), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, 0, 0, 0, rs); \
+        return cudaGetLastError();                                                                \
+    }
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
     default: return cudaErrorInvalidValue;
@@ -795,6 +875,7 @@ cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStre
     template cudaError_t launch_zpass_inv<T>(const Geo&, const Member<T>*, int, int, cudaStream_t);      \
     template cudaError_t launch_ypass_inv<T>(const Geo&, const Member<T>*, int, cudaStream_t);           \
     template cudaError_t launch_xpass<T>(const Geo&, const Member<T>*, int, int, int, cudaStream_t);     \
+    template cudaError_t launch_xpass_stats<T>(const Geo&, const Member<T>*, double*, cudaStream_t);    \
     template cudaError_t launch_ypass_fwd<T>(const Geo&, const Member<T>*, int, cudaStream_t);           \
     template cudaError_t launch_zpass_fwd_update<T>(const Geo&, const Member<T>*, int, int, int, cudaStream_t);
 PD_INST(double)

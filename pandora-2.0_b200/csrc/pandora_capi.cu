@@ -49,6 +49,7 @@ struct pandora_handle {
     double* pbuf2 = nullptr;          // sort destination, same layout
     PartSort sort{};
     void* nlbuf = nullptr;            // scratch for pandora_nonlinear
+    double* rsbuf = nullptr;          // real-space / particle statistics sums (32 x 32)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_graph = true;
@@ -154,7 +155,7 @@ static void release(pandora_handle* h) {
     if (h->graph) cudaGraphDestroy(h->graph);
     cudaFree(h->fbuf); cudaFree(h->F.zb); cudaFree(h->F.yb); cudaFree(h->F.phys);
     cudaFree(h->F.forcing); cudaFree(h->tw); cudaFree(h->clock); cudaFree(h->shell_step);
-    cudaFree(h->shell_now); cudaFree(h->pbuf); cudaFree(h->pbuf2); cudaFree(h->nlbuf);
+    cudaFree(h->shell_now); cudaFree(h->pbuf); cudaFree(h->pbuf2); cudaFree(h->nlbuf); cudaFree(h->rsbuf);
     cudaFree(h->sort.key); cudaFree(h->sort.count); cudaFree(h->sort.block_sums);
     if (h->clock_host) cudaFreeHost(h->clock_host);
     if (h->shell_host) cudaFreeHost(h->shell_host);
@@ -884,6 +885,57 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
     PD_CK(launch_ypass_fwd(h->g, Mv, 1, h->st));
     PD_CK(launch_zpass_fwd_update(h->g, Mv, 1, 1, 1, h->st));
     return copy3(h, Fn.rk, n1, n2, n3, (size_t)h->g.S, false);
+}
+
+// f_FluidstatsRs2D's sums over the physical field of the current state
+// (src/pf_fluidstats.f90:827-958): out[0..20] the raw sums of u1u1 u2u2 u3u3 u1u2 u1u3
+// u2u3, u^3 (3), u^4 (3) (laboratory frame), w^2 (3), w^3 (3), w^4 (3); out[21] max
+// |u1|+|u2|+|u3|; out[22..24] max |w_i|.  The caller normalises as
+// f_FluidstatsRsCollect does (src/pf_fluidstats.f90:960-1100).
+extern "C" int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n) {
+    if (!h || !out || n < 25) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    const size_t words = 32 * 32;
+    if (!h->rsbuf) {
+        if (cudaMalloc((void**)&h->rsbuf, sizeof(double) * words) != cudaSuccess) { cudaGetLastError(); return PANDORA_ERR_OOM; }
+    }
+    PD_CK(cudaMemsetAsync(h->rsbuf, 0, sizeof(double) * words, h->st));
+    if (h->mixed) {
+        const Member<float> mv = self_of<float>(h);
+        PD_CK(launch_zpass_inv(h->g, &mv, 1, 0, h->st));
+        PD_CK(launch_ypass_inv(h->g, &mv, 1, h->st));
+        PD_CK(launch_xpass_stats(h->g, &mv, h->rsbuf, h->st));
+    } else {
+        const Member<double> mv = self_of<double>(h);
+        PD_CK(launch_zpass_inv(h->g, &mv, 1, 0, h->st));
+        PD_CK(launch_ypass_inv(h->g, &mv, 1, h->st));
+        PD_CK(launch_xpass_stats(h->g, &mv, h->rsbuf, h->st));
+    }
+    std::vector<double> hb(words);
+    PD_CK(cudaMemcpyAsync(hb.data(), h->rsbuf, sizeof(double) * words, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    for (int a = 0; a < 25; a++) out[a] = 0.0;
+    for (int slot = 0; slot < 32; slot++) {
+        for (int a = 0; a < 21; a++) out[a] += hb[(size_t)slot * 32 + a];
+        for (int a = 21; a < 25; a++) out[a] = std::max(out[a], hb[(size_t)slot * 32 + a]);
+    }
+    return PANDORA_OK;
+}
+
+// p_StatsPrimary's sums over the particles (src/pp_stats.f90:119-200): out[0..5] the
+// sums of up_i up_j (u1u1 u2u2 u3u3 u1u2 u1u3 u2u3), out[6] the sum of the particles'
+// kinetic energy (1/2)(pi/6 dp^3 P_RHO)|up|^2; divided by P_NP_GLOBAL by the caller.
+extern "C" int pandora_particle_stats(pandora_handle* h, double* out, int32_t n) {
+    if (!h || !out || n < 7) return PANDORA_ERR_INVALID_ARG;
+    if (!h->particles_on || h->P.np <= 0) return PANDORA_ERR_UNSUPPORTED;
+    cudaSetDevice(h->dev);
+    if (!h->rsbuf) {
+        if (cudaMalloc((void**)&h->rsbuf, sizeof(double) * 32 * 32) != cudaSuccess) { cudaGetLastError(); return PANDORA_ERR_OOM; }
+    }
+    PD_CK(launch_particle_stats(h->P, h->P.np, h->p.p_rho, h->rsbuf, h->st));
+    PD_CK(cudaMemcpyAsync(out, h->rsbuf, sizeof(double) * 7, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    return PANDORA_OK;
 }
 
 extern "C" int pandora_get_physical_velocity(pandora_handle* h, double* u1, double* u2, double* u3) {

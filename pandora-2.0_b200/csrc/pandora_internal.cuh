@@ -230,6 +230,12 @@ cudaError_t launch_particles(const Geo& g, const Member<T>* M, int B, long long 
 template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 template <class T>
 cudaError_t launch_remesh(const Geo& g, const Member<T>* M, int B, long long np, cudaStream_t st);
+// The x pass with the real-space statistics of every point (single simulation):
+// kRsSlots (32) copies of 21 moment sums and 4 maxima (as ordered bits), 32 doubles each.
+template <class T>
+cudaError_t launch_xpass_stats(const Geo& g, const Member<T>* M, double* rs, cudaStream_t st);
+// Particle moments: sum up_i up_j (6) and the kinetic energy sum (1) into acc[7].
+cudaError_t launch_particle_stats(const Particles& p, long long np, double rho_p, double* acc, cudaStream_t st);
 // DEALIASING 2/3 applied to the members' state in place (no-op for the 2/3 rule)
 template <class T>
 cudaError_t launch_dealias(const Geo& g, const Member<T>* M, int B, cudaStream_t st);

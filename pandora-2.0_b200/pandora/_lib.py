@@ -68,6 +68,8 @@ SIGNATURES = {
     "pandora_stats": [_vp, _dp, _i32, _dp, _dp, _dp],
     "pandora_last_step_stats": [_vp, _dp, _i32, _dp, _dp, _dp],
     "pandora_nonlinear": [_vp, _dp, _dp, _dp],
+    "pandora_realspace_stats": [_vp, _dp, _i32],
+    "pandora_particle_stats": [_vp, _dp, _i32],
     "pandora_get_physical_velocity": [_vp, _dp, _dp, _dp],
     "pandora_check_status": [_vp],
     "pandora_launches_per_step": [_vp, ctypes.POINTER(_i32)],

@@ -35,6 +35,30 @@ def _as_f64(a, shape=None) -> np.ndarray:
     return a
 
 
+def realspace_normalise(raw, p) -> dict:
+    """f_FluidstatsRsCollect's normalisation (src/pf_fluidstats.f90:960-1100) of the raw
+    sums [u1u1 u2u2 u3u3 u1u2 u1u3 u2u3, u^3 (3), u^4 (3), w^2 (3), w^3 (3), w^4 (3),
+    umax, wmax (3)]."""
+    npts = float(p.nodes_x) * float(p.nodes_y) * float(p.nodes_z)
+    r = {}
+    for a, k in enumerate(("u1u1", "u2u2", "u3u3", "u1u2", "u1u3", "u2u3")):
+        r[k] = raw[a] / npts
+    for c in range(3):
+        uu = r[("u1u1", "u2u2", "u3u3")[c]]
+        r[f"skew{c + 1}"] = raw[6 + c] / npts / uu ** 1.5
+        r[f"flat{c + 1}"] = raw[9 + c] / npts / uu ** 2
+    rms = [raw[12], raw[13] / npts, raw[14] / npts]   # rmsvort1 unnormalised, as the reference
+    rms = [x ** 0.5 for x in rms]
+    for c in range(3):
+        r[f"rmsvort{c + 1}"] = rms[c]
+        r[f"skewvort{c + 1}"] = raw[15 + c] / npts / rms[c] ** 3
+        r[f"flatvort{c + 1}"] = raw[18 + c] / npts / rms[c] ** 4
+    r["ucfl"] = raw[21]
+    for c in range(3):
+        r[f"omegamax{c + 1}"] = raw[22 + c]
+    return r
+
+
 class Simulation:
     """One resident simulation on the current CUDA device."""
 
@@ -132,6 +156,31 @@ class Simulation:
                    "pandora_get_particles")
         return xp, up, ur, pr, dp
 
+    # ---- restart files (PETSc binary, g_RestartPetscFluid / g_RestartPetscParticle) ----
+    def write_restart(self, path: str, particle_path: str | None = None) -> None:
+        from . import restart
+        restart.write_fluid(path, self.get_state())
+        if particle_path is not None:
+            xp, up, _, _, dp = self.get_particles()
+            restart.write_particles(particle_path, xp.T, up.T, dp)
+
+    def read_restart(self, path: str, particle_path: str | None = None, scale: int = 1) -> None:
+        """State (and particles) from restart files; `scale` = F_RESTART_SCALE: the
+        file holds the field of a grid `scale` times coarser in every direction."""
+        from . import restart
+        if scale == 1:
+            u = restart.read_fluid(path, self.shape)
+        else:
+            p = self.p
+            ki, kj, kk = (p.nodes_x // scale) // 3, (p.nodes_y // scale) // 3, (p.nodes_z // scale) // 3
+            u = restart.scale_fluid(restart.read_fluid(path, (ki + 1, 2 * kj + 1, 2 * kk + 1)), self.shape)
+        self.set_state(u)
+        if particle_path is not None:
+            d = restart.read_particles(particle_path)
+            xp = np.stack([d["xp1"], d["xp2"], d["xp3"]], axis=1)
+            up = np.stack([d["up1"], d["up2"], d["up3"]], axis=1)
+            self.set_particles(xp, up=up, dp=d["dp"])
+
     # ---- stepping ----
     def step(self, tstep: int | None = None) -> float:
         """g_RK3Calc: one RK3 step; returns dt."""
@@ -164,6 +213,30 @@ class Simulation:
         _lib.check(fn(self.h, _dp(ek), self.kkmax, ctypes.byref(tke), ctypes.byref(eps), ctypes.byref(ucfl)),
                    "pandora_stats")
         return ek, tke.value, eps.value, ucfl.value
+
+    def realspace_sums(self) -> np.ndarray:
+        """Raw sums and maxima of `pandora_realspace_stats` (25 values)."""
+        out = np.zeros(25)
+        _lib.check(self.L.pandora_realspace_stats(self.h, _dp(out), 25), "pandora_realspace_stats")
+        return out
+
+    def realspace_stats(self) -> dict:
+        """f_FluidstatsRs2D + f_FluidstatsRsCollect (src/pf_fluidstats.f90:827-1100) of the
+        current state, normalised as the reference does (its rmsvort1 is not divided
+        by the number of points, src/pf_fluidstats.f90:1057; that is kept)."""
+        return realspace_normalise(self.realspace_sums(), self.p)
+
+    def particle_stats(self) -> dict:
+        """p_StatsPrimary (src/pp_stats.f90:119-200): particle velocity moments / NP and
+        the mean particle kinetic energy."""
+        out = np.zeros(7)
+        _lib.check(self.L.pandora_particle_stats(self.h, _dp(out), 7), "pandora_particle_stats")
+        n = float(self.p.p_np_global)
+        names = ("u1u1", "u2u2", "u3u3", "u1u2", "u1u3", "u2u3")
+        d = {k: out[a] / n for a, k in enumerate(names)}
+        d["tke"] = 0.5 * (d["u1u1"] + d["u2u2"] + d["u3u3"])
+        d["pken"] = out[6] / n
+        return d
 
     def nonlinear(self):
         return self._get3(self.L.pandora_nonlinear, self.shape, "pandora_nonlinear")

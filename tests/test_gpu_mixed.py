@@ -129,3 +129,11 @@ def test_mixed_dealias_spherical(gpu_lib):
     s.close()
     assert eu < 1e-5, eu
 
+
+def test_mixed_realspace_stats(gpu_lib):
+    p = gpu_lib.workload_params("iso_decay", 32)
+    o, s = _mixed(gpu_lib, p)
+    g, r = s.realspace_sums(), o.realspace_sums()
+    s.close()
+    np.testing.assert_allclose(g, r, rtol=1e-5)
+

@@ -358,3 +358,38 @@ def test_dealias_parity(gpu_lib, mode, cut):
         assert rel_l2(ek_g, ek_o) < 1e-8 and abs(eps_g - eps_o) < 1e-8 * abs(eps_o)
         assert rel_l2_fields(s.nonlinear(), o.nonlinear()) < 1e-12
 
+
+@pytest.mark.parametrize("workload", ["iso_decay", "shear"])
+def test_realspace_stats_parity(gpu_lib, workload):
+    """Real-space moments and maxima (f_FluidstatsRs2D) of the same state on both sides."""
+    import oracle as O
+    p = gpu_lib.workload_params(workload, 32)
+    p.p_track_part = 0
+    o, s = _pair(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 4):
+        t, _ = o.step(step, t)
+        s.step(step)
+    g = s.realspace_sums()
+    r = o.realspace_sums()
+    s.close()
+    np.testing.assert_allclose(g[:21], r[:21], rtol=1e-11, atol=1e-12 * np.abs(r[:21]).max())
+    np.testing.assert_allclose(g[21:], r[21:], rtol=1e-12)
+
+
+def test_particle_stats(gpu_lib):
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 1000
+    p.p_dia_vals, p.p_rho = 0.01, 1000.0   # inertial: dp > 0, so the kinetic-energy sum is not zero
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        s.init_particles()
+        s.advance(3)
+        d = s.particle_stats()
+        _, up, _, _, dp = s.get_particles()
+    n = 1000.0
+    assert d["u1u1"] == pytest.approx((up[:, 0] ** 2).sum() / n, rel=1e-12)
+    assert d["u2u3"] == pytest.approx((up[:, 1] * up[:, 2]).sum() / n, rel=1e-12, abs=1e-15)
+    pken = (0.5 * (np.pi / 6.0) * dp ** 3 * 1000.0 * (up ** 2).sum(axis=1)).sum() / n
+    assert pken > 0.0 and d["pken"] == pytest.approx(pken, rel=1e-12)
+

@@ -270,3 +270,19 @@ def test_dealias_default_is_the_two_thirds_cube():
     out = np.sqrt(k1 ** 2 + k2 ** 2 + k3 ** 2) > 32 // 3
     assert max(np.abs(c[out]).max() for c in o.get_state()) > 0.0
 
+
+@pytest.mark.parametrize("workload", ["iso_decay", "shear"])
+def test_realspace_sums_parseval(workload):
+    """f_FluidstatsRs2D's velocity second moments (laboratory frame for shear) carry the
+    spectral kinetic energy of f_FluidstatsFs (Parseval)."""
+    from pandora.params import workload_params
+    from pandora.rk3 import realspace_normalise
+    p = workload_params(workload, 32)
+    p.p_track_part = 0
+    o = _o(p)
+    o.init_fluid()
+    r = realspace_normalise(o.realspace_sums(), p)
+    _, tke, _ = o.stats()
+    assert 0.5 * (r["u1u1"] + r["u2u2"] + r["u3u3"]) == pytest.approx(tke, rel=1e-12)
+    assert 2.0 < r["flat1"] < 4.5 and abs(r["skew2"]) < 1.0
+
