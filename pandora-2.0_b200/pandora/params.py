@@ -82,7 +82,7 @@ def default_params(n: int = 32) -> Params:
     p.f_type = F_ISOTROPIC
     p.f_deform_s, p.f_remesh_t = 28.3, 32
     p.rk3_timestep, p.rk3_cfl, p.rk3_dt = RK3_TIMESTEP_DECIDE, 0.75, 0.01
-    p.ns_deformed, p.dealiasing = NS_BF_ROT, 1
+    p.ns_deformed, p.dealiasing, p.les_cutoff = NS_BF_ROT, 1, 1.0
     p.tsteps = 10
     p.f_init_type, p.f_init_u0, p.f_init_kp, p.f_init_kv = F_INIT_KERR, 0.1, 11.0, 20.0
     p.f_init_kstart, p.f_init_kend, p.f_init_epsilon = 5.0, 10.0, 0.0
