@@ -152,7 +152,8 @@ typedef struct oracle {
     double dx, dy, dz, lx, ly, lz;
     double bmat[3][3], binv[3][3], amat[3][3];
     int bexist[3][3], aexist[3][3];
-    int shear;            /* F_TYPE == F_SHEAR_DNS, BF-rot formulation */
+    int shear;            /* F_TYPE == F_SHEAR_DNS */
+    int rrot;             /* ... in the R-rot form (NS_DEFORMED = NS_R_ROT), else BF-rot */
     /* work */
     double* phys[6];      /* physical fields [z][y][x] */
     cx *wa, *wb;          /* pencil work arrays */
@@ -203,6 +204,7 @@ oracle* oracle_create(const pandora_params* p) {
         o->bexist[0][2] = 1; o->amat[0][2] = p->f_deform_s; o->aexist[0][2] = 1;
     }
     o->shear = (p->f_type == PANDORA_F_SHEAR_DNS);
+    o->rrot = o->shear && p->ns_deformed == PANDORA_NS_R_ROT;
     o->bmat[0][0] = 1.0 / o->binv[0][0]; o->bmat[1][1] = 1.0 / o->binv[1][1];
     o->bmat[2][2] = 1.0 / o->binv[2][2];
     for (int f = 0; f < 6; f++) o->phys[f] = dalloc(o->R);
@@ -459,6 +461,42 @@ static void vorticity_bf(oracle* o, cx* om[3]) {
     }
 }
 
+/* f_RK3DerivativeRRot (src/pf_rk3.f90:3749-3780): d/dx_j = i sum_m bmat(m,j) k_m, over
+ * every m (the reference's bvalexist test there guards nothing). */
+static cx deriv_rrot(const oracle* o, cx u, const double* k, int j) {
+    cx d = {0.0, 0.0};
+    for (int m = 0; m < 3; m++) {
+        d.im = d.im + (o->bmat[m][j] * k[m] * u.re);
+        d.re = d.re - (o->bmat[m][j] * k[m] * u.im);
+    }
+    return d;
+}
+
+/* R-rot vorticity (src/pf_rk3.f90:416-421, 470-475, 585-590): w = D x u with the
+ * sheared derivatives, assembled per velocity component in the reference's order. */
+static void vorticity_rrot(oracle* o, cx* om[3]) {
+#pragma omp parallel for schedule(static)
+    for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+        int i = (int)(ij / o->nkj), j = (int)(ij % o->nkj);
+        for (int k = 0; k < o->nkk; k++) {
+            long m = ij * o->nkk + k;
+            double kv[3] = {wvn(i, o->ki), wvn(j, o->kj), wvn(k, o->kk)};
+            cx w[3];
+            cx dudy = deriv_rrot(o, o->u[0][m], kv, 1), dudz = deriv_rrot(o, o->u[0][m], kv, 2);
+            w[0].re = 0.0; w[0].im = 0.0;
+            w[1] = dudz;
+            w[2].re = -dudy.re; w[2].im = -dudy.im;
+            cx dvdx = deriv_rrot(o, o->u[1][m], kv, 0), dvdz = deriv_rrot(o, o->u[1][m], kv, 2);
+            w[0].re = w[0].re - dvdz.re; w[0].im = w[0].im - dvdz.im;
+            w[2].re = w[2].re + dvdx.re; w[2].im = w[2].im + dvdx.im;
+            cx dwdx = deriv_rrot(o, o->u[2][m], kv, 0), dwdy = deriv_rrot(o, o->u[2][m], kv, 1);
+            w[0].re = w[0].re + dwdy.re; w[0].im = w[0].im + dwdy.im;
+            w[1].re = w[1].re - dwdx.re; w[1].im = w[1].im - dwdx.im;
+            om[0][m] = w[0]; om[1][m] = w[1]; om[2][m] = w[2];
+        }
+    }
+}
+
 /* f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711) */
 static void nonlinear_bf(oracle* o) {
     const double(*bi)[3] = o->binv;
@@ -583,6 +621,104 @@ static void form_f_bf(oracle* o, int stage, double dt) {
     }
 }
 
+/* f_RK3FormFRRot for F_SHEAR_DNS (src/pf_rk3.f90:2680-2856): f_RK3RRotPressure
+ * (2986-3070 pattern, the R-rot routine of 3078-3156), f_RK3RRotSource (3218-3249),
+ * f_RK3RRotViscous, then f_RK3RungeKutta and f_RK3ContinuityFixRRot (3620-3693).
+ * The nonlinear term enters untransformed (the isotropic product of the R-rot
+ * vorticity). */
+static void form_f_rrot(oracle* o, int stage, double dt) {
+    double beta, gamma;
+    void rk_coeffs(int, double*, double*);
+    rk_coeffs(stage, &beta, &gamma);
+    const double nu = o->p.f_nu;
+    const double(*bm)[3] = o->bmat;
+    const double(*bi)[3] = o->binv;
+    const double(*am)[3] = o->amat;
+    const int(*ex)[3] = o->bexist;
+    const int(*ax)[3] = o->aexist;
+#pragma omp parallel for schedule(static)
+    for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+        int i = (int)(ij / o->nkj), j = (int)(ij % o->nkj);
+        for (int kq = 0; kq < o->nkk; kq++) {
+            long m0 = ij * o->nkk + kq;
+            double k[3] = {wvn(i, o->ki), wvn(j, o->kj), wvn(kq, o->kk)};
+            double kmag2 = (k[0] * k[0]) + (k[1] * k[1]) + (k[2] * k[2]);
+            if (!(kmag2 > 0.0)) continue;
+            cx u[3] = {o->u[0][m0], o->u[1][m0], o->u[2][m0]};
+            cx nl[3] = {o->nl[0][m0], o->nl[1][m0], o->nl[2][m0]};
+            /* pressure */
+            double p1[3] = {0, 0, 0}, p4 = 0.0;
+            cx p2 = {0, 0}, p3 = {0, 0};
+            for (int m = 0; m < 3; m++)
+                for (int r = 0; r < 3; r++) {
+                    if (!ex[m][r]) continue;
+                    p2.re = p2.re + (k[m] * bm[m][r] * nl[r].re);
+                    p2.im = p2.im + (k[m] * bm[m][r] * nl[r].im);
+                    for (int q = 0; q < 3; q++)
+                        if (ax[r][q]) {
+                            p3.re = p3.re + (k[m] * bm[m][r] * am[r][q] * u[q].re);
+                            p3.im = p3.im + (k[m] * bm[m][r] * am[r][q] * u[q].im);
+                        }
+                    for (int q = 0; q < 3; q++)
+                        if (ex[q][r]) p4 = p4 + (k[m] * bm[m][r] * k[q] * bm[q][r]);
+                }
+            for (int a = 0; a < 3; a++)
+                for (int pp = 0; pp < 3; pp++)
+                    if (ex[pp][a]) p1[a] = p1[a] + k[pp] * bm[pp][a];
+            cx press[3];
+            for (int a = 0; a < 3; a++) {
+                if (p4 > 0.0) { press[a].re = (p1[a] / p4) * (p2.re + p3.re); press[a].im = (p1[a] / p4) * (p2.im + p3.im); }
+                else { press[a].re = 0.0; press[a].im = 0.0; }
+            }
+            /* homogeneous source A u */
+            cx hom[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int a = 0; a < 3; a++)
+                for (int q = 0; q < 3; q++)
+                    if (ax[a][q]) { hom[a].re = hom[a].re + (am[a][q] * u[q].re); hom[a].im = hom[a].im + (am[a][q] * u[q].im); }
+            /* viscous */
+            cx visc[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int l = 0; l < 3; l++)
+                for (int jj = 0; jj < 3; jj++) {
+                    if (!ex[l][jj]) continue;
+                    for (int n = 0; n < 3; n++) {
+                        if (!ex[n][jj]) continue;
+                        for (int a = 0; a < 3; a++) {
+                            visc[a].re = visc[a].re - nu * bm[l][jj] * bm[n][jj] * k[l] * k[n] * u[a].re;
+                            visc[a].im = visc[a].im - nu * bm[l][jj] * bm[n][jj] * k[l] * k[n] * u[a].im;
+                        }
+                    }
+                }
+            cx tot[3];
+            for (int a = 0; a < 3; a++) {
+                tot[a].re = visc[a].re - nl[a].re + press[a].re + 0.0 - hom[a].re;
+                tot[a].im = visc[a].im - nl[a].im + press[a].im + 0.0 - hom[a].im;
+            }
+            for (int a = 0; a < 3; a++) {
+                cx* r = &o->rk[a][m0];
+                r->re = (beta * r->re) + tot[a].re;
+                r->im = (beta * r->im) + tot[a].im;
+                u[a].re = u[a].re + (gamma * dt * r->re);
+                u[a].im = u[a].im + (gamma * dt * r->im);
+            }
+            /* f_RK3ContinuityFixRRot: project in the moving components umov = bmat u */
+            cx um[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (ex[a][b]) { um[a].re = um[a].re + (bm[a][b] * u[b].re); um[a].im = um[a].im + (bm[a][b] * u[b].im); }
+            cx kdu = {k[0] * um[0].re + k[1] * um[1].re + k[2] * um[2].re, k[0] * um[0].im + k[1] * um[1].im + k[2] * um[2].im};
+            for (int a = 0; a < 3; a++) {
+                um[a].re = um[a].re - (k[a] * kdu.re / kmag2);
+                um[a].im = um[a].im - (k[a] * kdu.im / kmag2);
+            }
+            cx ul[3] = {{0, 0}, {0, 0}, {0, 0}};
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++)
+                    if (ex[a][b]) { ul[a].re = ul[a].re + (bi[a][b] * um[b].re); ul[a].im = ul[a].im + (bi[a][b] * um[b].im); }
+            for (int a = 0; a < 3; a++) o->u[a][m0] = ul[a];
+        }
+    }
+}
+
 /* max |u1|+|u2|+|u3| (src/pf_fluidstats.f90:913-917,979) */
 static double cfl_velocity(const oracle* o) {
     double m = 0.0;
@@ -648,6 +784,7 @@ static void remesh_wave_space(oracle* o) {
             }
             for (int k = 0; k < NKK; k++) {
                 cx a = r[0][k], b3 = r[2][k];
+                if (o->rrot) { b3.re = 0.0; b3.im = 0.0; }   /* R-rot: no u1 += u3 (src/pf_rk3.f90:4155-4158) */
                 o->u[0][ij * NKK + k].re = a.re + b3.re;
                 o->u[0][ij * NKK + k].im = a.im + b3.im;
                 o->u[1][ij * NKK + k] = r[1][k];
@@ -699,12 +836,13 @@ static void dealias(oracle* o) {
 static void compute_nonlinear(oracle* o, int want_cfl) {
     dealias(o);
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};   /* spectral omega held in nl */
-    if (o->shear) vorticity_bf(o, om);
+    if (o->rrot) vorticity_rrot(o, om);
+    else if (o->shear) vorticity_bf(o, om);
     else vorticity_iso(o, om);
     for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
     for (int c = 0; c < 3; c++) spec_to_phys(o, om[c], o->phys[3 + c]);
     if (want_cfl) o->ucfl = cfl_velocity(o);
-    if (o->shear) nonlinear_bf(o);
+    if (o->shear && !o->rrot) nonlinear_bf(o);   /* R-rot: the isotropic product (src/pf_rk3.f90:1088-1089) */
     else nonlinear_iso(o);
     for (int c = 0; c < 3; c++) phys_to_spec(o, o->phys[3 + c], o->nl[c]);
 }
@@ -716,7 +854,8 @@ static void compute_nonlinear(oracle* o, int want_cfl) {
 void oracle_realspace_sums(oracle* o, double* out) {
     dealias(o);
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};
-    if (o->shear) vorticity_bf(o, om);
+    if (o->rrot) vorticity_rrot(o, om);
+    else if (o->shear) vorticity_bf(o, om);
     else vorticity_iso(o, om);
     for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
     for (int c = 0; c < 3; c++) spec_to_phys(o, om[c], o->phys[3 + c]);
@@ -1157,6 +1296,9 @@ static void stats_bf(const oracle* o, double* ek, double* tke, double* eps) {
                             ul[a].re = ul[a].re + o->binv[a][b] * um[b].re;
                             ul[a].im = ul[a].im + o->binv[a][b] * um[b].im;
                         }
+                /* f_FluidstatsFsPrimaryQuantsRRot: the R-rot state already holds the
+                 * laboratory components (src/pf_fluidstats.f90, ulab = umov) */
+                if (o->rrot) { ul[0] = um[0]; ul[1] = um[1]; ul[2] = um[2]; }
                 double km = sqrt((kl[0] * kl[0]) + (kl[1] * kl[1]) + (kl[2] * kl[2]));
                 double p11 = ul[0].re * ul[0].re + ul[0].im * ul[0].im;
                 double p22 = ul[1].re * ul[1].re + ul[1].im * ul[1].im;
@@ -1429,7 +1571,9 @@ int oracle_stage(oracle* o, int stage, int tstep, double* dt) {
     compute_nonlinear(o, stage == 1);
     if (stage == 1) *dt = tstep_dt(o, o->ucfl);
     particles_stage(o, stage, tstep, *dt);
-    if (o->shear) {
+    if (o->rrot) {
+        form_f_rrot(o, stage, *dt);
+    } else if (o->shear) {
         form_f_bf(o, stage, *dt);
     } else {
         force_calc(o, tstep, stage, *dt);

@@ -74,6 +74,112 @@ __device__ __forceinline__ void vort_bf(const BFT<R>& f, const C* u, const R* k,
     }
 }
 
+// R-rot form (NS_DEFORMED = NS_R_ROT): the velocity components are laboratory ones on
+// the sheared wavenumber grid.  f_RK3DerivativeRRot (src/pf_rk3.f90:3749-3780):
+// d/dx_j = i sum_m bmat(m,j) k_m over every m; the vorticity w = D x u assembled per
+// velocity component as the reference does (src/pf_rk3.f90:416-421, 470-475, 585-590).
+template <class R, class C>
+__device__ __forceinline__ C deriv_rrot(const BFT<R>& f, C u, const R* k, int j) {
+    C d;
+    d.x = R(0); d.y = R(0);
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        d.y = d.y + (f.bm[m][j] * k[m] * u.x);
+        d.x = d.x - (f.bm[m][j] * k[m] * u.y);
+    }
+    return d;
+}
+template <class R, class C>
+__device__ __forceinline__ void vort_rrot(const BFT<R>& f, const C* u, const R* k, C* w) {
+    const C dudy = deriv_rrot(f, u[0], k, 1), dudz = deriv_rrot(f, u[0], k, 2);
+    w[0].x = R(0); w[0].y = R(0);
+    w[1] = dudz;
+    w[2].x = -dudy.x; w[2].y = -dudy.y;
+    const C dvdx = deriv_rrot(f, u[1], k, 0), dvdz = deriv_rrot(f, u[1], k, 2);
+    w[0].x = w[0].x - dvdz.x; w[0].y = w[0].y - dvdz.y;
+    w[2].x = w[2].x + dvdx.x; w[2].y = w[2].y + dvdx.y;
+    const C dwdx = deriv_rrot(f, u[2], k, 0), dwdy = deriv_rrot(f, u[2], k, 1);
+    w[0].x = w[0].x + dwdy.x; w[0].y = w[0].y + dwdy.y;
+    w[1].x = w[1].x - dwdx.x; w[1].y = w[1].y - dwdx.y;
+}
+
+// f_RK3FormFRRot for F_SHEAR_DNS (src/pf_rk3.f90:2680-2856): viscous (f_RK3RRotViscous)
+// - NL + pressure (f_RK3RRotPressure) - source A u (f_RK3RRotSource); the nonlinear
+// term enters as computed (the isotropic product of the R-rot vorticity).
+__device__ __forceinline__ void rhs_rrot(const BF& f, double nu, const double* k, const double2* u,
+                                         const double2* nl, double2* tot) {
+    double p1[3] = {0.0, 0.0, 0.0}, p4 = 0.0;
+    double2 p2 = make_double2(0.0, 0.0), p3 = p2;
+#pragma unroll
+    for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            if (!bex(m, r)) continue;
+            p2.x = p2.x + (k[m] * f.bm[m][r] * nl[r].x);
+            p2.y = p2.y + (k[m] * f.bm[m][r] * nl[r].y);
+            if (r == 0) {   // amat(r, q) exists only for (r, q) = (1, 3)
+                p3.x = p3.x + (k[m] * f.bm[m][r] * f.a13 * u[2].x);
+                p3.y = p3.y + (k[m] * f.bm[m][r] * f.a13 * u[2].y);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                if (bex(q, r)) p4 = p4 + (k[m] * f.bm[m][r] * k[q] * f.bm[q][r]);
+        }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int pp = 0; pp < 3; pp++)
+            if (bex(pp, a)) p1[a] = p1[a] + k[pp] * f.bm[pp][a];
+    double2 visc[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+#pragma unroll
+    for (int l = 0; l < 3; l++)
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+            if (!bex(l, jj)) continue;
+#pragma unroll
+            for (int n = 0; n < 3; n++) {
+                if (!bex(n, jj)) continue;
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    visc[a].x = visc[a].x - nu * f.bm[l][jj] * f.bm[n][jj] * k[l] * k[n] * u[a].x;
+                    visc[a].y = visc[a].y - nu * f.bm[l][jj] * f.bm[n][jj] * k[l] * k[n] * u[a].y;
+                }
+            }
+        }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] / p4) * (p2.x + p3.x), (p1[a] / p4) * (p2.y + p3.y))
+                                      : make_double2(0.0, 0.0);
+        const double2 hom = (a == 0) ? make_double2(f.a13 * u[2].x, f.a13 * u[2].y) : make_double2(0.0, 0.0);
+        tot[a] = make_double2(visc[a].x - nl[a].x + pr.x + 0.0 - hom.x, visc[a].y - nl[a].y + pr.y + 0.0 - hom.y);
+    }
+}
+
+// f_RK3ContinuityFixRRot (src/pf_rk3.f90:3620-3693): project the moving components
+// bmat u on the (unsheared) wave vector, back with binv.
+__device__ __forceinline__ void contfix_rrot(const BF& f, const double* k, double kmag2, double2* u) {
+    double2 um[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (bex(a, b)) { um[a].x = um[a].x + (f.bm[a][b] * u[b].x); um[a].y = um[a].y + (f.bm[a][b] * u[b].y); }
+    const double2 kdu = make_double2(k[0] * um[0].x + k[1] * um[1].x + k[2] * um[2].x,
+                                     k[0] * um[0].y + k[1] * um[1].y + k[2] * um[2].y);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        um[a].x = um[a].x - (k[a] * kdu.x / kmag2);
+        um[a].y = um[a].y - (k[a] * kdu.y / kmag2);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        u[a] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+            if (bex(a, b)) { u[a].x = u[a].x + (f.bi[a][b] * um[b].x); u[a].y = u[a].y + (f.bi[a][b] * um[b].y); }
+    }
+}
+
 // f_ArraysDealiasSpherical / f_ArraysLESCutoff (src/pf_arrays.f90:1865-1987): a mode
 // whose laboratory-frame wave vector k_lab(n) = sum_m bmat(m,n) k(m) is longer than
 // g.dealias_cut is dropped.  Unfused, correctly rounded products and sums in the

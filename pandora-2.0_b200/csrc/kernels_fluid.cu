@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
                                 ul[a].x += bf.bi[a][b] * uv[b].x;
                                 ul[a].y += bf.bi[a][b] * uv[b].y;
                             }
+                    // R-rot holds laboratory components already (f_FluidstatsFsPrimaryQuantsRRot)
 #pragma unroll
-                    for (int a = 0; a < 3; a++) { kv[a] = kl[a]; uv[a] = ul[a]; }
+                    for (int a = 0; a < 3; a++) { kv[a] = kl[a]; if (!g.rrot) uv[a] = ul[a]; }
                 }
                 const double km = sqrt((kv[0] * kv[0]) + (kv[1] * kv[1]) + (kv[2] * kv[2]));
                 double q11 = uv[0].x * uv[0].x + uv[0].y * uv[0].y, q22 = uv[1].x * uv[1].x + uv[1].y * uv[1].y;
@@ -513,7 +514,8 @@ __global__ void __launch_bounds__(256) k_remesh(const __grid_constant__ MemberSe
             for (int c = 0; c < 3; c++) F.u[c][ij * NKK + k] = from_d<C>(mk(0.0, 0.0));
             continue;
         }
-        F.u[0][ij * NKK + k] = from_d<C>(mk(a.x + b3.x, a.y + b3.y));
+        // BF-rot: u1 += u3; R-rot keeps the components (src/pf_rk3.f90:4150-4162)
+        F.u[0][ij * NKK + k] = from_d<C>(g.rrot ? a : mk(a.x + b3.x, a.y + b3.y));
         F.u[1][ij * NKK + k] = from_d<C>(rowbuf[NKK + k]);
         F.u[2][ij * NKK + k] = from_d<C>(b3);
     }

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
                 }
                 if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
                 if constexpr (RS) rs_point(racc, rmax, g.shear, brs, u1, u2, u3, w1, w2, w3);
-                v[r] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3[r]);
+                v[r] = nl_point<T, C>(bf, g.shear && !g.rrot, u1, u2, u3, w1, w2, w3, n3[r]);
             }
         }
         __syncwarp();   // every lane has read arrays 0 and 1
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
             if (want_cfl) umax = fmax(umax, fabs(u1) + fabs(u2) + fabs(u3));
             if constexpr (RS) rs_point(racc, rmax, g.shear, brs, u1, u2, u3, w1, w2, w3);
             T n3;
-            e[0] = nl_point<T, C>(bf, g.shear, u1, u2, u3, w1, w2, w3, n3);
+            e[0] = nl_point<T, C>(bf, g.shear && !g.rrot, u1, u2, u3, w1, w2, w3, n3);
             e[XAS] = mk(n3, T(0));
         }
         __syncwarp();
@@ -345,8 +345,9 @@ template <class C> struct Out3 { C* p[3]; };
 // side: 3 and 4 CTAs of 256 threads per SM, without spills.
 // The per-mode arithmetic runs in FP64 registers in both forms (the FP32-mixed
 // form loads FP32 values and rounds once on the store).
-template <bool SHEAR, class T, int CAP>
-__global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+// FORM: 0 isotropic, 1 BF-rot shear, 2 R-rot shear.
+template <int FORM, class T, int CAP>
+__global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
@@ -372,9 +373,13 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_c
     double2 nl[3], uu[3], tot[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) { nl[c] = to_d(nlh[c * g.S + m]); uu[c] = to_d(F.u[c][m]); }
-    if constexpr (SHEAR) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
-        const BF bf = make_bf(g, F.clock);
+    BF bf;
+    if constexpr (FORM == 1) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
+        bf = make_bf(g, F.clock);
         rhs_bf(bf, g.nu, kv, uu, nl, tot);
+    } else if constexpr (FORM == 2) {   // f_RK3FormFRRot, F_SHEAR_DNS
+        bf = make_bf(g, F.clock);
+        rhs_rrot(bf, g.nu, kv, uu, nl, tot);
     } else {
         const double2 kdn = mk(k1 * nl[0].x + k2 * nl[1].x + k3 * nl[2].x,
                                k1 * nl[0].y + k2 * nl[1].y + k3 * nl[2].y);
@@ -411,6 +416,12 @@ __global__ void __launch_bounds__(256, SHEAR ? 4 : 3) k_rk_update(const __grid_c
         }
         F.rk[c][m] = from_d<C>(r);
         uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
+    }
+    if constexpr (FORM == 2) {   // f_RK3ContinuityFixRRot
+        contfix_rrot(bf, kv, kmag2, uu);
+#pragma unroll
+        for (int c = 0; c < 3; c++) F.u[c][m] = from_d<C>(uu[c]);
+        return;
     }
     const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x, k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
 #pragma unroll
@@ -524,7 +535,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
             // omega1 has no term in u1 and omega2 none in u2: those loads are skipped
             const C uv[3] = {f != 3 ? F.u[0][m] : zero, f != 4 ? F.u[1][m] : zero, F.u[2][m]};
             C w3[3];
-            vort_bf(bf, uv, kv, w3);
+            if (g.rrot) vort_rrot(bf, uv, kv, w3);   // R-rot: sheared curl of laboratory components
+            else vort_bf(bf, uv, kv, w3);
             return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
         } else {
             const T k1 = (T)i, k3 = (T)wvn(k, KK);
@@ -842,8 +854,9 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int
     return for_member_sets(M, B, [&](const auto& ms, int nb) {
         constexpr int CAP = PD_CAP(ms);
         const dim3 grid((unsigned)((g.S + 255) / 256), nb);
-        if (g.shear) k_rk_update<true, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
-        else k_rk_update<false, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+        if (g.rrot) k_rk_update<2, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+        else if (g.shear) k_rk_update<1, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+        else k_rk_update<0, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
     });
 }
 #undef PD_CAP

@@ -194,7 +194,9 @@ static int validate(const pandora_params* p) {
     if (p->precision != PANDORA_PREC_FP64 && p->precision != PANDORA_PREC_FP32_MIXED) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type != PANDORA_F_ISOTROPIC && p->f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type == PANDORA_F_SHEAR_DNS) {
-        if (p->ns_deformed != PANDORA_NS_BF_ROT) return PANDORA_ERR_UNSUPPORTED;
+        if (p->ns_deformed != PANDORA_NS_BF_ROT && p->ns_deformed != PANDORA_NS_R_ROT) return PANDORA_ERR_UNSUPPORTED;
+        // the R-form particle routines (p_RK3SolveParticleR, src/pp_control.f90:563-568) are not built
+        if (p->ns_deformed == PANDORA_NS_R_ROT && p->p_track_part) return PANDORA_ERR_UNSUPPORTED;
         if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
             return PANDORA_ERR_INVALID_ARG;
     }
@@ -240,6 +242,7 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.fnk = (int)p->force_kf;
     g.kkmax = kkmax_of(p);
     g.shear = (p->f_type == PANDORA_F_SHEAR_DNS) ? 1 : 0;
+    g.rrot = (g.shear && p->ns_deformed == PANDORA_NS_R_ROT) ? 1 : 0;
     g.bdiag[0] = 1.0 / (double)p->b110; g.bdiag[1] = 1.0 / (double)p->b220; g.bdiag[2] = 1.0 / (double)p->b330;
     g.bidiag[0] = (double)p->b110; g.bidiag[1] = (double)p->b220; g.bidiag[2] = (double)p->b330;
     g.shear_s = p->f_deform_s;

@@ -24,8 +24,9 @@ struct Geo {
     double force_kf;
     int fnk;              // aint(FORCE_KF)
     int kkmax;            // E(k) shells
-    // homogeneous shear (F_TYPE = F_SHEAR_DNS, BF-rot); zero for isotropic flow
+    // homogeneous shear (F_TYPE = F_SHEAR_DNS); zero for isotropic flow
     int shear;
+    int rrot;             // shear in the R-rot form (NS_DEFORMED = NS_R_ROT), else BF-rot
     double bdiag[3];      // bmat(1,1), bmat(2,2), bmat(3,3) = 1/B110, 1/B220, 1/B330
     double bidiag[3];     // binv diagonal = B110, B220, B330
     double shear_s;       // F_DEFORM_S = amat(1,3)

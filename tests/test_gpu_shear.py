@@ -58,6 +58,40 @@ def test_shear_steps_across_remesh(gpu_lib, mode):
     s.close()
 
 
+def test_rrot_steps_across_remesh(gpu_lib):
+    """NS_DEFORMED = 3 (R-rot): laboratory velocity components on the sheared
+    wavenumber grid, continuity fixed on the moving components; state, frame and
+    statistics against the oracle across the first remesh."""
+    import oracle as O
+    p = _shear(gpu_lib, 32, remesh_t=5)
+    p.ns_deformed = gpu_lib.NS_R_ROT
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    o.set_state(s.get_state())
+    t = 0.0
+    for step in range(1, 15):
+        t, dt = o.step(step, t)
+        dtg = s.step(step)
+        assert dtg == dt
+        if step in (1, 10, 11, 14):
+            e = rel_l2_fields(s.get_state(), o.get_state())
+            assert e < 1e-10, (step, e)
+            assert s.frame() == pytest.approx(o.frame(), rel=1e-14, abs=1e-15), step
+            ek_g, tke_g, eps_g, _ = s.stats()
+            ek_o, tke_o, eps_o = o.stats()
+            assert rel_l2(ek_g, ek_o) < 1e-8 and abs(eps_g - eps_o) < 1e-8 * abs(eps_o), step
+            assert tke_g == pytest.approx(tke_o, rel=1e-10)
+    s.close()
+
+
+def test_rrot_with_particles_unsupported(gpu_lib):
+    p = _shear(gpu_lib, 32, remesh_t=5, npart=256)
+    p.ns_deformed = gpu_lib.NS_R_ROT
+    with pytest.raises(gpu_lib.PandoraError):
+        gpu_lib.Simulation(p)
+
+
 def test_shear_particles(gpu_lib):
     p = _shear(gpu_lib, 32, remesh_t=4, npart=2048)
     import oracle as O

@@ -3,7 +3,7 @@ fixed shear time step, solenoidal state (no GPU)."""
 import numpy as np
 import pytest
 
-from helpers import divergence
+from helpers import divergence, wavenumbers
 
 
 def _o(n=24, remesh_t=5):
@@ -53,3 +53,28 @@ def test_shear_state_stays_solenoidal():
     assert np.abs(divergence(p, o.get_state())).max() < 1e-15
     ek, tke, eps = o.stats()
     assert np.isfinite(ek).all() and tke > 0 and eps > 0
+
+
+def test_rrot_continuity_across_remesh():
+    """R-rot form (NS_DEFORMED = 3): after a stage's update, the moving components
+    bmat u of the stored (laboratory) components are solenoidal, k . (bmat u) = 0, in
+    the frame of that stage (f_RK3ContinuityFixRRot), also after the remesh."""
+    import oracle as O
+    from pandora.params import workload_params
+    p = workload_params("shear", 32)
+    p.f_remesh_t, p.p_track_part, p.ns_deformed = 5, 0, 3
+    o = O.Oracle(p)
+    o.init_fluid()
+    t = 0.0
+    for step in range(1, 12):   # the remesh is step 11
+        t, dt = o.step(step, t)
+    o.stage(1, 12, dt)          # stage 1 of step 12 in the frame set at the end of step 11
+    u = o.get_state()
+    b13, _ = o.frame()
+    k1, k2, k3 = wavenumbers(p)
+    um = [u[0] / p.b110 + b13 * u[2], u[1] / p.b220, u[2] / p.b330]
+    div = k1 * um[0] + k2 * um[1] + k3 * um[2]
+    assert np.abs(div).max() < 1e-12 * max(np.abs(c).max() for c in u)
+    _, tke, eps = o.stats()
+    assert tke > 0.0 and eps > 0.0
+
