@@ -48,6 +48,7 @@ extern "C" {
 #define PANDORA_RK3_TIMESTEP_FIXED   2   /* pg_parameters.f90:212 */
 #define PANDORA_RK3_TIMESTEP_CFL     3   /* pg_parameters.f90:213 */
 #define PANDORA_NS_BF_ROT            1   /* pg_parameters.f90:219 */
+#define PANDORA_NS_R_CONV            2   /* pg_parameters.f90:220, convective Rogallo form */
 #define PANDORA_NS_R_ROT             3   /* pg_parameters.f90:221, rotational Rogallo form */
 #define PANDORA_DEALIASING_23        1   /* 2/3 rule (cube truncation), pg_parameters.f90:224 */
 #define PANDORA_DEALIASING_SPHERICAL 2   /* 2/3 sphere |k_lab| <= KMAX, pg_parameters.f90:225 */

@@ -153,9 +153,10 @@ typedef struct oracle {
     double bmat[3][3], binv[3][3], amat[3][3];
     int bexist[3][3], aexist[3][3];
     int shear;            /* F_TYPE == F_SHEAR_DNS */
-    int rrot;             /* ... in the R-rot form (NS_DEFORMED = NS_R_ROT), else BF-rot */
+    int rrot;             /* ... in a Rogallo form (NS_DEFORMED = NS_R_ROT or NS_R_CONV), else BF-rot */
+    int rconv;            /* ... in the convective Rogallo form (NS_R_CONV) */
     /* work */
-    double* phys[6];      /* physical fields [z][y][x] */
+    double* phys[12];     /* physical fields [z][y][x]: u, then omega (or the nine R-conv gradients) */
     cx *wa, *wb;          /* pencil work arrays */
     cx* nl[3];            /* spectral nonlinear term (normalised) */
     fplan px, py, pz;
@@ -204,10 +205,11 @@ oracle* oracle_create(const pandora_params* p) {
         o->bexist[0][2] = 1; o->amat[0][2] = p->f_deform_s; o->aexist[0][2] = 1;
     }
     o->shear = (p->f_type == PANDORA_F_SHEAR_DNS);
-    o->rrot = o->shear && p->ns_deformed == PANDORA_NS_R_ROT;
+    o->rrot = o->shear && (p->ns_deformed == PANDORA_NS_R_ROT || p->ns_deformed == PANDORA_NS_R_CONV);
+    o->rconv = o->shear && p->ns_deformed == PANDORA_NS_R_CONV;
     o->bmat[0][0] = 1.0 / o->binv[0][0]; o->bmat[1][1] = 1.0 / o->binv[1][1];
     o->bmat[2][2] = 1.0 / o->binv[2][2];
-    for (int f = 0; f < 6; f++) o->phys[f] = dalloc(o->R);
+    for (int f = 0; f < (o->rconv ? 12 : 6); f++) o->phys[f] = dalloc(o->R);
     long wa = (long)o->nki * o->nkj * o->nz, wb = (long)o->nki * o->nz * o->ny;
     o->wa = calloc_cx(wa); o->wb = calloc_cx(wb);
     if (plan_init(&o->px, o->nx) || plan_init(&o->py, o->ny) || plan_init(&o->pz, o->nz)) {
@@ -220,7 +222,7 @@ oracle* oracle_create(const pandora_params* p) {
 void oracle_destroy(oracle* o) {
     if (!o) return;
     for (int c = 0; c < 3; c++) { free(o->u[c]); free(o->rk[c]); free(o->nl[c]); free(o->ff[c]); }
-    for (int f = 0; f < 6; f++) free(o->phys[f]);
+    for (int f = 0; f < 12; f++) free(o->phys[f]);
     free(o->wa); free(o->wb); free(o->dens_mod);
     free(o->xp); free(o->up); free(o->uprk); free(o->prk); free(o->dp);
     plan_free(&o->px); plan_free(&o->py); plan_free(&o->pz);
@@ -494,6 +496,50 @@ static void vorticity_rrot(oracle* o, cx* om[3]) {
             w[1].re = w[1].re - dwdx.re; w[1].im = w[1].im - dwdx.im;
             om[0][m] = w[0]; om[1][m] = w[1]; om[2][m] = w[2];
         }
+    }
+}
+
+/* R-conv form (NS_DEFORMED = NS_R_CONV): the nine plain derivatives d u_c / d x_d =
+ * i k_d u_c (f_RK3Derivative, src/pf_rk3.f90:3735-3743) held as the reference's u4..u12
+ * (u4, u5, u6 = d(u, v, w)/dx, u7..u9 the y and u10..u12 the z derivatives;
+ * src/pf_rk3.f90:422-428, 476-482, 538-544), into phys[3 + 3 d + c]. */
+static void gradients_rconv(oracle* o) {
+    cx* g = o->nl[0];
+    for (int d = 0; d < 3; d++)
+        for (int c = 0; c < 3; c++) {
+#pragma omp parallel for schedule(static)
+            for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+                int i = (int)(ij / o->nkj), j = (int)(ij % o->nkj);
+                for (int k = 0; k < o->nkk; k++) {
+                    long m = ij * o->nkk + k;
+                    const double kd = d == 0 ? wvn(i, o->ki) : (d == 1 ? wvn(j, o->kj) : wvn(k, o->kk));
+                    const cx u = o->u[c][m];
+                    g[m].im = kd * u.re;
+                    g[m].re = -kd * u.im;
+                }
+            }
+            spec_to_phys(o, g, o->phys[3 + 3 * d + c]);
+        }
+}
+
+/* f_RK3ComputeNonlinearRConv (src/pf_rk3.f90:1717-1774): with duidk(k, i) = d u_i / d x_k
+ * (phys[3 + 3 (k-1) + (i-1)]), NL_i = sum_j sum_k bmat(k,j) duidk(k,i) u_j over the
+ * existing bmat entries, into phys[3..5]. */
+static void nonlinear_rconv(oracle* o) {
+    const double(*bm)[3] = o->bmat;
+    const int(*ex)[3] = o->bexist;
+#pragma omp parallel for schedule(static)
+    for (long p = 0; p < o->R; p++) {
+        const double uj[3] = {o->phys[0][p], o->phys[1][p], o->phys[2][p]};
+        double du[3][3];
+        for (int k = 0; k < 3; k++)
+            for (int i = 0; i < 3; i++) du[k][i] = o->phys[3 + 3 * k + i][p];
+        double nl[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++)
+                    if (ex[k][j]) nl[i] = nl[i] + ((bm[k][j] * du[k][i]) * uj[j]);
+        o->phys[3][p] = nl[0]; o->phys[4][p] = nl[1]; o->phys[5][p] = nl[2];
     }
 }
 
@@ -835,6 +881,14 @@ static void dealias(oracle* o) {
  * src/pf_rk3.f90:2101-2109, finds the state unchanged) */
 static void compute_nonlinear(oracle* o, int want_cfl) {
     dealias(o);
+    if (o->rconv) {   /* 12 transformed fields (src/pf_rk3.f90:254-267, 825-869) */
+        for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
+        gradients_rconv(o);
+        if (want_cfl) o->ucfl = cfl_velocity(o);
+        nonlinear_rconv(o);
+        for (int c = 0; c < 3; c++) phys_to_spec(o, o->phys[3 + c], o->nl[c]);
+        return;
+    }
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};   /* spectral omega held in nl */
     if (o->rrot) vorticity_rrot(o, om);
     else if (o->shear) vorticity_bf(o, om);

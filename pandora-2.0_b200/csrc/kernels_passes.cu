@@ -323,6 +323,144 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
 }
 
 // ---------------------------------------------------------------------------
+// K3 of the R-conv form (NS_DEFORMED = NS_R_CONV): the x pass of the twelve fields
+// u1..u3 and d u_c / d x_d (yb field 3 + 3d + c), then f_RK3ComputeNonlinearRConv
+// (src/pf_rk3.f90:1717-1774), NL_i = sum_d v_d d u_i / d x_d with v_d = sum_j
+// bmat(d,j) u_j, then the forward transforms and split of K3.  One warp per line
+// over four arrays: the pairs (u1,u2) and (u3, du1/dx1) first; v and the partial sums
+// then stay in the arrays that the later pairs do not use, which are transformed two
+// and then one at a time.  Single simulations only.
+// ---------------------------------------------------------------------------
+template <int N, class T> struct ConvCfg {
+    static constexpr int per_warp = 4 * xas<N>() * (int)sizeof(typename Cplx<T>::type);
+    static constexpr int fit = (200 * 1024) / per_warp;
+    static constexpr int NW = fit >= 8 ? 8 : (fit < 1 ? 1 : fit);
+    static constexpr size_t smem = (size_t)NW * per_warp;
+};
+
+template <int NX, class T>
+__global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const __grid_constant__ MemberSet<T, 1> ms,
+                                                                          int want_cfl, long long pf_lines) {
+    using C = typename FieldsT<T>::C;
+    using XP = pdfft::FusedPlan<NX>;   // the backward plan r0, r1, r2 (run unfused here)
+    const Member<T>& mm = ms.m[0];
+    if (!mm.active) return;
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+    constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>(), NW = ConvCfg<NX, T>::NW;
+    constexpr int KB = NX / 3;
+    constexpr int R0 = XP::r0, R1 = XP::r1, R2 = XP::r2, NP = XP::np;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long lines = (long long)g.ny * g.nz;
+    const C* tw = F.tw_x;
+    const long long q = (long long)blockIdx.x * NW + w;
+    if (q >= lines) return;                       // whole warp; no block barrier follows
+    C* s = smem_as<C>() + (size_t)w * 4 * XAS;
+    const long long fstride = lines * g.nkip;
+    const int NKI = g.nki;
+    C* b = F.yb + q * g.nkip;
+    const BFT<T> bf = bf_as<T>(make_bf(g, F.clock));
+    // the Hermitian extension of the half spectra of fields fa and fb into array p, as K3
+    auto build = [&](int p, int fa, int fb) {
+        for (int m = lane; m < NKI; m += 32) {
+            C X = b[fa * fstride + m], Y = b[fb * fstride + m];
+            if (m == 0) { X.y = T(0); Y.y = T(0); }
+            s[p * XAS + prow<XPS>(m)] = mk(X.x - Y.y, X.y + Y.x);
+            if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
+        }
+        __syncwarp();
+    };
+    auto bwd1 = [&](C* a) { pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(a, tw, lane); };
+    auto bwd2 = [&](C* a) {   // arrays a and a + XAS
+        if constexpr (NA == 2) pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB>(a, tw, lane);
+        else { bwd1(a); bwd1(a + XAS); }
+    };
+    // (u1,u2), (u3, du1/dx1) -> v = bmat u, NL1 = v1 du1/dx1; arrays 0, 1 = (v1,v2), (v3,NL1)
+    build(0, 0, 1);
+    build(1, 2, 3);
+    bwd2(s);
+    T umax = T(0);
+    for (int n = lane; n < NX; n += 32) {
+        C* e = s + prow<XPS>(n);
+        const C a = e[0], c1 = e[XAS];
+        const T u[3] = {a.x, a.y, c1.x};
+        if (want_cfl) umax = fmax(umax, fabs(u[0]) + fabs(u[1]) + fabs(u[2]));
+        T v[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            v[d] = T(0);
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if (bex(d, j)) v[d] += bf.bm[d][j] * u[j];
+        }
+        e[0] = mk(v[0], v[1]);
+        e[XAS] = mk(v[2], v[0] * c1.y);
+    }
+    // (du2/dx1, du3/dx1), (du1/dx2, du2/dx2); arrays 0..2 = (v2,v3), (NL1,NL2), (NL3,-)
+    build(2, 4, 5);
+    build(3, 6, 7);
+    bwd2(s + 2 * XAS);
+    for (int n = lane; n < NX; n += 32) {
+        C* e = s + prow<XPS>(n);
+        const C a = e[0], c1 = e[XAS], g1 = e[2 * XAS], g2 = e[3 * XAS];
+        const T v1 = a.x, v2 = a.y, v3 = c1.x;
+        const T n1 = c1.y + v2 * g2.x;
+        const T n2 = v1 * g1.x + v2 * g2.y;
+        const T n3 = v1 * g1.y;
+        e[0] = mk(v2, v3);
+        e[XAS] = mk(n1, n2);
+        e[2 * XAS] = mk(n3, T(0));
+    }
+    // (du3/dx2, du1/dx3)
+    build(3, 8, 9);
+    bwd1(s + 3 * XAS);
+    for (int n = lane; n < NX; n += 32) {
+        C* e = s + prow<XPS>(n);
+        const C a = e[0], c1 = e[XAS], c2 = e[2 * XAS], g1 = e[3 * XAS];
+        e[XAS] = mk(c1.x + a.y * g1.y, c1.y);
+        e[2 * XAS] = mk(c2.x + a.x * g1.x, T(0));
+    }
+    // (du2/dx3, du3/dx3); arrays 0, 1 = (NL1,NL2), (NL3,0) for the forward transforms
+    build(3, 10, 11);
+    bwd1(s + 3 * XAS);
+    for (int n = lane; n < NX; n += 32) {
+        C* e = s + prow<XPS>(n);
+        const C a = e[0], c1 = e[XAS], c2 = e[2 * XAS], g1 = e[3 * XAS];
+        const T v3 = a.y;
+        e[0] = mk(c1.x, c1.y + v3 * g1.x);
+        e[XAS] = mk(c2.x + v3 * g1.y, T(0));
+    }
+    __syncwarp();
+    if (want_cfl) {
+        for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+        if (threadIdx.x % 32 == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
+    }
+    if (pf_lines > 0 && q + pf_lines < lines && lane < 12)
+        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
+    if constexpr (NA == 2) {
+        pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
+    } else {
+        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
+        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s + XAS, tw, lane);
+    }
+    const T half = T(0.5);
+    for (int m = lane; m < g.nkip; m += 32) {
+        C n1 = mk(T(0), T(0)), n2 = n1, n3 = n1;
+        if (m < NKI) {
+            const int mc = (NX - m) % NX;
+            const C Z = s[prow<XPS>(m)], Zc = s[prow<XPS>(mc)];
+            n1 = mk(half * (Z.x + Zc.x), half * (Z.y - Zc.y));
+            n2 = mk(half * (Z.y + Zc.y), -half * (Z.x - Zc.x));
+            const C W = s[XAS + prow<XPS>(m)], Wc = s[XAS + prow<XPS>(mc)];
+            n3 = mk(half * (W.x + Wc.x), half * (W.y - Wc.y));
+        }
+        b[m] = n1;
+        b[fstride + m] = n2;
+        b[2 * fstride + m] = n3;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // K5: forward z transforms x normalisation, truncate k (f_RK3TransformkRs2Fs +
 // f_Fftw_k_Rs2Fs, src/pf_rk3.f90:2242-2316, src/pf_fftw.f90:841-879) into NL-hat
 // (K5a), then the per-mode update (K5b).  NL-hat goes to the y-pencil buffer,
@@ -485,7 +623,8 @@ template <int NZ, bool SHEAR, class T, int CAP>
 __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
                                                                                                    long long pf_ctas) {
     using C = typename FieldsT<T>::C;
-    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / 6];
+    const int nf = CAP == 1 ? pass_fields(ms.m[0].g) : 6;   // batches: no R-conv members
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / nf];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
         if (mm.F.clock->status & PD_ST_IDLE) return;
@@ -494,7 +633,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     const Geo g = mm.g;
     C* s = smem_as<C>();
     constexpr int LT = TCfg<NZ>::template lines<T>();
-    const int f = blockIdx.x % 6, i0 = blockIdx.y * LT, j = blockIdx.z;
+    const int f = blockIdx.x % nf, i0 = blockIdx.y * LT, j = blockIdx.z;
     const int lmax = g.nkip - i0;   // lines of this tile inside the i padding
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
     const int KK = g.kk, NKK = g.nkk, nki = g.nki;
@@ -503,8 +642,11 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     const long long istride = (long long)g.nkj * NKK;
     const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
-    // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1)
-    C* const pa = (f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]);
+    // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1).  R-conv: field 3 + 3d + c
+    // is d u_c / d x_d.
+    const bool rconv = SHEAR && g.rconv;
+    C* const pa = (rconv && f >= 3) ? F.u[(f - 3) % 3]
+                : ((f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]));
     const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
     BFT<T> bf;
     if constexpr (SHEAR) {
@@ -529,7 +671,14 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
             return mk(T(0), T(0));
         }
         if (f < 3) return pa[m];
-        if constexpr (SHEAR) {   // BF-rot vorticity (f_RK3VorticityBFRot), in T
+        if constexpr (SHEAR) {
+            if (rconv) {   // f_RK3Derivative (src/pf_rk3.f90:3735-3743): i k_d u_c, plain k_d
+                const int d = (f - 3) / 3;
+                const T kd = d == 0 ? (T)i : (d == 1 ? k2t : (T)wvn(k, KK));
+                const C uc = pa[m];
+                return mk(-kd * uc.y, kd * uc.x);
+            }
+            // BF-rot vorticity (f_RK3VorticityBFRot), in T
             const T kv[3] = {(T)i, k2t, (T)wvn(k, KK)};
             const C zero = mk(T(0), T(0));
             // omega1 has no term in u1 and omega2 none in u2: those loads are skipped
@@ -555,20 +704,20 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     // After the first pass: prefetch into L2 the velocity rows of the CTA a wave of
     // resident CTAs later (single simulations: blocks (f, tile, j) in launch order),
     // so that its loads wait on L2 rather than HBM.  A vorticity CTA's rows are all
-    // three components.
+    // three components, an R-conv gradient CTA's one.
     const C* const u0 = F.u[0];
     const C* const u1 = F.u[1];
     const C* const u2 = F.u[2];
     const int nkj = g.nkj;
-    auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2]() {
+    auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2, nf, rconv]() {
         if (pf_ctas <= 0) return;
-        const long long nblk = 6LL * gridDim.y * gridDim.z;
-        const long long nxt = blockIdx.x + 6LL * (blockIdx.y + (long long)gridDim.y * blockIdx.z) + pf_ctas;
+        const long long nblk = (long long)nf * gridDim.y * gridDim.z;
+        const long long nxt = blockIdx.x + (long long)nf * (blockIdx.y + (long long)gridDim.y * blockIdx.z) + pf_ctas;
         if (nxt >= nblk) return;
-        const int f2 = (int)(nxt % 6), ti = (int)((nxt / 6) % gridDim.y), j2 = (int)(nxt / (6LL * gridDim.y));
-        const int nc = f2 < 3 ? 1 : 3, t = threadIdx.x;
+        const int f2 = (int)(nxt % nf), ti = (int)((nxt / nf) % gridDim.y), j2 = (int)(nxt / ((long long)nf * gridDim.y));
+        const int nc = (f2 < 3 || rconv) ? 1 : 3, t = threadIdx.x;
         if (t >= LT * nc) return;
-        const int c = f2 < 3 ? f2 : t / LT, i = ti * LT + t % LT;
+        const int c = f2 < 3 ? f2 : (rconv ? (f2 - 3) % 3 : t / LT), i = ti * LT + t % LT;
         const C* uc = c == 0 ? u0 : (c == 1 ? u1 : u2);
         if (i < nki) prefetch_l2(uc + ((long long)i * nkj + j2) * NKK, NKK * sizeof(C));
     };
@@ -580,7 +729,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
 template <int NY, class T, int CAP>
 __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
-    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 6];
+    const int nf = CAP == 1 ? pass_fields(ms.m[0].g) : 6;   // batches: no R-conv members
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / nf];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
         if (mm.F.clock->status & PD_ST_IDLE) return;
@@ -589,7 +739,7 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
     const Geo g = mm.g;
     C* s = smem_as<C>();
     constexpr int LT = TCfg<NY>::template lines<T>();
-    const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % 6;
+    const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % nf;
     const int lmax = g.nkip - i0;
     const int KJ = g.kj, NKJ = g.nkj;
     const long long rs = g.nkip;
@@ -720,6 +870,9 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
     }                                                                                          \
     if (g.nx == N) {                                                                           \
         if ((e = set_smem(k_xpass<N, T, CAP>, smem_kx<N, T>()))) return e;                     \
+        if constexpr (CAP == 1) {                                                              \
+            if (g.rconv && (e = set_smem(k_xpass_conv<N, T>, ConvCfg<N, T>::smem))) return e;  \
+        }                                                                                      \
     }
 #define PD_CFG(N)                                                                              \
     PD_CFG1(N, 1)                                                                              \
@@ -743,7 +896,7 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
-                const dim3 grid(6 * nb, TCfg<N>::template tiles<T>(g), g.nkj);                                       \
+                const dim3 grid(pass_fields(g) * nb, TCfg<N>::template tiles<T>(g), g.nkj);                          \
                 constexpr int NT = TCfg<N>::template nt<T>();                                      \
                 const size_t sm = TCfg<N>::template smem<T>();                                     \
                 if (g.shear) {                                                                    \
@@ -768,7 +921,7 @@ template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, 6 * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms); \
+                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, pass_fields(g) * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -784,6 +937,15 @@ cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys,
     case N:                                                                                       \
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
+            if constexpr (CAP == 1) {                                                             \
+                if (g.rconv) {   /* R-conv: twelve fields, single simulations */                 \
+                    constexpr int NW = ConvCfg<N, T>::NW;                                         \
+                    const long long nl = (lines + NW - 1) / NW;                                   \
+                    const long long pf = NW * resident_ctas(k_xpass_conv<N, T>, 32 * NW, ConvCfg<N, T>::smem); \
+                    k_xpass_conv<N, T><<<dim3((unsigned)nl), 32 * NW, ConvCfg<N, T>::smem, st>>>(ms, want_cfl, pf); \
+                    return;                                                                       \
+                }                                                                                 \
+            }                                                                                     \
             if constexpr (CAP == 1 || batch_len<N>()) {                                           \
                 const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;                     \
                 /* L2 prefetch distance: one wave of resident CTAs (single simulations) */      \

@@ -194,9 +194,11 @@ static int validate(const pandora_params* p) {
     if (p->precision != PANDORA_PREC_FP64 && p->precision != PANDORA_PREC_FP32_MIXED) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type != PANDORA_F_ISOTROPIC && p->f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
     if (p->f_type == PANDORA_F_SHEAR_DNS) {
-        if (p->ns_deformed != PANDORA_NS_BF_ROT && p->ns_deformed != PANDORA_NS_R_ROT) return PANDORA_ERR_UNSUPPORTED;
+        if (p->ns_deformed != PANDORA_NS_BF_ROT && p->ns_deformed != PANDORA_NS_R_ROT &&
+            p->ns_deformed != PANDORA_NS_R_CONV)
+            return PANDORA_ERR_UNSUPPORTED;
         // the R-form particle routines (p_RK3SolveParticleR, src/pp_control.f90:563-568) are not built
-        if (p->ns_deformed == PANDORA_NS_R_ROT && p->p_track_part) return PANDORA_ERR_UNSUPPORTED;
+        if (p->ns_deformed != PANDORA_NS_BF_ROT && p->p_track_part) return PANDORA_ERR_UNSUPPORTED;
         if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
             return PANDORA_ERR_INVALID_ARG;
     }
@@ -242,7 +244,8 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.fnk = (int)p->force_kf;
     g.kkmax = kkmax_of(p);
     g.shear = (p->f_type == PANDORA_F_SHEAR_DNS) ? 1 : 0;
-    g.rrot = (g.shear && p->ns_deformed == PANDORA_NS_R_ROT) ? 1 : 0;
+    g.rrot = (g.shear && (p->ns_deformed == PANDORA_NS_R_ROT || p->ns_deformed == PANDORA_NS_R_CONV)) ? 1 : 0;
+    g.rconv = (g.shear && p->ns_deformed == PANDORA_NS_R_CONV) ? 1 : 0;
     g.bdiag[0] = 1.0 / (double)p->b110; g.bdiag[1] = 1.0 / (double)p->b220; g.bdiag[2] = 1.0 / (double)p->b330;
     g.bidiag[0] = (double)p->b110; g.bidiag[1] = (double)p->b220; g.bidiag[2] = (double)p->b330;
     g.shear_s = p->f_deform_s;
@@ -267,10 +270,12 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
         if (e != cudaSuccess) { cudaGetLastError(); release(h); return PANDORA_ERR_OOM; } \
     } while (0)
     // fields in the stored precision; zb (6 x NZ x NKJ x NKIP values, NZ >= NKK and
-    // NKIP >= NKI) always holds 3S FP64 values, the conversion scratch of the mixed form
+    // NKIP >= NKI) always holds 3S FP64 values, the conversion scratch of the mixed form.
+    // The R-conv form carries 12 fields through the inverse passes.
+    const size_t nfb = pass_fields(g);
     PD_ALLOC(h->fbuf, ce * 6 * (size_t)g.S);
-    PD_ALLOC(h->F.zb, ce * 6 * (size_t)g.nz * g.nkj * g.nkip);
-    PD_ALLOC(h->F.yb, ce * 6 * (size_t)g.nz * g.ny * g.nkip);
+    PD_ALLOC(h->F.zb, ce * nfb * (size_t)g.nz * g.nkj * g.nkip);
+    PD_ALLOC(h->F.yb, ce * nfb * (size_t)g.nz * g.ny * g.nkip);
     if (h->particles_on) PD_ALLOC(h->F.phys, ce / 2 * 3 * (size_t)g.R);
     PD_ALLOC(h->F.forcing, sizeof(double2) * 3 * (size_t)h->nforce);
     PD_ALLOC(h->tw, ce * (size_t)(g.nx + g.ny + g.nz));
@@ -897,6 +902,8 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
 // f_FluidstatsRsCollect does (src/pf_fluidstats.f90:960-1100).
 extern "C" int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n) {
     if (!h || !out || n < 25) return PANDORA_ERR_INVALID_ARG;
+    // the R-conv form transforms velocity gradients, not a vorticity, to real space
+    if (h->g.rconv) return PANDORA_ERR_UNSUPPORTED;
     cudaSetDevice(h->dev);
     const size_t words = 32 * 32;
     if (!h->rsbuf) {
@@ -1240,7 +1247,8 @@ extern "C" int pandora_batch_bytes(const pandora_params* p, int32_t capacity, in
     const long long S = nki * nkj * nkk, R = nx * ny * nz;
     const long long ce = p->precision == PANDORA_PREC_FP32_MIXED ? 8 : 16;
     const long long np = p->p_track_part ? p->p_np_global : 0;
-    long long per = ce * 6 * S + ce * 6 * nz * nkj * nkip + ce * 6 * nz * ny * nkip + ce * (nx + ny + nz);
+    const long long nfb = (p->f_type == PANDORA_F_SHEAR_DNS && p->ns_deformed == PANDORA_NS_R_CONV) ? 12 : 6;
+    long long per = ce * 6 * S + ce * nfb * nz * nkj * nkip + ce * nfb * nz * ny * nkip + ce * (nx + ny + nz);
     if (p->p_track_part) per += ce / 2 * 3 * R + 2 * 8 * 14 * np + 4 * np;
     per += 1 << 20;   // clock, forcing, shells, member descriptors, allocator granularity
     *bytes = per * capacity;
@@ -1252,6 +1260,8 @@ extern "C" int pandora_batch_create(const pandora_params* cls, int32_t capacity,
     *out = nullptr;
     int rc = validate(cls);
     if (rc) return rc;
+    // the R-conv x pass has single-simulation instantiations only
+    if (cls->f_type == PANDORA_F_SHEAR_DNS && cls->ns_deformed == PANDORA_NS_R_CONV) return PANDORA_ERR_UNSUPPORTED;
     pandora_batch* b = new (std::nothrow) pandora_batch();
     if (!b) return PANDORA_ERR_OOM;
     cudaGetDevice(&b->dev);

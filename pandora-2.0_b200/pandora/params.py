@@ -19,6 +19,7 @@ RK3_TIMESTEP_DECIDE = 1
 RK3_TIMESTEP_FIXED = 2
 RK3_TIMESTEP_CFL = 3
 NS_BF_ROT = 1
+NS_R_CONV = 2       # convective Rogallo form, 12 transformed fields (src/pf_rk3.f90:1717-1774)
 NS_R_ROT = 3        # laboratory components on the sheared grid (src/pf_rk3.f90 R-rot)
 F_INIT_NULL = 0
 F_INIT_GAUSS = 3

@@ -108,6 +108,23 @@ def test_mixed_shear_across_remesh(gpu_lib):
     assert e < 1e-4, e
 
 
+@pytest.mark.parametrize("form", [2, 3])
+def test_mixed_rogallo_across_remesh(gpu_lib, form):
+    """R-conv (2) and R-rot (3) shear forms in FP32 at 32^3 across a remesh."""
+    p = gpu_lib.workload_params("shear", 32)
+    p.p_track_part = 0
+    p.f_remesh_t = 2
+    p.ns_deformed = form
+    o, s = _mixed(gpu_lib, p)
+    t = 0.0
+    for step in range(1, 7):
+        t, _ = o.step(step, t)
+        s.step(step)
+    e = rel_l2_fields(s.get_state(), o.get_state())
+    s.close()
+    assert e < 1e-4, e
+
+
 def test_mixed_error_module_small(gpu_lib):
     """pandora.mixed_error on a small case: both forms from one seed, errors stated."""
     from pandora import mixed_error

@@ -58,13 +58,15 @@ def test_shear_steps_across_remesh(gpu_lib, mode):
     s.close()
 
 
-def test_rrot_steps_across_remesh(gpu_lib):
-    """NS_DEFORMED = 3 (R-rot): laboratory velocity components on the sheared
-    wavenumber grid, continuity fixed on the moving components; state, frame and
-    statistics against the oracle across the first remesh."""
+@pytest.mark.parametrize("form", [2, 3])
+def test_rogallo_steps_across_remesh(gpu_lib, form):
+    """NS_DEFORMED = 2 (R-conv) and 3 (R-rot): laboratory velocity components on the
+    sheared wavenumber grid, continuity fixed on the moving components; state, frame
+    and statistics against the oracle across the first remesh.  R-conv carries u and
+    its nine gradients through the inverse passes."""
     import oracle as O
     p = _shear(gpu_lib, 32, remesh_t=5)
-    p.ns_deformed = gpu_lib.NS_R_ROT
+    p.ns_deformed = form
     o = O.Oracle(p)
     s = gpu_lib.Simulation(p)
     s.init_fluid()
@@ -85,11 +87,52 @@ def test_rrot_steps_across_remesh(gpu_lib):
     s.close()
 
 
-def test_rrot_with_particles_unsupported(gpu_lib):
+@pytest.mark.parametrize("dims", [(16, 16, 16), (24, 16, 16), (32, 16, 16), (48, 32, 24), (64, 16, 16),
+                                  (96, 16, 16), (128, 16, 16), (192, 16, 16), (256, 16, 16),
+                                  (384, 16, 16), (512, 16, 16), (768, 16, 16), (1024, 16, 16),
+                                  (16, 96, 16), (16, 16, 96)])
+def test_rconv_nonlinear_every_length(gpu_lib, dims):
+    """The R-conv product (twelve fields through K1/K2, the four-array x pass) at every
+    x length, in a frame with bmat(1,3) != 0 (after two steps)."""
+    import oracle as O
+    p = _shear(gpu_lib, 32, remesh_t=5)
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    p.ns_deformed = gpu_lib.NS_R_CONV
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    o.set_state(s.get_state())
+    t = 0.0
+    for step in (1, 2):
+        t, _ = o.step(step, t)
+        s.step(step)
+    assert s.frame()[0] != 0.0
+    assert s.frame() == pytest.approx(o.frame(), rel=1e-14)
+    o.set_state(s.get_state())      # the product of one state: no drift of the two runs
+    e = rel_l2_fields(s.nonlinear(), o.nonlinear())
+    s.close()
+    assert e < 1e-12, e
+
+
+@pytest.mark.parametrize("form", [2, 3])
+def test_rogallo_with_particles_unsupported(gpu_lib, form):
     p = _shear(gpu_lib, 32, remesh_t=5, npart=256)
-    p.ns_deformed = gpu_lib.NS_R_ROT
+    p.ns_deformed = form
     with pytest.raises(gpu_lib.PandoraError):
         gpu_lib.Simulation(p)
+
+
+def test_rconv_limits(gpu_lib):
+    """R-conv: no real-space vorticity statistics (its real-space fields are gradients)
+    and single simulations only (no batched x pass)."""
+    p = _shear(gpu_lib, 32, remesh_t=5)
+    p.ns_deformed = gpu_lib.NS_R_CONV
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        with pytest.raises(gpu_lib.PandoraError):
+            s.realspace_stats()
+    with pytest.raises(gpu_lib.PandoraError):
+        gpu_lib.Batch(p, 2)
 
 
 def test_shear_particles(gpu_lib):

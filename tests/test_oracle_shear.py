@@ -55,14 +55,16 @@ def test_shear_state_stays_solenoidal():
     assert np.isfinite(ek).all() and tke > 0 and eps > 0
 
 
-def test_rrot_continuity_across_remesh():
-    """R-rot form (NS_DEFORMED = 3): after a stage's update, the moving components
-    bmat u of the stored (laboratory) components are solenoidal, k . (bmat u) = 0, in
-    the frame of that stage (f_RK3ContinuityFixRRot), also after the remesh."""
+@pytest.mark.parametrize("form", [2, 3])
+def test_rogallo_continuity_across_remesh(form):
+    """R-conv (NS_DEFORMED = 2) and R-rot (3) forms: after a stage's update, the moving
+    components bmat u of the stored (laboratory) components are solenoidal,
+    k . (bmat u) = 0, in the frame of that stage (f_RK3ContinuityFixRRot), also after
+    the remesh."""
     import oracle as O
     from pandora.params import workload_params
     p = workload_params("shear", 32)
-    p.f_remesh_t, p.p_track_part, p.ns_deformed = 5, 0, 3
+    p.f_remesh_t, p.p_track_part, p.ns_deformed = 5, 0, form
     o = O.Oracle(p)
     o.init_fluid()
     t = 0.0
@@ -77,4 +79,46 @@ def test_rrot_continuity_across_remesh():
     assert np.abs(div).max() < 1e-12 * max(np.abs(c).max() for c in u)
     _, tke, eps = o.stats()
     assert tke > 0.0 and eps > 0.0
+
+
+def test_rconv_equals_rrot_without_aliasing():
+    """The convective product (u . D) u of R-conv and the rotational one w x u of R-rot
+    differ by the laboratory gradient D(|u|^2 / 2), which the R-rot pressure term
+    (shared by both forms, src/pf_rk3.f90:2089-2093) projects out.  For a field with
+    moving-frame wavenumbers |k_d| <= N/6 the products are not aliased, so one stage of
+    the two forms agrees to round-off, in a frame with bmat(1,3) != 0."""
+    import oracle as O
+    from pandora.params import workload_params
+    p = workload_params("shear", 32)
+    p.f_remesh_t, p.p_track_part, p.ns_deformed = 5, 0, 3
+    o = O.Oracle(p)
+    o.init_fluid()
+    u = o.get_state()
+    k1, k2, k3 = wavenumbers(p)
+    keep = (np.abs(k1) <= 32 // 6) & (np.abs(k2) <= 32 // 6) & (np.abs(k3) <= 32 // 6)
+    u = [np.where(keep, c, 0.0) for c in u]
+    out = {}
+    for form in (2, 3):
+        q = p.copy()
+        q.ns_deformed = form
+        o2 = O.Oracle(q)
+        o2.update_b(5, 0.3)
+        assert o2.frame()[0] != 0.0
+        o2.set_state(u)
+        o2.stage(1, 5, 0.5 / p.f_deform_s / p.f_remesh_t)
+        out[form] = o2.get_state()
+    scale = max(np.abs(c).max() for c in out[3])
+    diff = max(np.abs(a - b).max() for a, b in zip(out[2], out[3]))
+    assert diff < 1e-13 * scale, diff / scale
+    # while the two products themselves differ by that gradient
+    nl = {}
+    for form in (2, 3):
+        q = p.copy()
+        q.ns_deformed = form
+        o2 = O.Oracle(q)
+        o2.update_b(5, 0.3)
+        o2.set_state(u)
+        nl[form] = o2.nonlinear()
+    gap = max(np.abs(a - b).max() for a, b in zip(nl[2], nl[3]))
+    assert gap > 1e-2 * max(np.abs(c).max() for c in nl[3])
 
