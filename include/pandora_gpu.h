@@ -215,8 +215,17 @@ int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, double* n3);
  * NX NY NZ points of u1u1 u2u2 u3u3 u1u2 u1u3 u2u3, u1^3 u2^3 u3^3, u1^4 u2^4 u3^4
  * (laboratory-frame velocity), w1^2 w2^2 w3^2, w1^3.., w1^4..; out[21] max |u1|+|u2|+|u3|,
  * out[22..24] max |w_i|.  n >= 25.  Normalisation as f_FluidstatsRsCollect
- * (src/pf_fluidstats.f90:960-1100) is the caller's. */
+ * (src/pf_fluidstats.f90:960-1100) is the caller's.  In the R-conv form w is
+ * d(u1,u2,u3)/dx1, the fields the reference holds in u4..u6 there. */
 int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n);
+
+/* TS_CORR's longitudinal autocorrelation of the current state (f_FluidstatsRs2D,
+ * src/pf_fluidstats.f90:933-945): r[l] = sum over the NX NY NZ points of u1(x) u1(x + l dx),
+ * l = 0..NX/2, periodic in x, u1(x) in the laboratory frame for shear and u1(x + l dx) the
+ * stored component (the reference's temp_r1i).  n >= NX/2 + 1.  r1i = r / (rs_u1u1 N^3)
+ * and rs_lint11 = dx_laboratoryframe sum_l r[l] / (rs_u1u1 N^3) are the caller's
+ * (src/pf_fluidstats.f90:1092-1105). */
+int pandora_x_correlation(pandora_handle* h, double* r, int32_t n);
 /* Particle statistics (p_StatsPrimary, src/pp_stats.f90:119-200): out[0..5] sums of
  * up_i up_j, out[6] sum of (1/2)(pi/6 dp^3 P_RHO)|up|^2.  n >= 7. */
 int pandora_particle_stats(pandora_handle* h, double* out, int32_t n);

@@ -75,6 +75,7 @@ def lib():
         L.oracle_force_calls_per_stage.restype = i64
         L.oracle_force_calls_per_stage.argtypes = [vp]
         L.oracle_realspace_sums.argtypes = [vp, dp]
+        L.oracle_x_correlation.argtypes = [vp, dp]
         _lib = L
     return _lib
 
@@ -147,6 +148,13 @@ class Oracle:
         """f_FluidstatsRs2D's raw sums and maxima of the current state (25 values)."""
         out = np.zeros(25)
         self.L.oracle_realspace_sums(self.h, _ptr(out))
+        return out
+
+    def x_correlation(self):
+        """TS_CORR's lag sums temp_r1i (NX/2 + 1 values) and lint11 (last), as the reference
+        accumulates them."""
+        out = np.zeros(self.p.nodes_x // 2 + 2)
+        self.L.oracle_x_correlation(self.h, _ptr(out))
         return out
 
     def get_forcing(self):

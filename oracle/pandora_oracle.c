@@ -908,7 +908,19 @@ static void compute_nonlinear(oracle* o, int want_cfl) {
 void oracle_realspace_sums(oracle* o, double* out) {
     dealias(o);
     cx* om[3] = {o->nl[0], o->nl[1], o->nl[2]};
-    if (o->rrot) vorticity_rrot(o, om);
+    if (o->rconv) {   /* R-conv: u4..u6 hold d(u1,u2,u3)/dx1 (src/pf_rk3.f90:422-428, 476-482, 538-544) */
+        for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
+            const double k1 = wvn((int)(ij / o->nkj), o->ki);
+            for (int k = 0; k < o->nkk; k++) {
+                const long m = ij * o->nkk + k;
+                for (int c = 0; c < 3; c++) {
+                    const cx u = o->u[c][m];
+                    om[c][m].im = k1 * u.re;
+                    om[c][m].re = -k1 * u.im;
+                }
+            }
+        }
+    } else if (o->rrot) vorticity_rrot(o, om);
     else if (o->shear) vorticity_bf(o, om);
     else vorticity_iso(o, om);
     for (int c = 0; c < 3; c++) spec_to_phys(o, o->u[c], o->phys[c]);
@@ -937,6 +949,36 @@ void oracle_realspace_sums(oracle* o, double* out) {
         const double us = fabs(u[0]) + fabs(u[1]) + fabs(u[2]);
         if (us > out[21]) out[21] = us;
     }
+}
+
+/* TS_CORR's longitudinal autocorrelation (f_FluidstatsRs2D, src/pf_fluidstats.f90:933-945)
+ * as the reference loops: per point (z slice, y, x) and ii = i .. i + (NX-1)/2 + 1,
+ * temp_r1i(ii - i) += u1 * arr_u1(ii, wrapped by NX), u1 in the laboratory frame for shear
+ * (binv(1,1) u1 + binv(1,3) u3) and arr_u1 the stored component; lint11 += the same product
+ * times dx_laboratoryframe (2 pi B110 / NX, src/pg_domain.f90:178-183).  out[0..NX/2] =
+ * temp_r1i, out[NX/2 + 1] = lint11.  The state is truncated first as at a stage's start. */
+void oracle_x_correlation(oracle* o, double* out) {
+    dealias(o);
+    spec_to_phys(o, o->u[0], o->phys[0]);
+    spec_to_phys(o, o->u[2], o->phys[2]);
+    const int nx = o->nx, nl = nx / 2 + 1;
+    const double dxl = ((double)(6.283185307179586476925286766559005768L) * (double)o->p.b110) / (double)nx;
+    for (int l = 0; l <= nl; l++) out[l] = 0.0;
+    double lint = 0.0;
+    for (long zy = 0; zy < (long)o->ny * o->nz; zy++) {
+        const double* a = o->phys[0] + zy * nx;
+        const double* a3 = o->phys[2] + zy * nx;
+        for (int i = 0; i < nx; i++) {
+            double u1 = a[i];
+            if (o->p.f_type != PANDORA_F_ISOTROPIC) u1 = (0.0 + o->binv[0][0] * a[i]) + o->binv[0][2] * a3[i];
+            for (int ii = i; ii <= i + (nx - 1) / 2 + 1; ii++) {
+                const double v = ii <= nx - 1 ? a[ii] : a[ii - nx];
+                out[ii - i] = out[ii - i] + u1 * v;
+                lint = lint + (u1 * v * dxl);
+            }
+        }
+    }
+    out[nl] = lint;
 }
 
 int oracle_nonlinear(oracle* o, double* a, double* b, double* c) {

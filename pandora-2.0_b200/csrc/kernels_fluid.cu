@@ -726,7 +726,58 @@ template <class T> cudaError_t launch_check_finite(const Geo& g, const Member<T>
 
 #undef PD_CAP
 
+// TS_CORR's longitudinal autocorrelation (f_FluidstatsRs2D, src/pf_fluidstats.f90:933-945)
+// in wave space.  The sum over the grid of a(x) b(x + l dx) is N^3 sum_k a^(k) conj(b^(k))
+// e^{-2 pi i m l / NX} over the full spectrum, so per x wavenumber m the co-spectrum
+// P_m = sum_{j,k} a^ conj(b^) of a = u1 in the laboratory frame (binv u for shear, as
+// the reference's real-space statistics take it) and b = the stored u1 carries all of
+// it; the modes DEALIASING 2/3 drops are left out, as the real-space field holds none.
+// One CTA per m plane with a fixed-order block sum: P[2m], P[2m+1] = Re, Im.
+template <class T>
+__global__ void __launch_bounds__(256) k_xcorr_cospec(const __grid_constant__ MemberSet<T, 1> ms, double* P) {
+    const FieldsT<T> F = ms.m[0].F;
+    const Geo g = ms.m[0].g;
+    const BF bf = make_bf(g, F.clock);
+    const bool dealias = g.dealias_cut > 0.0;
+    const int i = blockIdx.x;
+    const long long plane = (long long)g.nkj * g.nkk, base = (long long)i * plane;
+    double re = 0.0, im = 0.0;
+    for (long long q = threadIdx.x; q < plane; q += blockDim.x) {
+        const int j = (int)(q / g.nkk), k = (int)(q % g.nkk);
+        if (dealias && dealias_drop(g, bf, (double)i, wvn(j, g.kj), wvn(k, g.kk))) continue;
+        const double2 b = to_d(F.u[0][base + q]);
+        double2 a = b;
+        if (g.shear) {
+            const double2 u3 = to_d(F.u[2][base + q]);
+            a = make_double2(bf.bi[0][0] * b.x + bf.bi[0][2] * u3.x, bf.bi[0][0] * b.y + bf.bi[0][2] * u3.y);
+        }
+        re += a.x * b.x + a.y * b.y;
+        im += a.y * b.x - a.x * b.y;
+    }
+    __shared__ double sr[8], si[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sr[threadIdx.x >> 5] = re; si[threadIdx.x >> 5] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tr = 0.0, ti = 0.0;
+        for (int w = 0; w < 8; w++) { tr += sr[w]; ti += si[w]; }
+        P[2 * i] = tr;
+        P[2 * i + 1] = ti;
+    }
+}
+
+template <class T> cudaError_t launch_xcorr_cospec(const Member<T>& m, double* P, cudaStream_t st) {
+    MemberSet<T, 1> one;
+    one.m[0] = m;
+    k_xcorr_cospec<T><<<(unsigned)m.g.nki, 256, 0, st>>>(one, P);
+    return cudaGetLastError();
+}
+
 #define PD_INST(T)                                                                                   \
+    template cudaError_t launch_xcorr_cospec<T>(const Member<T>&, double*, cudaStream_t);            \
     template cudaError_t launch_stats<T>(const Geo&, const Member<T>*, int, double*, cudaStream_t);  \
     template cudaError_t launch_stage_scalars<T>(const Geo&, const Member<T>*, int, const ForceParams&, int, \
                                                  cudaStream_t);                                      \

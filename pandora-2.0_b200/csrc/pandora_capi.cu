@@ -10,6 +10,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <cmath>
 #include <new>
 #include <vector>
 #include "pandora_internal.cuh"
@@ -902,8 +903,8 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
 // f_FluidstatsRsCollect does (src/pf_fluidstats.f90:960-1100).
 extern "C" int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n) {
     if (!h || !out || n < 25) return PANDORA_ERR_INVALID_ARG;
-    // the R-conv form transforms velocity gradients, not a vorticity, to real space
-    if (h->g.rconv) return PANDORA_ERR_UNSUPPORTED;
+    // R-conv: the reference's u4..u6 in real space are d(u1,u2,u3)/dx1 (src/pf_rk3.f90:422-428,
+    // 476-482, 538-544), and its vorticity moments are taken of those; so are these
     cudaSetDevice(h->dev);
     const size_t words = 32 * 32;
     if (!h->rsbuf) {
@@ -928,6 +929,37 @@ extern "C" int pandora_realspace_stats(pandora_handle* h, double* out, int32_t n
     for (int slot = 0; slot < 32; slot++) {
         for (int a = 0; a < 21; a++) out[a] += hb[(size_t)slot * 32 + a];
         for (int a = 21; a < 25; a++) out[a] = std::max(out[a], hb[(size_t)slot * 32 + a]);
+    }
+    return PANDORA_OK;
+}
+
+// TS_CORR's longitudinal autocorrelation (f_FluidstatsRs2D, src/pf_fluidstats.f90:933-945):
+// r[l] = sum over the grid of u1(x) u1(x + l dx), l = 0..NX/2, with u1(x) in the laboratory
+// frame for shear and u1(x + l dx) the stored component (the reference's temp_r1i before
+// f_FluidstatsRsCollect divides it).  From the x co-spectrum P_m of the current state:
+// r[l] = NX NY NZ sum_m c_m Re(P_m e^{-2 pi i m l / NX}), c_0 = 1, c_m = 2 (the -m half).
+extern "C" int pandora_x_correlation(pandora_handle* h, double* r, int32_t n) {
+    if (!h || !r) return PANDORA_ERR_INVALID_ARG;
+    const int nx = h->g.nx, nl = nx / 2 + 1, nki = h->g.nki;
+    if (n < nl) return PANDORA_ERR_INVALID_ARG;
+    cudaSetDevice(h->dev);
+    if (!h->rsbuf) {   // 1024 words: 2 NKI <= 684 for NX <= 1024
+        if (cudaMalloc((void**)&h->rsbuf, sizeof(double) * 32 * 32) != cudaSuccess) { cudaGetLastError(); return PANDORA_ERR_OOM; }
+    }
+    if (h->mixed) PD_CK(launch_xcorr_cospec(self_of<float>(h), h->rsbuf, h->st));
+    else PD_CK(launch_xcorr_cospec(self_of<double>(h), h->rsbuf, h->st));
+    std::vector<double> P((size_t)2 * nki);
+    PD_CK(cudaMemcpyAsync(P.data(), h->rsbuf, sizeof(double) * 2 * nki, cudaMemcpyDeviceToHost, h->st));
+    PD_CK(cudaStreamSynchronize(h->st));
+    const double npts = (double)h->g.R, w = 6.283185307179586476925286766559005768 / (double)nx;
+    for (int l = 0; l < nl; l++) {
+        double acc = 0.0;
+        for (int m = 0; m < nki; m++) {
+            const double th = w * (double)(((long long)m * l) % nx);   // the phase reduced exactly
+            const double t = P[2 * m] * std::cos(th) + P[2 * m + 1] * std::sin(th);
+            acc += m == 0 ? t : 2.0 * t;
+        }
+        r[l] = npts * acc;
     }
     return PANDORA_OK;
 }

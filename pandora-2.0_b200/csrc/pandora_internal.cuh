@@ -245,6 +245,8 @@ cudaError_t launch_particle_stats(const Particles& p, long long np, double rho_p
 // DEALIASING 2/3 applied to the members' state in place (no-op for the 2/3 rule)
 template <class T>
 cudaError_t launch_dealias(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
+// P[2m], P[2m+1] (m = 0..NKI-1): the x co-spectrum of u1 (laboratory) and u1 (stored)
+template <class T> cudaError_t launch_xcorr_cospec(const Member<T>& m, double* P, cudaStream_t st);
 // Per simulation (not batched): initial field (generated in FP64; the FP32-mixed
 // form converts it), particle initialisation and the per-step spatial sort.
 cudaError_t launch_init_fluid(const Geo& g, const Fields& f, const InitParams& ip, cudaStream_t st);

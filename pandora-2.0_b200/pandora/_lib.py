@@ -69,6 +69,7 @@ SIGNATURES = {
     "pandora_last_step_stats": [_vp, _dp, _i32, _dp, _dp, _dp],
     "pandora_nonlinear": [_vp, _dp, _dp, _dp],
     "pandora_realspace_stats": [_vp, _dp, _i32],
+    "pandora_x_correlation": [_vp, _dp, _i32],
     "pandora_particle_stats": [_vp, _dp, _i32],
     "pandora_get_physical_velocity": [_vp, _dp, _dp, _dp],
     "pandora_check_status": [_vp],

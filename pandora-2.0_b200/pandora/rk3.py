@@ -56,7 +56,19 @@ def realspace_normalise(raw, p) -> dict:
     r["ucfl"] = raw[21]
     for c in range(3):
         r[f"omegamax{c + 1}"] = raw[22 + c]
+    r["lint11"] = 0.0   # without the correlation (TS_CORR > TSTEPS), src/pf_fluidstats.f90:1104-1105
     return r
+
+
+def correlation_normalise(rsum, u1u1, p) -> dict:
+    """f_FluidstatsRsCollect's finish of TS_CORR (src/pf_fluidstats.f90:1092-1105): r1i =
+    temp_r1i / (rs_u1u1 N^3) at the lags l dx_laboratoryframe, l = 0..NX/2, and rs_lint11 =
+    sum_l temp_r1i(l) dx_laboratoryframe / (rs_u1u1 N^3); ``u1u1`` is the normalised rs_u1u1."""
+    npts = float(p.nodes_x) * float(p.nodes_y) * float(p.nodes_z)
+    dxl = 2.0 * np.pi * float(p.b110) / float(p.nodes_x)
+    rsum = np.asarray(rsum, dtype=np.float64)
+    return {"r": np.arange(rsum.size) * dxl, "r1i": rsum / (u1u1 * npts),
+            "lint11": float(np.sum(rsum * dxl)) / (u1u1 * npts)}
 
 
 class Simulation:
@@ -220,11 +232,22 @@ class Simulation:
         _lib.check(self.L.pandora_realspace_stats(self.h, _dp(out), 25), "pandora_realspace_stats")
         return out
 
-    def realspace_stats(self) -> dict:
+    def realspace_stats(self, corr: bool = False) -> dict:
         """f_FluidstatsRs2D + f_FluidstatsRsCollect (src/pf_fluidstats.f90:827-1100) of the
         current state, normalised as the reference does (its rmsvort1 is not divided
-        by the number of points, src/pf_fluidstats.f90:1057; that is kept)."""
-        return realspace_normalise(self.realspace_sums(), self.p)
+        by the number of points, src/pf_fluidstats.f90:1057; that is kept).  With
+        ``corr`` (a TS_CORR step) also the longitudinal autocorrelation ``r1i`` at the lags
+        ``r`` and the integral length ``lint11``."""
+        r = realspace_normalise(self.realspace_sums(), self.p)
+        if corr:
+            r.update(correlation_normalise(self.x_correlation_sums(), r["u1u1"], self.p))
+        return r
+
+    def x_correlation_sums(self) -> np.ndarray:
+        """Raw lag sums of `pandora_x_correlation` (NX/2 + 1 values)."""
+        out = np.zeros(self.p.nodes_x // 2 + 1)
+        _lib.check(self.L.pandora_x_correlation(self.h, _dp(out), out.size), "pandora_x_correlation")
+        return out
 
     def particle_stats(self) -> dict:
         """p_StatsPrimary (src/pp_stats.f90:119-200): particle velocity moments / NP and

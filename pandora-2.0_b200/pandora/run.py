@@ -3,13 +3,20 @@ simulation (create, seed, advance, statistics), for profiling a kernel on a case
 smaller than the benchmark's.
 
     python -m pandora.run --workload shear --nodes 512 128 128 --steps 3
+    python -m pandora.run --workload shear --nodes 512 512 512 --form r-conv --pass-times
+
+``--form`` picks the shear formulation (NS_DEFORMED); ``--pass-times`` times every
+pass of the last step with CUDA event pairs and prints them (ms, stage x pass).
 """
 from __future__ import annotations
 
 import argparse
 import sys
 
-from .params import PREC_FP32_MIXED, PREC_FP64, workload_params
+from .params import NS_BF_ROT, NS_R_CONV, NS_R_ROT, PREC_FP32_MIXED, PREC_FP64, workload_params
+
+FORMS = {"bf-rot": NS_BF_ROT, "r-conv": NS_R_CONV, "r-rot": NS_R_ROT}
+PASSES = ("zpass_inv", "ypass_inv", "xpass", "ypass_fwd", "zpass_fwd", "rk_update")
 from .rk3 import Simulation
 
 
@@ -20,16 +27,32 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--np", type=int, default=0, help="tracers (0: none)")
     ap.add_argument("--precision", choices=["fp64", "fp32_mixed"], default="fp64")
+    ap.add_argument("--form", choices=sorted(FORMS), default="bf-rot", help="shear formulation")
+    ap.add_argument("--pass-times", action="store_true", help="time each pass of the last step")
     a = ap.parse_args(argv)
     p = workload_params(a.workload, a.nodes[0])
     p.nodes_x, p.nodes_y, p.nodes_z = a.nodes
     p.p_track_part, p.p_np_global = (1, a.np) if a.np > 0 else (0, 0)
     p.precision = PREC_FP32_MIXED if a.precision == "fp32_mixed" else PREC_FP64
+    p.ns_deformed = FORMS[a.form]
     with Simulation(p) as s:
         s.init_fluid()
         if a.np > 0:
             s.init_particles()
-        s.advance(a.steps)
+        if a.pass_times and a.steps > 1:
+            s.advance(a.steps - 1)
+        if a.pass_times:
+            s.set_pass_timing(0x3F)
+            s.advance(1)
+            t = s.pass_times()
+            s.set_pass_timing(0)
+            for name, col in zip(PASSES, t.T):   # -1: not run on its own (K5b inside K5a's pair)
+                if (col < 0).all():
+                    continue
+                print(f"{name:10s} " + " ".join(f"{v:8.3f}" for v in col) + f"   sum {col[col > 0].sum():8.3f} ms")
+            print(f"step (sum of passes) {t[t > 0].sum():.3f} ms")
+        else:
+            s.advance(a.steps)
         ek, tke, eps, _ = s.stats()
         s.check_status()
     print(f"{a.workload} {a.nodes[0]}x{a.nodes[1]}x{a.nodes[2]} {a.precision}: {a.steps} steps, tke {tke:.6e}, eps {eps:.6e}")

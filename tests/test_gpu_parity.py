@@ -359,12 +359,16 @@ def test_dealias_parity(gpu_lib, mode, cut):
         assert rel_l2_fields(s.nonlinear(), o.nonlinear()) < 1e-12
 
 
-@pytest.mark.parametrize("workload", ["iso_decay", "shear"])
+@pytest.mark.parametrize("workload", ["iso_decay", "shear", "shear_rconv"])
 def test_realspace_stats_parity(gpu_lib, workload):
-    """Real-space moments and maxima (f_FluidstatsRs2D) of the same state on both sides."""
+    """Real-space moments and maxima (f_FluidstatsRs2D) of the same state on both sides;
+    in the R-conv form the "vorticity" moments are those of d(u1,u2,u3)/dx1, the fields
+    the reference holds in u4..u6 there."""
     import oracle as O
-    p = gpu_lib.workload_params(workload, 32)
+    p = gpu_lib.workload_params("shear" if workload == "shear_rconv" else workload, 32)
     p.p_track_part = 0
+    if workload == "shear_rconv":
+        p.ns_deformed = gpu_lib.NS_R_CONV
     o, s = _pair(gpu_lib, p)
     t = 0.0
     for step in range(1, 4):
@@ -392,4 +396,40 @@ def test_particle_stats(gpu_lib):
     assert d["u2u3"] == pytest.approx((up[:, 1] * up[:, 2]).sum() / n, rel=1e-12, abs=1e-15)
     pken = (0.5 * (np.pi / 6.0) * dp ** 3 * 1000.0 * (up ** 2).sum(axis=1)).sum() / n
     assert pken > 0.0 and d["pken"] == pytest.approx(pken, rel=1e-12)
+
+
+@pytest.mark.parametrize("case", ["iso", "aniso", "shear", "shear_sphere", "fp32"])
+def test_x_correlation_parity(gpu_lib, case):
+    """TS_CORR's lag sums (src/pf_fluidstats.f90:933-945): the GPU's co-spectrum form
+    against the oracle's lag loop on the same state, after a few steps (shear: a frame with
+    binv(1,3) != 0; shear_sphere: DEALIASING 2, the dropped modes left out)."""
+    import oracle as O
+    wl = "shear" if case.startswith("shear") else "iso_decay"
+    p = gpu_lib.workload_params(wl, 32)
+    p.p_track_part = 0
+    if case == "aniso":
+        p.nodes_x, p.nodes_y, p.nodes_z = 48, 32, 24
+    if case == "shear_sphere":
+        p.dealiasing = 2
+    if case == "fp32":
+        p.precision = gpu_lib.PREC_FP32_MIXED
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    s.advance(3)
+    q = p.copy()
+    q.precision = gpu_lib.PREC_FP64
+    o = O.Oracle(q)
+    o.set_state(s.get_state())
+    if wl == "shear":
+        o.update_b(4, s.simtime)
+        assert o.frame() == pytest.approx(s.frame(), rel=1e-14)
+    g = s.x_correlation_sums()
+    want = o.x_correlation()[:-1]
+    tol = 1e-5 if case == "fp32" else 1e-12
+    assert np.abs(g - want).max() < tol * abs(want[0]), np.abs(g - want).max() / abs(want[0])
+    d = s.realspace_stats(corr=True)
+    assert d["r1i"].size == p.nodes_x // 2 + 1 and d["lint11"] != 0.0
+    if wl != "shear":    # lag 0 is u1u1 itself (for shear a product of laboratory and stored u1)
+        assert d["r1i"][0] == pytest.approx(1.0, rel=1e-6 if case == "fp32" else 1e-12)
+    s.close()
 

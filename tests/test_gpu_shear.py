@@ -122,15 +122,10 @@ def test_rogallo_with_particles_unsupported(gpu_lib, form):
         gpu_lib.Simulation(p)
 
 
-def test_rconv_limits(gpu_lib):
-    """R-conv: no real-space vorticity statistics (its real-space fields are gradients)
-    and single simulations only (no batched x pass)."""
+def test_rconv_single_simulations_only(gpu_lib):
+    """R-conv has no batched x pass: a batch of R-conv members is refused."""
     p = _shear(gpu_lib, 32, remesh_t=5)
     p.ns_deformed = gpu_lib.NS_R_CONV
-    with gpu_lib.Simulation(p) as s:
-        s.init_fluid()
-        with pytest.raises(gpu_lib.PandoraError):
-            s.realspace_stats()
     with pytest.raises(gpu_lib.PandoraError):
         gpu_lib.Batch(p, 2)
 

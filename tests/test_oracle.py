@@ -286,3 +286,45 @@ def test_realspace_sums_parseval(workload):
     assert 0.5 * (r["u1u1"] + r["u2u2"] + r["u3u3"]) == pytest.approx(tke, rel=1e-12)
     assert 2.0 < r["flat1"] < 4.5 and abs(r["skew2"]) < 1.0
 
+
+
+def _cospectrum_correlation(p, u, bi13):
+    """r[l] = N^3 sum_m c_m Re(P_m e^{-2 pi i m l / NX}) with P_m = sum_{j,k} a conj(b),
+    a = u1 in the laboratory frame, b = the stored u1: the wave-space form of the lag sums."""
+    b = u[0]
+    a = b if p.f_type == 1 else float(p.b110) * u[0] + bi13 * u[2]
+    P = np.sum(a * np.conj(b), axis=(1, 2))
+    m = np.arange(P.size)
+    c = np.where(m == 0, 1.0, 2.0)
+    lags = np.arange(p.nodes_x // 2 + 1)
+    ph = np.exp(-2j * np.pi * np.outer(lags, m) / p.nodes_x)
+    return float(p.nodes_x * p.nodes_y * p.nodes_z) * np.real(ph @ (c * P))
+
+
+@pytest.mark.parametrize("workload,dims", [("iso_decay", (32, 32, 32)), ("iso_decay", (48, 32, 24)),
+                                           ("shear", (32, 32, 32))])
+def test_x_correlation_lag_loop_and_cospectrum(workload, dims):
+    """TS_CORR (src/pf_fluidstats.f90:933-945): the oracle's lag loop, as the reference runs
+    it, equals the co-spectrum form the GPU evaluates; lag 0 is the u1 second moment
+    (exactly, for isotropic flow) and lint11 is the lags' sum times dx_laboratoryframe."""
+    from pandora.params import workload_params
+    from pandora.rk3 import correlation_normalise, realspace_normalise
+    p = workload_params(workload, dims[0])
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    p.p_track_part = 0
+    o = _o(p)
+    o.init_fluid()
+    if workload == "shear":
+        o.update_b(5, 0.3)            # a frame with binv(1,3) != 0
+    out = o.x_correlation()
+    r, lint = out[:-1], out[-1]
+    want = _cospectrum_correlation(p, o.get_state(), o.frame()[1])
+    assert np.abs(r - want).max() < 1e-12 * abs(r[0])
+    rs = realspace_normalise(o.realspace_sums(), p)
+    if workload == "iso_decay":
+        assert r[0] == o.realspace_sums()[0]
+    cn = correlation_normalise(r, rs["u1u1"], p)
+    assert cn["lint11"] == pytest.approx(lint / (rs["u1u1"] * np.prod(dims)), rel=1e-12)
+    if workload == "iso_decay":
+        assert cn["r1i"][0] == pytest.approx(1.0, rel=1e-14)
+        assert np.all(np.abs(cn["r1i"]) <= 1.0 + 1e-12)
