@@ -615,15 +615,19 @@ template <int N, bool TWO = false> struct TCfg {
 // K1: spectral velocity and vorticity, backward z transforms.  Field f =
 // blockIdx.x: 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
 // f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
-// f_RK3Derivative 3735-3743), or the BF-rot vorticity; the tile's lines from i0 at one j;
+// f_RK3Derivative 3735-3743), or the BF-rot or R-rot vorticity, or (R-conv, twelve fields)
+// the nine gradients i k_d u_c; the tile's lines from i0 at one j;
 // k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
 // of a tile are adjacent in launch order, so the three that read a velocity
-// component run together and two of the three reads hit L2.
-template <int NZ, bool SHEAR, class T, int CAP>
+// component run together and two of the three reads hit L2.  FORM (compile time, so
+// that each instantiation carries only its own derivative code): 0 isotropic, 1 BF-rot,
+// 2 R-rot, 3 R-conv.
+template <int NZ, int FORM, class T, int CAP>
 __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
                                                                                                    long long pf_ctas) {
     using C = typename FieldsT<T>::C;
-    const int nf = CAP == 1 ? pass_fields(ms.m[0].g) : 6;   // batches: no R-conv members
+    constexpr bool SHEAR = FORM != 0;
+    constexpr int nf = FORM == 3 ? 12 : 6;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / nf];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
@@ -644,20 +648,16 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
     // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1).  R-conv: field 3 + 3d + c
     // is d u_c / d x_d.
-    const bool rconv = SHEAR && g.rconv;
-    C* const pa = (rconv && f >= 3) ? F.u[(f - 3) % 3]
-                : ((f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]));
+    // (selects, not an index into F.u: a computed index would move F to local memory)
+    constexpr bool rconv = FORM == 3;
+    const int fc = rconv ? (f >= 3 ? (f - 3) % 3 : f) : -1;
+    const C* const pa = rconv ? (fc == 0 ? F.u[0] : (fc == 1 ? F.u[1] : F.u[2]))
+                              : ((f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]));
     const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
     BFT<T> bf;
     if constexpr (SHEAR) {
         if (f >= 3) bf = bf_as<T>(make_bf(g, F.clock));
     }
-    // DEALIASING 2/3: f_RK3PrepareRealSpace first zeroes the modes outside the cutoff
-    // (src/pf_rk3.f90:269-277); each velocity CTA clears its component's dropped modes
-    // in u as it reads them, every CTA reads them as zero
-    const bool dealias = g.dealias_cut > 0.0;
-    BF bfd;
-    if (dealias) bfd = make_bf(g, F.clock);
     auto ld = [&](int z, int l) -> C {
         const int i = i0 + l;
         int k;
@@ -666,25 +666,20 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
         else return mk(T(0), T(0));
         if (i >= nki) return mk(T(0), T(0));
         const long long m = row0 + l * istride + k;
-        if (dealias && dealias_drop(g, bfd, (double)i, k2, wvn(k, KK))) {
-            if (f < 3) pa[m] = mk(T(0), T(0));
-            return mk(T(0), T(0));
-        }
         if (f < 3) return pa[m];
-        if constexpr (SHEAR) {
-            if (rconv) {   // f_RK3Derivative (src/pf_rk3.f90:3735-3743): i k_d u_c, plain k_d
-                const int d = (f - 3) / 3;
-                const T kd = d == 0 ? (T)i : (d == 1 ? k2t : (T)wvn(k, KK));
-                const C uc = pa[m];
-                return mk(-kd * uc.y, kd * uc.x);
-            }
-            // BF-rot vorticity (f_RK3VorticityBFRot), in T
+        if constexpr (FORM == 3) {   // f_RK3Derivative (src/pf_rk3.f90:3735-3743): i k_d u_c, plain k_d
+            const int d = (f - 3) / 3;
+            const T kd = d == 0 ? (T)i : (d == 1 ? k2t : (T)wvn(k, KK));
+            const C uc = pa[m];
+            return mk(-kd * uc.y, kd * uc.x);
+        } else if constexpr (SHEAR) {
+            // BF-rot vorticity (f_RK3VorticityBFRot) or the R-rot sheared curl, in T
             const T kv[3] = {(T)i, k2t, (T)wvn(k, KK)};
             const C zero = mk(T(0), T(0));
             // omega1 has no term in u1 and omega2 none in u2: those loads are skipped
             const C uv[3] = {f != 3 ? F.u[0][m] : zero, f != 4 ? F.u[1][m] : zero, F.u[2][m]};
             C w3[3];
-            if (g.rrot) vort_rrot(bf, uv, kv, w3);   // R-rot: sheared curl of laboratory components
+            if constexpr (FORM == 2) vort_rrot(bf, uv, kv, w3);
             else vort_bf(bf, uv, kv, w3);
             return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
         } else {
@@ -709,7 +704,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     const C* const u1 = F.u[1];
     const C* const u2 = F.u[2];
     const int nkj = g.nkj;
-    auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2, nf, rconv]() {
+    auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2]() {
         if (pf_ctas <= 0) return;
         const long long nblk = (long long)nf * gridDim.y * gridDim.z;
         const long long nxt = blockIdx.x + (long long)nf * (blockIdx.y + (long long)gridDim.y * blockIdx.z) + pf_ctas;
@@ -860,8 +855,12 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
     cudaError_t e = cudaSuccess;
 #define PD_CFG1(N, CAP)                                                                        \
     if (g.nz == N) {                                                                           \
-        if ((e = set_smem(k_zpass_inv<N, false, T, CAP>, TCfg<N>::template smem<T>()))) return e; \
-        if ((e = set_smem(k_zpass_inv<N, true, T, CAP>, TCfg<N>::template smem<T>()))) return e;  \
+        if ((e = set_smem(k_zpass_inv<N, 0, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
+        if ((e = set_smem(k_zpass_inv<N, 1, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
+        if ((e = set_smem(k_zpass_inv<N, 2, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
+        if constexpr (CAP == 1) {                                                              \
+            if ((e = set_smem(k_zpass_inv<N, 3, T, CAP>, TCfg<N>::template smem<T>()))) return e; \
+        }                                                                                      \
         if ((e = set_smem(k_zpass_fwd<N, T, CAP>, TCfg<N, true>::template smem<T>()))) return e;        \
     }                                                                                          \
     if (g.ny == N) {                                                                           \
@@ -890,6 +889,13 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
 
 template <class T>
 cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st) {
+    // DEALIASING 2/3: f_RK3PrepareRealSpace first zeroes the modes outside the cutoff
+    // (src/pf_rk3.f90:269-277): k_dealias writes those zeros (it reads nothing) ahead of
+    // K1, whose loads then carry no mask test
+    if (g.dealias_cut > 0.0) {
+        const cudaError_t e = launch_dealias(g, M, B, st);
+        if (e != cudaSuccess) return e;
+    }
     switch (g.nz) {
 #define PD_L(N)                                                                                   \
     case N:                                                                                       \
@@ -899,13 +905,14 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
                 const dim3 grid(pass_fields(g) * nb, TCfg<N>::template tiles<T>(g), g.nkj);                          \
                 constexpr int NT = TCfg<N>::template nt<T>();                                      \
                 const size_t sm = TCfg<N>::template smem<T>();                                     \
-                if (g.shear) {                                                                    \
-                    const long long pf = CAP == 1 ? resident_ctas(k_zpass_inv<N, true, T, CAP>, NT, sm) : 0; \
-                    k_zpass_inv<N, true, T, CAP><<<grid, NT, sm, st>>>(ms, stage, pf);            \
-                } else {                                                                          \
-                    const long long pf = CAP == 1 ? resident_ctas(k_zpass_inv<N, false, T, CAP>, NT, sm) : 0; \
-                    k_zpass_inv<N, false, T, CAP><<<grid, NT, sm, st>>>(ms, stage, pf);           \
-                }                                                                                 \
+                auto go = [&](auto kern) {                                                        \
+                    const long long pf = CAP == 1 ? resident_ctas(kern, NT, sm) : 0;              \
+                    kern<<<grid, NT, sm, st>>>(ms, stage, pf);                                    \
+                };                                                                                \
+                if (!g.shear) go(k_zpass_inv<N, 0, T, CAP>);                                      \
+                else if (!g.rrot) go(k_zpass_inv<N, 1, T, CAP>);                                  \
+                else if (!g.rconv) go(k_zpass_inv<N, 2, T, CAP>);                                 \
+                else if constexpr (CAP == 1) go(k_zpass_inv<N, 3, T, CAP>);                       \
             }                                                                                     \
         });
         PD_FOR_EACH_N(PD_L)

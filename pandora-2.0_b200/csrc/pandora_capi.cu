@@ -654,7 +654,7 @@ template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, 
         return cudaEventRecordWithFlags(h->tev[stage - 1][ps - 1][end], s, cudaEventRecordExternal);
     };
     PD_CK(mark(1, 0, c.st));
-    PD_CK(launch_zpass_inv(g, M, B, stage, c.st)); n++;
+    PD_CK(launch_zpass_inv(g, M, B, stage, c.st)); n += g.dealias_cut > 0.0 ? 2 : 1;   // k_dealias first
     PD_CK(mark(1, 1, c.st));
     PD_CK(mark(2, 0, c.st));
     PD_CK(launch_ypass_inv(g, M, B, c.st)); n++;
