@@ -191,6 +191,15 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
                 if (i0 + it < ITM && m < NKI) {
 #pragma unroll
                     for (int c = 0; c < 6; c++) X[it][c] = b[c * fstride + m];
+                    if constexpr (RS) {
+                        // R-conv: the reference's u4..u6 are d(u1,u2,u3)/dx1 (src/pf_rk3.f90:
+                        // 422-428), i m times the u rows
+                        if (g.rconv) {
+                            const T km = (T)m;
+#pragma unroll
+                            for (int c = 3; c < 6; c++) X[it][c] = mk(-km * X[it][c - 3].y, km * X[it][c - 3].x);
+                        }
+                    }
                 }
             }
 #pragma unroll
@@ -323,8 +332,9 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
 }
 
 // ---------------------------------------------------------------------------
-// K3 of the R-conv form (NS_DEFORMED = NS_R_CONV): the x pass of the twelve fields
-// u1..u3 and d u_c / d x_d (yb field 3 + 3d + c), then f_RK3ComputeNonlinearRConv
+// K3 of the R-conv form (NS_DEFORMED = NS_R_CONV): the x pass of the twelve fields u1..u3
+// and d u_c / d x_d, from the nine rows u, d u / dy, d u / dz of yb (d u_c / dx is i m times
+// the x spectrum of u_c, formed here), then f_RK3ComputeNonlinearRConv
 // (src/pf_rk3.f90:1717-1774), NL_i = sum_d v_d d u_i / d x_d with v_d = sum_j
 // bmat(d,j) u_j, then the forward transforms and split of K3.  One warp per line
 // over four arrays: the pairs (u1,u2) and (u3, du1/dx1) first; v and the partial sums
@@ -360,10 +370,14 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
     const int NKI = g.nki;
     C* b = F.yb + q * g.nkip;
     const BFT<T> bf = bf_as<T>(make_bf(g, F.clock));
-    // the Hermitian extension of the half spectra of fields fa and fb into array p, as K3
-    auto build = [&](int p, int fa, int fb) {
+    // the Hermitian extension of the half spectra of fields fa and fb into array p, as K3;
+    // xa, xb: i m times the field (its x derivative)
+    auto build = [&](int p, int fa, bool xa, int fb, bool xb) {
         for (int m = lane; m < NKI; m += 32) {
             C X = b[fa * fstride + m], Y = b[fb * fstride + m];
+            const T km = (T)m;
+            if (xa) X = mk(-km * X.y, km * X.x);
+            if (xb) Y = mk(-km * Y.y, km * Y.x);
             if (m == 0) { X.y = T(0); Y.y = T(0); }
             s[p * XAS + prow<XPS>(m)] = mk(X.x - Y.y, X.y + Y.x);
             if (m > 0) s[p * XAS + prow<XPS>(NX - m)] = mk(X.x + Y.y, -X.y + Y.x);
@@ -376,8 +390,8 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         else { bwd1(a); bwd1(a + XAS); }
     };
     // (u1,u2), (u3, du1/dx1) -> v = bmat u, NL1 = v1 du1/dx1; arrays 0, 1 = (v1,v2), (v3,NL1)
-    build(0, 0, 1);
-    build(1, 2, 3);
+    build(0, 0, false, 1, false);
+    build(1, 2, false, 0, true);
     bwd2(s);
     T umax = T(0);
     for (int n = lane; n < NX; n += 32) {
@@ -397,8 +411,8 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         e[XAS] = mk(v[2], v[0] * c1.y);
     }
     // (du2/dx1, du3/dx1), (du1/dx2, du2/dx2); arrays 0..2 = (v2,v3), (NL1,NL2), (NL3,-)
-    build(2, 4, 5);
-    build(3, 6, 7);
+    build(2, 1, true, 2, true);
+    build(3, 3, false, 4, false);
     bwd2(s + 2 * XAS);
     for (int n = lane; n < NX; n += 32) {
         C* e = s + prow<XPS>(n);
@@ -412,7 +426,7 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         e[2 * XAS] = mk(n3, T(0));
     }
     // (du3/dx2, du1/dx3)
-    build(3, 8, 9);
+    build(3, 5, false, 6, false);
     bwd1(s + 3 * XAS);
     for (int n = lane; n < NX; n += 32) {
         C* e = s + prow<XPS>(n);
@@ -421,7 +435,7 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         e[2 * XAS] = mk(c2.x + a.x * g1.x, T(0));
     }
     // (du2/dx3, du3/dx3); arrays 0, 1 = (NL1,NL2), (NL3,0) for the forward transforms
-    build(3, 10, 11);
+    build(3, 7, false, 8, false);
     bwd1(s + 3 * XAS);
     for (int n = lane; n < NX; n += 32) {
         C* e = s + prow<XPS>(n);
@@ -435,7 +449,7 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
         if (threadIdx.x % 32 == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
     }
-    if (pf_lines > 0 && q + pf_lines < lines && lane < 12)
+    if (pf_lines > 0 && q + pf_lines < lines && lane < 9)
         prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
     if constexpr (NA == 2) {
         pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
@@ -615,8 +629,8 @@ template <int N, bool TWO = false> struct TCfg {
 // K1: spectral velocity and vorticity, backward z transforms.  Field f =
 // blockIdx.x: 0..2 velocity, 3..5 vorticity omega = i k x u, isotropic branch of
 // f_RK3PrepareVelocity (src/pf_rk3.f90:402-407,520-525,630-634, derivative
-// f_RK3Derivative 3735-3743), or the BF-rot or R-rot vorticity, or (R-conv, twelve fields)
-// the nine gradients i k_d u_c; the tile's lines from i0 at one j;
+// f_RK3Derivative 3735-3743), or the BF-rot or R-rot vorticity, or (R-conv) the z
+// derivatives i k3 u_c; the tile's lines from i0 at one j;
 // k is zero-padded into [KK+1, NZ-KK-1] as src/pf_rk3.f90:437-443.  The six CTAs
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.  FORM (compile time, so
@@ -627,7 +641,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
                                                                                                    long long pf_ctas) {
     using C = typename FieldsT<T>::C;
     constexpr bool SHEAR = FORM != 0;
-    constexpr int nf = FORM == 3 ? 12 : 6;
+    constexpr int nf = FORM == 3 ? 9 : 6;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.x / nf];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
@@ -646,11 +660,11 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     const long long istride = (long long)g.nkj * NKK;
     const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
-    // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1).  R-conv: field 3 + 3d + c
-    // is d u_c / d x_d.
+    // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1).  R-conv: fields 3 + c and
+    // 6 + c are d u_c / dy and d u_c / dz (d u_c / dx is formed in the x pass).
     // (selects, not an index into F.u: a computed index would move F to local memory)
     constexpr bool rconv = FORM == 3;
-    const int fc = rconv ? (f >= 3 ? (f - 3) % 3 : f) : -1;
+    const int fc = rconv ? f % 3 : -1;
     const C* const pa = rconv ? (fc == 0 ? F.u[0] : (fc == 1 ? F.u[1] : F.u[2]))
                               : ((f == 0 || f == 4) ? F.u[0] : ((f == 1 || f == 5) ? F.u[1] : F.u[2]));
     const C* pb = (f == 3) ? F.u[1] : ((f == 4) ? F.u[2] : F.u[0]);
@@ -667,9 +681,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
         if (i >= nki) return mk(T(0), T(0));
         const long long m = row0 + l * istride + k;
         if (f < 3) return pa[m];
-        if constexpr (FORM == 3) {   // f_RK3Derivative (src/pf_rk3.f90:3735-3743): i k_d u_c, plain k_d
-            const int d = (f - 3) / 3;
-            const T kd = d == 0 ? (T)i : (d == 1 ? k2t : (T)wvn(k, KK));
+        if constexpr (FORM == 3) {   // f_RK3Derivative (src/pf_rk3.f90:3735-3743): i k2 u_c or i k3 u_c
+            const T kd = f < 6 ? k2t : (T)wvn(k, KK);
             const C uc = pa[m];
             return mk(-kd * uc.y, kd * uc.x);
         } else if constexpr (SHEAR) {
@@ -712,7 +725,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
         const int f2 = (int)(nxt % nf), ti = (int)((nxt / nf) % gridDim.y), j2 = (int)(nxt / ((long long)nf * gridDim.y));
         const int nc = (f2 < 3 || rconv) ? 1 : 3, t = threadIdx.x;
         if (t >= LT * nc) return;
-        const int c = f2 < 3 ? f2 : (rconv ? (f2 - 3) % 3 : t / LT), i = ti * LT + t % LT;
+        const int c = f2 < 3 ? f2 : (rconv ? f2 % 3 : t / LT), i = ti * LT + t % LT;
         const C* uc = c == 0 ? u0 : (c == 1 ? u1 : u2);
         if (i < nki) prefetch_l2(uc + ((long long)i * nkj + j2) * NKK, NKK * sizeof(C));
     };
@@ -720,7 +733,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
-// [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).
+// [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).  Six fields, or
+// nine in the R-conv form (single simulations).
 template <int NY, class T, int CAP>
 __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
@@ -945,7 +959,7 @@ cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys,
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1) {                                                             \
-                if (g.rconv) {   /* R-conv: twelve fields, single simulations */                 \
+                if (g.rconv) {   /* R-conv: its own x pass, single simulations */                \
                     constexpr int NW = ConvCfg<N, T>::NW;                                         \
                     const long long nl = (lines + NW - 1) / NW;                                   \
                     const long long pf = NW * resident_ctas(k_xpass_conv<N, T>, 32 * NW, ConvCfg<N, T>::smem); \

@@ -272,11 +272,10 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     } while (0)
     // fields in the stored precision; zb (6 x NZ x NKJ x NKIP values, NZ >= NKK and
     // NKIP >= NKI) always holds 3S FP64 values, the conversion scratch of the mixed form.
-    // The R-conv form carries 12 fields through the inverse passes.
-    const size_t nfb = pass_fields(g);
+    // The R-conv form carries 9 fields through the inverse z and y passes.
     PD_ALLOC(h->fbuf, ce * 6 * (size_t)g.S);
-    PD_ALLOC(h->F.zb, ce * nfb * (size_t)g.nz * g.nkj * g.nkip);
-    PD_ALLOC(h->F.yb, ce * nfb * (size_t)g.nz * g.ny * g.nkip);
+    PD_ALLOC(h->F.zb, ce * (size_t)pass_fields(g) * g.nz * g.nkj * g.nkip);
+    PD_ALLOC(h->F.yb, ce * (size_t)pass_fields(g) * g.nz * g.ny * g.nkip);
     if (h->particles_on) PD_ALLOC(h->F.phys, ce / 2 * 3 * (size_t)g.R);
     PD_ALLOC(h->F.forcing, sizeof(double2) * 3 * (size_t)h->nforce);
     PD_ALLOC(h->tw, ce * (size_t)(g.nx + g.ny + g.nz));
@@ -1279,7 +1278,7 @@ extern "C" int pandora_batch_bytes(const pandora_params* p, int32_t capacity, in
     const long long S = nki * nkj * nkk, R = nx * ny * nz;
     const long long ce = p->precision == PANDORA_PREC_FP32_MIXED ? 8 : 16;
     const long long np = p->p_track_part ? p->p_np_global : 0;
-    const long long nfb = (p->f_type == PANDORA_F_SHEAR_DNS && p->ns_deformed == PANDORA_NS_R_CONV) ? 12 : 6;
+    const long long nfb = (p->f_type == PANDORA_F_SHEAR_DNS && p->ns_deformed == PANDORA_NS_R_CONV) ? 9 : 6;
     long long per = ce * 6 * S + ce * nfb * nz * nkj * nkip + ce * nfb * nz * ny * nkip + ce * (nx + ny + nz);
     if (p->p_track_part) per += ce / 2 * 3 * R + 2 * 8 * 14 * np + 4 * np;
     per += 1 << 20;   // clock, forcing, shells, member descriptors, allocator granularity

@@ -27,7 +27,7 @@ struct Geo {
     // homogeneous shear (F_TYPE = F_SHEAR_DNS); zero for isotropic flow
     int shear;
     int rrot;             // shear in a Rogallo form (NS_DEFORMED = NS_R_ROT or NS_R_CONV), else BF-rot
-    int rconv;            // ... the convective one (NS_R_CONV): u and its nine gradients transformed
+    int rconv;            // ... the convective one (NS_R_CONV): u and its nine gradients in real space
     double bdiag[3];      // bmat(1,1), bmat(2,2), bmat(3,3) = 1/B110, 1/B220, 1/B330
     double bidiag[3];     // binv diagonal = B110, B220, B330
     double shear_s;       // F_DEFORM_S = amat(1,3)
@@ -185,9 +185,9 @@ template <class T, int CAP> struct MemberSet {
 
 bool supported_length(int n);
 
-// Fields through the inverse passes (zb, yb): velocity and vorticity, or velocity and
-// the nine velocity gradients of the R-conv form.
-__host__ __device__ __forceinline__ int pass_fields(const Geo& g) { return g.rconv ? 12 : 6; }
+// Fields through the inverse z and y passes (zb, yb): velocity and vorticity, or in the
+// R-conv form velocity, d u / dy and d u / dz (d u / dx is formed in the x pass).
+__host__ __device__ __forceinline__ int pass_fields(const Geo& g) { return g.rconv ? 9 : 6; }
 
 // Calls f(set, n) for each chunk of at most kBatchChunk members of the B in M: a
 // MemberSet<T, 1> for a single simulation, MemberSet<T, kBatchChunk> (unused

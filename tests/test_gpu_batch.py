@@ -77,10 +77,13 @@ def test_batch_mixed_precision_and_slot_reuse(gpu_lib):
         assert _same(b.get_state(s2), _alone(gpu_lib, _member(base, 23), 2)[0])
 
 
-def test_batch_shear_across_remesh(gpu_lib):
+@pytest.mark.parametrize("form", [1, 3])
+def test_batch_shear_across_remesh(gpu_lib, form):
+    """BF-rot (1) and R-rot (3) members: the batched K1, x pass and K5b of each form."""
     base = gpu_lib.workload_params("shear", 32)
     base.p_track_part = 0
     base.f_remesh_t = 2                      # remesh at step 5
+    base.ns_deformed = form
     with gpu_lib.Batch(base, 2) as b:
         s0 = b.admit(_member(base, 31))
         b.step(2)
