@@ -221,9 +221,9 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     constexpr int R0 = XP::r0, R1 = XP::r1, R2 = XP::r2, NP = XP::np;
     if constexpr (NA == 2) {
         pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB>(s, tw, lane);
-    } else {
-        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s, tw, lane);
-        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + XAS, tw, lane);
+    } else {   // one array at a time, one copy of the code (instruction-cache footprint)
+#pragma unroll 1
+        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + a * XAS, tw, lane);
     }
     T umax = T(0);
     if constexpr (XP::fused) {
@@ -311,8 +311,8 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     if constexpr (NA == 2) {
         pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, F0, F1, F2, P0, NP, 0, KB>(s, tw, lane);
     } else {
-        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s, tw, lane);
-        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s + XAS, tw, lane);
+#pragma unroll 1
+        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s + a * XAS, tw, lane);
     }
     const T half = T(0.5);
     for (int m = lane; m < g.nkip; m += 32) {
@@ -387,7 +387,10 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
     auto bwd1 = [&](C* a) { pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(a, tw, lane); };
     auto bwd2 = [&](C* a) {   // arrays a and a + XAS
         if constexpr (NA == 2) pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB>(a, tw, lane);
-        else { bwd1(a); bwd1(a + XAS); }
+        else {
+#pragma unroll 1
+            for (int r = 0; r < 2; r++) bwd1(a + r * XAS);
+        }
     };
     // (u1,u2), (u3, du1/dx1) -> v = bmat u, NL1 = v1 du1/dx1; arrays 0, 1 = (v1,v2), (v3,NL1)
     build(0, 0, false, 1, false);
@@ -454,8 +457,8 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
     if constexpr (NA == 2) {
         pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
     } else {
-        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
-        pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s + XAS, tw, lane);
+#pragma unroll 1
+        for (int r = 0; r < 2; r++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s + r * XAS, tw, lane);
     }
     const T half = T(0.5);
     for (int m = lane; m < g.nkip; m += 32) {
