@@ -50,7 +50,8 @@ template <class R> __device__ __forceinline__ BFT<R> bf_as(const BF& f) {
 // components: w = sum_n omega(u_n).  Structurally w[0] has no term in u[0] and
 // w[1] none in u[1] (bex), so a caller that needs only w[0] or w[1] may pass zero
 // for that component.
-template <class R, class C>
+// ONLY >= 0: only component ONLY of w is formed (the others are left zero).
+template <int ONLY = -1, class R, class C>
 __device__ __forceinline__ void vort_bf(const BFT<R>& f, const C* u, const R* k, C* w) {
     w[0].x = R(0); w[0].y = R(0); w[1] = w[0]; w[2] = w[0];
 #pragma unroll
@@ -59,16 +60,16 @@ __device__ __forceinline__ void vort_bf(const BFT<R>& f, const C* u, const R* k,
 #pragma unroll
         for (int m = 0; m < 3; m++) {
             if (bex(m, 0)) {
-                if (bex(2, n)) { const R c = f.bm[m][0] * f.bi[2][n] * k[m]; w[1].y -= c * un.x; w[1].x += c * un.y; }
-                if (bex(1, n)) { const R c = f.bm[m][0] * f.bi[1][n] * k[m]; w[2].y += c * un.x; w[2].x -= c * un.y; }
+                if ((ONLY < 0 || ONLY == 1) && bex(2, n)) { const R c = f.bm[m][0] * f.bi[2][n] * k[m]; w[1].y -= c * un.x; w[1].x += c * un.y; }
+                if ((ONLY < 0 || ONLY == 2) && bex(1, n)) { const R c = f.bm[m][0] * f.bi[1][n] * k[m]; w[2].y += c * un.x; w[2].x -= c * un.y; }
             }
             if (bex(m, 1)) {
-                if (bex(2, n)) { const R c = f.bm[m][1] * f.bi[2][n] * k[m]; w[0].y += c * un.x; w[0].x -= c * un.y; }
-                if (bex(0, n)) { const R c = f.bm[m][1] * f.bi[0][n] * k[m]; w[2].y -= c * un.x; w[2].x += c * un.y; }
+                if ((ONLY < 0 || ONLY == 0) && bex(2, n)) { const R c = f.bm[m][1] * f.bi[2][n] * k[m]; w[0].y += c * un.x; w[0].x -= c * un.y; }
+                if ((ONLY < 0 || ONLY == 2) && bex(0, n)) { const R c = f.bm[m][1] * f.bi[0][n] * k[m]; w[2].y -= c * un.x; w[2].x += c * un.y; }
             }
             if (bex(m, 2)) {
-                if (bex(1, n)) { const R c = f.bm[m][2] * f.bi[1][n] * k[m]; w[0].y -= c * un.x; w[0].x += c * un.y; }
-                if (bex(0, n)) { const R c = f.bm[m][2] * f.bi[0][n] * k[m]; w[1].y += c * un.x; w[1].x -= c * un.y; }
+                if ((ONLY < 0 || ONLY == 0) && bex(1, n)) { const R c = f.bm[m][2] * f.bi[1][n] * k[m]; w[0].y -= c * un.x; w[0].x += c * un.y; }
+                if ((ONLY < 0 || ONLY == 1) && bex(0, n)) { const R c = f.bm[m][2] * f.bi[0][n] * k[m]; w[1].y += c * un.x; w[1].x -= c * un.y; }
             }
         }
     }
