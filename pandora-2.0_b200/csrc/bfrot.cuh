@@ -90,18 +90,33 @@ __device__ __forceinline__ C deriv_rrot(const BFT<R>& f, C u, const R* k, int j)
     }
     return d;
 }
-template <class R, class C>
+// ONLY >= 0: only component ONLY of w is formed, from its two derivatives (the others
+// are left zero); the same operations in the same order as for all three.
+template <int ONLY = -1, class R, class C>
 __device__ __forceinline__ void vort_rrot(const BFT<R>& f, const C* u, const R* k, C* w) {
-    const C dudy = deriv_rrot(f, u[0], k, 1), dudz = deriv_rrot(f, u[0], k, 2);
-    w[0].x = R(0); w[0].y = R(0);
-    w[1] = dudz;
-    w[2].x = -dudy.x; w[2].y = -dudy.y;
-    const C dvdx = deriv_rrot(f, u[1], k, 0), dvdz = deriv_rrot(f, u[1], k, 2);
-    w[0].x = w[0].x - dvdz.x; w[0].y = w[0].y - dvdz.y;
-    w[2].x = w[2].x + dvdx.x; w[2].y = w[2].y + dvdx.y;
-    const C dwdx = deriv_rrot(f, u[2], k, 0), dwdy = deriv_rrot(f, u[2], k, 1);
-    w[0].x = w[0].x + dwdy.x; w[0].y = w[0].y + dwdy.y;
-    w[1].x = w[1].x - dwdx.x; w[1].y = w[1].y - dwdx.y;
+    constexpr bool A0 = ONLY < 0 || ONLY == 0, A1 = ONLY < 0 || ONLY == 1, A2 = ONLY < 0 || ONLY == 2;
+    w[0].x = R(0); w[0].y = R(0); w[1] = w[0]; w[2] = w[0];
+    if constexpr (A1) w[1] = deriv_rrot(f, u[0], k, 2);
+    if constexpr (A2) {
+        const C dudy = deriv_rrot(f, u[0], k, 1);
+        w[2].x = -dudy.x; w[2].y = -dudy.y;
+    }
+    if constexpr (A0) {
+        const C dvdz = deriv_rrot(f, u[1], k, 2);
+        w[0].x = w[0].x - dvdz.x; w[0].y = w[0].y - dvdz.y;
+    }
+    if constexpr (A2) {
+        const C dvdx = deriv_rrot(f, u[1], k, 0);
+        w[2].x = w[2].x + dvdx.x; w[2].y = w[2].y + dvdx.y;
+    }
+    if constexpr (A0) {
+        const C dwdy = deriv_rrot(f, u[2], k, 1);
+        w[0].x = w[0].x + dwdy.x; w[0].y = w[0].y + dwdy.y;
+    }
+    if constexpr (A1) {
+        const C dwdx = deriv_rrot(f, u[2], k, 0);
+        w[1].x = w[1].x - dwdx.x; w[1].y = w[1].y - dwdx.y;
+    }
 }
 
 // f_RK3FormFRRot for F_SHEAR_DNS (src/pf_rk3.f90:2680-2856): viscous (f_RK3RRotViscous)

@@ -695,9 +695,12 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
             // omega1 has no term in u1 and omega2 none in u2: those loads are skipped
             const C uv[3] = {f != 3 ? F.u[0][m] : zero, f != 4 ? F.u[1][m] : zero, F.u[2][m]};
             C w3[3];
+            // only the CTA's own component (f is uniform over the CTA)
             if constexpr (FORM == 2) {
-                vort_rrot(bf, uv, kv, w3);
-            } else {   // only the CTA's own component (f is uniform over the CTA)
+                if (f == 3) vort_rrot<0>(bf, uv, kv, w3);
+                else if (f == 4) vort_rrot<1>(bf, uv, kv, w3);
+                else vort_rrot<2>(bf, uv, kv, w3);
+            } else {
                 if (f == 3) vort_bf<0>(bf, uv, kv, w3);
                 else if (f == 4) vort_bf<1>(bf, uv, kv, w3);
                 else vort_bf<2>(bf, uv, kv, w3);
