@@ -78,11 +78,9 @@ __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ Me
     constexpr int nh = ORD / 2;
     const double D[3] = {g.dx, g.dy, g.dz};
     const int NN[3] = {g.nx, g.ny, g.nz};
-    double xp[3], up[3], ur[3], pr[3];
+    double xp[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        xp[c] = P.xp[c][nn]; up[c] = P.up[c][nn]; ur[c] = P.uprk[c][nn]; pr[c] = P.prk[c][nn];
-    }
+    for (int c = 0; c < 3; c++) xp[c] = P.xp[c][nn];
     // p_InterpFindMolecule: stencil start from the same rounded arithmetic
     double w[3][ORD];
     int idx[3][ORD];
@@ -168,6 +166,11 @@ __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ Me
         }
         if (sub != 0 || !valid) return;
     }
+    // the particle's RK3 state, read only by the thread that updates it, after the
+    // gather (not held in registers across it)
+    double up[3], ur[3], pr[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) { up[c] = P.up[c][nn]; ur[c] = P.uprk[c][nn]; pr[c] = P.prk[c][nn]; }
     double xw[3] = {xp[0], xp[1], xp[2]};   // frame in which the RK3 update runs
     if (g.shear) {
         // p_RK3SolveParticleBF (src/pp_rk3.f90:169-303): velocity and position to
