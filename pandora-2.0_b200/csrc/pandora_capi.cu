@@ -64,6 +64,9 @@ static int cuda_fail(cudaError_t e, const char* where) {
     snprintf(g_errmsg, sizeof(g_errmsg), "%s: %s", where, cudaGetErrorString(e));
     return PANDORA_ERR_CUDA;
 }
+namespace pd {
+int cuda_fail_msg(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+}  // namespace pd
 #define PD_CK(x)                                          \
     do {                                                  \
         cudaError_t _e = (x);                             \
@@ -1211,7 +1214,7 @@ static bool same_class(const pandora_params* a, const pandora_params* b) {
            a->precision == b->precision && a->f_type == b->f_type && a->ns_deformed == b->ns_deformed &&
            a->b110 == b->b110 && a->b220 == b->b220 && a->b330 == b->b330 && a->dealiasing == b->dealiasing && a->les_cutoff == b->les_cutoff &&
            na == nb && (na == 0 || a->p_interp_order == b->p_interp_order) &&
-           (int)a->force_kf == (int)b->force_kf;
+           a->force_kf == b->force_kf;   // the forcing radius of the class geometry (mask kmag <= kf)
 }
 
 template <class T> static Member<T> slot_member(pandora_batch* b, int slot, int on) {
@@ -1407,7 +1410,9 @@ extern "C" int pandora_batch_finish(pandora_batch* b, int32_t slot, int64_t* tic
 
 extern "C" int pandora_batch_ticket_done(pandora_batch* b, int64_t ticket, int32_t* done) {
     if (!b || !done || ticket < 0 || ticket >= b->ticket) return PANDORA_ERR_INVALID_ARG;
-    if (b->ticket - ticket > pandora_batch::kTickets) { *done = 1; return PANDORA_OK; }   // long retired
+    // The slot of an old ticket may hold a newer record on the same stream; that one
+    // completes after the old one, so its completion still implies the old ticket's
+    // (a not-ready answer is then conservative).
     const cudaError_t e = cudaEventQuery(b->ev[ticket % pandora_batch::kTickets]);
     if (e == cudaErrorNotReady) { cudaGetLastError(); *done = 0; return PANDORA_OK; }
     PD_CK(e);

@@ -185,6 +185,10 @@ template <class T, int CAP> struct MemberSet {
 
 bool supported_length(int n);
 
+// Records "where: <CUDA error string>" as the message pandora_strerror returns for
+// PANDORA_ERR_CUDA (thread-local, the last failure wins) and returns PANDORA_ERR_CUDA.
+int cuda_fail_msg(cudaError_t e, const char* where);
+
 // Fields through the inverse z and y passes (zb, yb): velocity and vorticity, or in the
 // R-conv form velocity, d u / dy and d u / dz (d u / dx is formed in the x pass).
 __host__ __device__ __forceinline__ int pass_fields(const Geo& g) { return g.rconv ? 9 : 6; }

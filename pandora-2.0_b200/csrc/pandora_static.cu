@@ -52,16 +52,17 @@ int static_ptrs(int dev, StaticPtrs** out) {
     std::lock_guard<std::mutex> lock(g_mutex);
     StaticPtrs& s = g_ptrs[dev];
     if (!s.ready) {
-        if (cudaGetSymbolAddress((void**)&s.zb, g_static_zb) != cudaSuccess ||
-            cudaGetSymbolAddress((void**)&s.yb, g_static_yb) != cudaSuccess ||
-            cudaGetSymbolAddress((void**)&s.tw, g_static_tw) != cudaSuccess ||
-            cudaGetSymbolAddress((void**)&s.clock, g_static_clock) != cudaSuccess) {
+        cudaError_t e;
+        if ((e = cudaGetSymbolAddress((void**)&s.zb, g_static_zb)) != cudaSuccess ||
+            (e = cudaGetSymbolAddress((void**)&s.yb, g_static_yb)) != cudaSuccess ||
+            (e = cudaGetSymbolAddress((void**)&s.tw, g_static_tw)) != cudaSuccess ||
+            (e = cudaGetSymbolAddress((void**)&s.clock, g_static_clock)) != cudaSuccess) {
             cudaGetLastError();
-            return PANDORA_ERR_CUDA;
+            return pd::cuda_fail_msg(e, "pandora_nonlinear_static: cudaGetSymbolAddress");
         }
-        if (cudaMemset(s.clock, 0, sizeof(pd::Clock)) != cudaSuccess) {
+        if ((e = cudaMemset(s.clock, 0, sizeof(pd::Clock))) != cudaSuccess) {
             cudaGetLastError();
-            return PANDORA_ERR_CUDA;
+            return pd::cuda_fail_msg(e, "pandora_nonlinear_static: clearing the scalar block");
         }
         s.ready = true;
     }
@@ -113,10 +114,14 @@ extern "C" int pandora_nonlinear_static(const pandora_params* p, const double* u
         }
         off += lens[d];
     }
-    if (cudaMemcpyAsync(sp->tw, tw, sizeof(double2) * off, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        pd::configure_kernels<double>(g) != cudaSuccess) {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(sp->tw, tw, sizeof(double2) * off, cudaMemcpyHostToDevice, st)) != cudaSuccess) {
         cudaGetLastError();
-        return PANDORA_ERR_CUDA;
+        return pd::cuda_fail_msg(e, "pandora_nonlinear_static: twiddle upload");
+    }
+    if ((e = pd::configure_kernels<double>(g)) != cudaSuccess) {
+        cudaGetLastError();
+        return pd::cuda_fail_msg(e, "pandora_nonlinear_static: kernel attributes");
     }
     pd::Fields F{};
     F.u[0] = (double2*)u1; F.u[1] = (double2*)u2; F.u[2] = (double2*)u3;
@@ -131,13 +136,18 @@ extern "C" int pandora_nonlinear_static(const pandora_params* p, const double* u
     m.active = 1;
     const pd::Member<double>* M = &m;   // passed to the kernels by value
     // the same five passes as the step, with the last one storing NL-hat instead of updating
-    if (pd::launch_zpass_inv(g, M, 1, 0, st) != cudaSuccess || pd::launch_ypass_inv(g, M, 1, st) != cudaSuccess ||
-        pd::launch_xpass(g, M, 1, 0, 0, st) != cudaSuccess || pd::launch_ypass_fwd(g, M, 1, st) != cudaSuccess ||
-        pd::launch_zpass_fwd_update(g, M, 1, 1, 1, st) != cudaSuccess) {
+    if ((e = pd::launch_zpass_inv(g, M, 1, 0, st)) != cudaSuccess ||
+        (e = pd::launch_ypass_inv(g, M, 1, st)) != cudaSuccess ||
+        (e = pd::launch_xpass(g, M, 1, 0, 0, st)) != cudaSuccess ||
+        (e = pd::launch_ypass_fwd(g, M, 1, st)) != cudaSuccess ||
+        (e = pd::launch_zpass_fwd_update(g, M, 1, 1, 1, st)) != cudaSuccess) {
         cudaGetLastError();
-        return PANDORA_ERR_CUDA;
+        return pd::cuda_fail_msg(e, "pandora_nonlinear_static: transform pass launch");
     }
     // the host twiddle table must outlive the copy
-    if (cudaStreamSynchronize(st) != cudaSuccess) { cudaGetLastError(); return PANDORA_ERR_CUDA; }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        cudaGetLastError();
+        return pd::cuda_fail_msg(e, "pandora_nonlinear_static: stream synchronise");
+    }
     return PANDORA_OK;
 }

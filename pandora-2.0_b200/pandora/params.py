@@ -103,7 +103,9 @@ def workload_params(name: str, n: int | None = None) -> Params:
     ``iso_decay``: decaying isotropic turbulence, nu=0.01, dt=0.005 fixed, no
     forcing, Ahmed/Elghobashi spectrum with U0 = 2/3 u0^2 (u0=1, kp=4).
     ``iso_forced_particles``: forced isotropic turbulence, nu=0.002, dt=0.002
-    fixed, OU forcing on |k| <= 2.5 with sigma^2 T_F = 0.1, kp=3, 2^20 tracers
+    fixed, OU forcing on |k| <= 2.5 with sigma^2 = P / (100 T_F) for an injected
+    power P = 0.1 (the factor 100 is a calibration measured on this forcing, not
+    the reference's e* = sigma^2 T_F), kp=3, 2^20 tracers
     (P_INIT_RANDOM, 4th-order interpolation, released at step 1).
     ``iso_forced``: the same forcing at nu=0.0008, dt=0.001, no particles (1024^3).
     ``shear``: homogeneous shear S=1 in the Rogallo frame (BF-rot), B110=2, 2^18 tracers.
@@ -119,9 +121,11 @@ def workload_params(name: str, n: int | None = None) -> Params:
         p = default_params(n or 256)
         p.f_nu, p.rk3_timestep, p.rk3_dt, p.tsteps = 0.002, RK3_TIMESTEP_FIXED, 0.002, 500
         p.force_kf, p.force_tf, p.force_stop = 2.5, 0.2, 100000
-        # injected power P = 0.1: the reference's printed e* = sigma^2 T_F
-        # (src/pf_force.f90:410) does not count the ~80 forced modes; measured
-        # injection is P ~ 100 sigma^2 T_F, so sigma^2 = P / (100 T_F)
+        # injected power P = 0.1.  The reference prints e* = sigma^2 T_F
+        # (src/pf_force.f90:394-424) as its forcing's power, which does not count
+        # the ~80 forced modes; the injection measured on this forcing (the mean
+        # of sum_k Re(f . conj u) over many steps) is P ~ 100 sigma^2 T_F, an
+        # observed calibration, so sigma^2 = P / (100 T_F)
         p.force_sigma = math.sqrt(0.1 / (100.0 * 0.2))
         p.f_init_type, p.f_init_kp, p.f_init_u0 = F_INIT_AHMED_ELGHOBASHI, 3.0, 2.0 / 3.0
         p.p_track_part, p.p_init_type, p.p_np_global = 1, P_INIT_RANDOM, 1 << 20

@@ -123,3 +123,38 @@ def test_ensemble_server_results_same_alone(gpu_lib):
     for r in trace:
         u, _ = _alone(gpu_lib, r.params, r.steps)
         assert _same(r.result["u"], u), r.rid
+
+
+def test_batch_rejects_other_forcing_radius(gpu_lib):
+    """The forcing mask is kmag <= FORCE_KF, a real number: a member whose radius differs
+    only in its fractional part is another class, not a member that would run with the
+    batch's radius."""
+    base = gpu_lib.workload_params("iso_forced_particles", 32)
+    base.p_track_part = 0
+    other = _member(base, 5)
+    other.force_kf = 2.9                  # same aint(FORCE_KF) = 2 as the batch's 2.5
+    with gpu_lib.Batch(base, 2) as b:
+        with pytest.raises(gpu_lib.PandoraError):
+            b.admit(other)
+        assert gpu_lib.class_key(other) != gpu_lib.class_key(base)
+
+
+def test_batch_many_outstanding_tickets(gpu_lib):
+    """More tickets outstanding than the batch keeps events for: an old ticket is done
+    only once its work is, and a finished member's statistics are readable then."""
+    base = gpu_lib.workload_params("iso_decay", 32)
+    with gpu_lib.Batch(base, 2) as b:
+        s0 = b.admit(_member(base, 41))
+        first = b.step(1)
+        tickets = [b.step(1) for _ in range(600)]     # more than the 512 event slots
+        fin = b.finish(s0)
+        assert fin > tickets[-1] > first
+        b.sync()
+        assert b.done(first) and b.done(tickets[0]) and b.done(fin)
+        ek, tke, eps = b.result_stats(s0)
+        # the statistics of stage 1 of the member's last step (its 601st)
+        u, _ = _alone(gpu_lib, _member(base, 41), 600)
+        with gpu_lib.Simulation(_member(base, 41)) as s:
+            s.set_state(u)
+            ek2, tke2, eps2, _ = s.stats()
+        assert tke == pytest.approx(tke2, rel=1e-12) and eps == pytest.approx(eps2, rel=1e-12)
