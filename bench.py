@@ -1,9 +1,12 @@
 """Benchmark of the PANDORA 2.0 RK3 time step on B200.
 
-Workload (default): forced isotropic turbulence at 256^3, FP64, OU forcing on
-|k| <= 2.5, 2^20 tracers with 4th-order interpolation advanced at every stage;
-synthetic seeded initial field (Ahmed/Elghobashi spectrum, kp = 3).  A "step" is
-one full RK3 step (three stages, statistics at stage 1, forcing, particles).
+Workload (default): homogeneous shear at 512^3 in the Rogallo frame (BF-rot form,
+F_TYPE = F_SHEAR_DNS), lab box 4pi x 2pi x 2pi (B110 = 2), S = 1, nu = 0.005,
+dt = (0.5/S)/F_REMESH_T = 0.002, FP64, 2^18 tracers with 4th-order interpolation
+advanced at every stage; synthetic seeded initial field (Ahmed/Elghobashi spectrum,
+kp = 4, u0 = 0.5).  A "step" is one full RK3 step (three stages, statistics at
+stage 1, particles, the remesh check).  ``--workload iso_forced_particles --n 256``
+gives the forced isotropic case with 2^20 tracers.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -28,10 +31,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "pandora-2.0_b200"))
 
 METRIC = "Mpts·RK3steps/s"
-WORKLOAD = "iso_forced_particles"
-# per-launch DRAM traffic (read + write) of the dominant pass, from the ncu capture
-# summarised in profiles/xpass_iso_forced_particles_256_dram.md (None where not captured)
-NCU_TRAFFIC_BYTES = {(256, "xpass_nl"): 553719296 + 627172608}
+WORKLOAD = "shear"
+# DRAM traffic (read + write bytes) of one launch of a pass, from single-kernel ncu
+# captures of these workloads: (workload, N, form, pass) -> bytes.  The captures and
+# their commands are summarised under profiles/.
+NCU_TRAFFIC_BYTES = {
+    ("iso_forced_particles", 256, "fp64_plain", "xpass_nl"): 553719296 + 627172608,
+}
+# Seconds of host work the reference arm spends on its timed steps at most (the
+# whole arm, warm-up and set-up included, stays within a few minutes).
+REF_BUDGET_S = 100.0
 
 
 def _args():
@@ -41,8 +50,10 @@ def _args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
-    ap.add_argument("--n", "--grid", dest="n", type=int, default=256)
-    ap.add_argument("--np", "--particles", dest="np", type=int, default=1 << 20)
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=None,
+                    help="grid points per direction (default: the workload's own, 512 for shear)")
+    ap.add_argument("--np", "--particles", dest="np", type=int, default=None,
+                    help="tracers (default: the workload's own, 2^18 for shear)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed"],
                     help="fp32_mixed: FP32 fields and transforms, FP64 bookkeeping (our arm only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -52,7 +63,7 @@ def _args():
 def _params(a, fp64=False):
     from pandora.params import PREC_FP32_MIXED, PREC_FP64, workload_params
     p = workload_params(a.workload, a.n)
-    if p.p_track_part:
+    if p.p_track_part and a.np is not None:
         p.p_np_global = a.np
     p.precision = PREC_FP32_MIXED if (a.precision == "fp32_mixed" and not fp64) else PREC_FP64
     return p
@@ -171,69 +182,103 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(p, stages: int = 3):
-    """The oracle (CPU restatement of the reference, OpenMP) on the host cores:
-    `stages` RK3 stages of the same workload.  Returns (Mpts*steps/s, cores, secs)."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def _oracle(p):
+    """The oracle (CPU restatement of the reference, OpenMP over the host cores) on the
+    workload's seeded initial state."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     o = O.Oracle(p)
     o.init_fluid()
     if p.p_track_part:
         o.init_particles()
-    dt = 0.0
+    return O, o
+
+
+def cpu_baseline(p):
+    """One warm RK3 step of the same workload on the host: one step untimed (first touch
+    of every array, thread pool start), then one step timed.
+    Returns (Mpts*steps/s, cores, secs of the timed step)."""
+    O, o = _oracle(p)
+    t, _ = o.step(1, 0.0)
     t0 = time.perf_counter()
-    for s in range(1, stages + 1):
-        dt = o.stage(s, 1, dt)
+    o.step(2, t)
     secs = time.perf_counter() - t0
     npts = p.nodes_x * p.nodes_y * p.nodes_z
     o.close()
-    return npts * (stages / 3.0) / secs / 1e6, O.threads(), secs
+    return npts / secs / 1e6, O.threads(), secs
 
 
 def run_reference(a, p):
+    """The reference's algorithm on the host cores (the oracle's OpenMP C restatement:
+    the Fortran + MPI + PETSc + FFTW reference has no toolchain on this image).  Times
+    whole RK3 steps: up to W warm-up steps (at least one, at most three), then K timed
+    steps or as many as fit in REF_BUDGET_S seconds, whichever is fewer; the line reports
+    the counts actually run."""
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    o = O.Oracle(p)
-    o.init_fluid()
-    if p.p_track_part:
-        o.init_particles()
+    O, o = _oracle(p)
     npts = p.nodes_x * p.nodes_y * p.nodes_z
-    dt = 0.0
-    stage = 0
-    # each bench step = one RK3 stage (1/3 of a time step) of the full workload
-    for _ in range(a.warmup):
-        dt = o.stage(stage % 3 + 1, 1 + stage // 3, dt)
-        stage += 1
+    t = 0.0
+    step = 1
+    n_warm = max(1, min(a.warmup, 3))
+    w0 = time.perf_counter()
+    for _ in range(n_warm):
+        t, _ = o.step(step, t)
+        step += 1
+    per = (time.perf_counter() - w0) / n_warm
+    n_timed = max(1, min(a.steps, int(REF_BUDGET_S // max(per, 1e-9))))
     t0 = time.perf_counter()
-    for _ in range(a.steps):
-        dt = o.stage(stage % 3 + 1, 1 + stage // 3, dt)
-        stage += 1
+    for _ in range(n_timed):
+        t, _ = o.step(step, t)
+        step += 1
     secs = time.perf_counter() - t0
-    value = npts * (a.steps / 3.0) / secs / 1e6
+    o.close()
+    value = npts * n_timed / secs / 1e6
+    cores = O.threads()
+    sample = (f"{n_timed} whole RK3 steps (3 stages each) of the full workload after {n_warm} warm-up "
+              f"step(s), OpenMP C restatement of the reference's algorithm (oracle/pandora_oracle.c) on "
+              f"{cores} threads of {cpu_model()}; the reference binary (Fortran+MPI+PETSc+FFTW) has no "
+              f"toolchain on this image")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * secs / a.steps * 3.0,
+        "steps": n_timed, "warmup": n_warm, "ms_per_step": 1e3 * secs / n_timed,
+        "requested": {"steps": a.steps, "warmup": a.warmup, "budget_s": REF_BUDGET_S},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Rogallo field, seeded tracers)",
         "config": _config(a, p),
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": O.threads(), "kind": "port",
-                         "sample": f"{a.steps} RK3 stages (1/3 step each) of the full workload; the reference "
-                                   "binary (Fortran+MPI+PETSc+FFTW) has no toolchain on this image, so this "
-                                   "is the C restatement of its algorithm (oracle/pandora_oracle.c)"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port", "cpu": cpu_model(),
+                         "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def form_key(p) -> str:
+    return "fp32_mixed" if p.precision == 1 else "fp64_plain"
+
+
 def _config(a, p):
     npart = int(p.p_np_global) if p.p_track_part else 0
     if p.f_type == 2:
-        phys = (f"homogeneous shear S={p.f_deform_s} (Rogallo frame, BF-rot), B110={p.b110}, "
-                f"dt=(0.5/S)/{p.f_remesh_t}, no forcing")
+        dt = 0.5 / p.f_deform_s / p.f_remesh_t
+        form_name = {1: "BF-rot", 2: "R-conv", 3: "R-rot"}.get(p.ns_deformed, "?")
+        first = p.b110 * p.f_remesh_t + 1
+        phys = (f"homogeneous shear S={p.f_deform_s} (Rogallo frame, {form_name}), box "
+                f"{2 * p.b110}pi x 2pi x 2pi (B110={p.b110}), nu={p.f_nu}, dt=(0.5/S)/F_REMESH_T={dt:g} "
+                f"(remesh at step {first} and every {2 * p.b110 * p.f_remesh_t} steps after), no forcing")
     elif p.force_stop > 0:
         phys = f"OU forcing |k|<={p.force_kf}, nu={p.f_nu}, dt={p.rk3_dt}"
     else:
@@ -365,7 +410,7 @@ def run_ours(a, p):
                 "timed": ("dominant pass (of those with the GPU to themselves): event pair in the step graph, stages 2-3 of the last timed step; "
                           "other passes: the same in the last warm-up step") if per_pass_live
                          else "alone, 20 back-to-back launches",
-                "traffic": NCU_TRAFFIC_BYTES.get((a.n, dom)),
+                "traffic": NCU_TRAFFIC_BYTES.get((a.workload, p.nodes_x, form_key(p), dom)),
                 "per_pass": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)} for k, v in src.items()},
                 "per_pass_alone": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)}
                                    for k, v in per_pass.items()}}
@@ -392,9 +437,10 @@ def run_ours(a, p):
     line["step_model_gbs"] = _step_model(p, ms / a.steps, peak)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         v, cores, secs = cpu_baseline(_params(a, fp64=True))
-        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                                "sample": f"one RK3 step (3 stages) of the same workload on the host, "
-                                          f"{secs:.1f} s, OpenMP C restatement (oracle/pandora_oracle.c)"}
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": cores, "kind": "port", "cpu": cpu_model(),
+                                "sample": f"one warm RK3 step (3 stages, after one untimed step) of the same "
+                                          f"workload in FP64 on {cores} threads of the host, {secs:.1f} s, OpenMP C "
+                                          f"restatement of the reference's algorithm (oracle/pandora_oracle.c)"}
     sim.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -54,4 +54,7 @@ def test_reference_arm_under_torchrun_prints_on_rank_zero_only():
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    # whole RK3 steps, the counts actually run: one warm-up step at least, then the timed one
+    assert d["steps"] == 1 and d["warmup"] == 1
+    assert d["ms_per_step"] * d["steps"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
