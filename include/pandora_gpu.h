@@ -69,6 +69,18 @@ extern "C" {
  * RHS/RK3 arithmetic, the particles and the E(k)/epsilon shell sums in FP64.  Every
  * boundary call still takes and returns FP64 arrays. */
 #define PANDORA_PREC_FP32_MIXED      1
+/* Viscous term of the RK3 step (pandora_params.rk3_viscous).  EXPLICIT is the
+ * reference's: -F_NU k^2 u inside the right-hand side of every stage
+ * (src/pf_rk3.f90:2388-2390, combined at 2471).  INTEGRATING_FACTOR has no
+ * counterpart in the reference: the low-storage RK3 runs on v = exp(F_NU k^2 t) u,
+ * which with u and the register kept in physical units reads, per stage s,
+ *   r_s = E_s (beta_s r_{s-1} + N(u_{s-1})),  u_s = E_s u_{s-1} + gamma_s dt r_s,
+ *   E_s = exp(-F_NU k^2 (c_{s+1} - c_s) dt),  c = 0, 1/3, 3/4, 1,
+ * N the right-hand side without the viscous term; the exponent is formed in FP64 in
+ * both precisions.  Isotropic flow only (the wavenumbers of the sheared frame move
+ * with time); other flow types return PANDORA_ERR_UNSUPPORTED. */
+#define PANDORA_VISCOUS_EXPLICIT     0
+#define PANDORA_VISCOUS_INTEGRATING_FACTOR 1
 
 /*
  * Namelist fields of ip_file.in that the RK3 step reads (src/pg_control.f90:385-436),
@@ -113,7 +125,9 @@ typedef struct pandora_params {
     uint64_t seed_fluid, seed_force, seed_particles;
     /* arithmetic of the step: PANDORA_PREC_FP64 or PANDORA_PREC_FP32_MIXED */
     int32_t precision;
-    int32_t reserved0;
+    /* viscous term: PANDORA_VISCOUS_EXPLICIT (0, the reference's) or
+     * PANDORA_VISCOUS_INTEGRATING_FACTOR (1) */
+    int32_t rk3_viscous;
     /* nl_numerics LES_CUTOFF: cutoff of DEALIASING = 3 as a multiple of KMAX */
     double  les_cutoff;
     int32_t reserved[4];

@@ -1068,10 +1068,21 @@ void rk_coeffs(int stage, double* beta, double* gamma) {
     else { *beta = -(153.0 / 128.0); *gamma = 8.0 / 15.0; }
 }
 
+/* Integrating-factor variant (PANDORA_VISCOUS_INTEGRATING_FACTOR, no counterpart in
+ * the reference, whose viscous term is explicit): the low-storage RK3 applied to
+ * v = exp(nu k^2 (t - t0)) u with u and the register stored in physical units, so stage s
+ * scales both by E_s = exp(-nu k^2 (c_{s+1} - c_s) dt), c = 0, 1/3, 3/4, 1, and the
+ * right-hand side drops -nu k^2 u. */
+static double if_fraction(int stage) {
+    return stage == 1 ? 1.0 / 3.0 : (stage == 2 ? 5.0 / 12.0 : 1.0 / 4.0);
+}
+
 static void form_f_iso(oracle* o, int stage, double dt) {
     double beta, gamma;
     rk_coeffs(stage, &beta, &gamma);
     const double nu = o->p.f_nu, kf = o->p.force_kf;
+    const int ifac = o->p.rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR;
+    const double dcs = if_fraction(stage);
     const int NK = o->fnk;
 #pragma omp parallel for schedule(static)
     for (long ij = 0; ij < (long)o->nki * o->nkj; ij++) {
@@ -1103,18 +1114,34 @@ static void form_f_iso(oracle* o, int stage, double dt) {
                     }
                 }
             }
-            for (int c = 0; c < 3; c++) {
-                double vr = -nu * kmag2 * uu[c].re, vi = -nu * kmag2 * uu[c].im;
-                double pr = (kv[c] / kmag2) * kdn.re, pi = (kv[c] / kmag2) * kdn.im;
-                tot[c].re = vr - nl[c].re + pr + force[c].re + 0.0;
-                tot[c].im = vi - nl[c].im + pi + force[c].im + 0.0;
-            }
-            for (int c = 0; c < 3; c++) {
-                cx* r = &o->rk[c][m];
-                r->re = (beta * r->re) + tot[c].re;
-                r->im = (beta * r->im) + tot[c].im;
-                uu[c].re = uu[c].re + (gamma * dt * r->re);
-                uu[c].im = uu[c].im + (gamma * dt * r->im);
+            if (ifac) {
+                const double ex = exp(-(nu * kmag2 * dcs * dt));
+                for (int c = 0; c < 3; c++) {
+                    double pr = (kv[c] / kmag2) * kdn.re, pi = (kv[c] / kmag2) * kdn.im;
+                    tot[c].re = -nl[c].re + pr + force[c].re;
+                    tot[c].im = -nl[c].im + pi + force[c].im;
+                }
+                for (int c = 0; c < 3; c++) {
+                    cx* r = &o->rk[c][m];
+                    r->re = ex * ((beta * r->re) + tot[c].re);
+                    r->im = ex * ((beta * r->im) + tot[c].im);
+                    uu[c].re = (ex * uu[c].re) + (gamma * dt * r->re);
+                    uu[c].im = (ex * uu[c].im) + (gamma * dt * r->im);
+                }
+            } else {
+                for (int c = 0; c < 3; c++) {
+                    double vr = -nu * kmag2 * uu[c].re, vi = -nu * kmag2 * uu[c].im;
+                    double pr = (kv[c] / kmag2) * kdn.re, pi = (kv[c] / kmag2) * kdn.im;
+                    tot[c].re = vr - nl[c].re + pr + force[c].re + 0.0;
+                    tot[c].im = vi - nl[c].im + pi + force[c].im + 0.0;
+                }
+                for (int c = 0; c < 3; c++) {
+                    cx* r = &o->rk[c][m];
+                    r->re = (beta * r->re) + tot[c].re;
+                    r->im = (beta * r->im) + tot[c].im;
+                    uu[c].re = uu[c].re + (gamma * dt * r->re);
+                    uu[c].im = uu[c].im + (gamma * dt * r->im);
+                }
             }
             cx kdu = {k1 * uu[0].re + k2 * uu[1].re + k3 * uu[2].re,
                       k1 * uu[0].im + k2 * uu[1].im + k3 * uu[2].im};
@@ -1658,6 +1685,8 @@ static double tstep_dt(const oracle* o, double ucfl) {
 /* f_RK3Stage{1,2,3} (src/pf_rk3.f90:40-200); *dt in/out */
 int oracle_stage(oracle* o, int stage, int tstep, double* dt) {
     if (o->p.f_type != PANDORA_F_ISOTROPIC && o->p.f_type != PANDORA_F_SHEAR_DNS) return PANDORA_ERR_UNSUPPORTED;
+    if (o->p.rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR && o->p.f_type != PANDORA_F_ISOTROPIC)
+        return PANDORA_ERR_UNSUPPORTED;
     if (stage == 1 && o->shear && oracle_remesh_due(o, tstep)) {   /* src/pf_rk3.f90:3990-4025 */
         dealias(o);
         particles_remesh(o);

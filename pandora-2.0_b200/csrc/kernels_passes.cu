@@ -500,7 +500,8 @@ template <class C> struct Out3 { C* p[3]; };
 // side: 3 and 4 CTAs of 256 threads per SM, without spills.
 // The per-mode arithmetic runs in FP64 registers in both forms (the FP32-mixed
 // form loads FP32 values and rounds once on the store).
-// FORM: 0 isotropic, 1 BF-rot shear, 2 R-rot shear.
+// FORM: 0 isotropic, 1 BF-rot shear, 2 R-rot shear, 3 isotropic with the integrating
+// factor (its own instantiation, so the explicit forms carry no exponent code).
 template <int FORM, class T, int CAP>
 __global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
     using C = typename FieldsT<T>::C;
@@ -556,11 +557,23 @@ __global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __gr
                     force[c] = mk(fv[c].x - ((kv[c] / kmag2) * kdb.x), fv[c].y - ((kv[c] / kmag2) * kdb.y));
             }
         }
+        if constexpr (FORM == 3) {   // integrating factor: the viscous term leaves the right-hand side
 #pragma unroll
-        for (int c = 0; c < 3; c++)
-            tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
-                        -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+            for (int c = 0; c < 3; c++)
+                tot[c] = mk(-nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
+                            -nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
+                            -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+        }
     }
+    // Integrating factor (isotropic flow): E = exp(-nu k^2 (c_{s+1} - c_s) dt), c = 0, 1/3,
+    // 3/4, 1, scales the register and u of the stage (FP64 exponent in both precisions)
+    constexpr bool vif = FORM == 3;
+    double ex = 1.0;
+    if constexpr (vif) ex = exp(-(g.nu * kmag2 * (stage == 1 ? 1.0 / 3.0 : (stage == 2 ? 5.0 / 12.0 : 0.25)) * dt));
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         double2 r;
@@ -568,6 +581,10 @@ __global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __gr
         else {
             const double2 r0 = to_d(F.rk[c][m]);
             r = mk((beta * r0.x) + tot[c].x, (beta * r0.y) + tot[c].y);
+        }
+        if constexpr (vif) {
+            r = mk(ex * r.x, ex * r.y);
+            uu[c] = mk(ex * uu[c].x, ex * uu[c].y);
         }
         F.rk[c][m] = from_d<C>(r);
         uu[c] = mk(uu[c].x + (gamma * dt * r.x), uu[c].y + (gamma * dt * r.y));
@@ -1050,6 +1067,7 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int
         const dim3 grid((unsigned)((g.S + 255) / 256), nb);
         if (g.rrot) k_rk_update<2, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
         else if (g.shear) k_rk_update<1, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
+        else if (g.visc_if) k_rk_update<3, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
         else k_rk_update<0, T, CAP><<<grid, 256, 0, st>>>(ms, stage);
     });
 }

@@ -206,6 +206,11 @@ static int validate(const pandora_params* p) {
         if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
             return PANDORA_ERR_INVALID_ARG;
     }
+    if (p->rk3_viscous != PANDORA_VISCOUS_EXPLICIT && p->rk3_viscous != PANDORA_VISCOUS_INTEGRATING_FACTOR)
+        return PANDORA_ERR_INVALID_ARG;
+    // the integrating factor of a sheared frame would need the time integral of its moving k^2
+    if (p->rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR && p->f_type != PANDORA_F_ISOTROPIC)
+        return PANDORA_ERR_UNSUPPORTED;
     if (p->dealiasing < PANDORA_DEALIASING_23 || p->dealiasing > PANDORA_DEALIASING_LES) return PANDORA_ERR_UNSUPPORTED;
     if (p->dealiasing == PANDORA_DEALIASING_LES && !(p->les_cutoff > 0.0)) return PANDORA_ERR_INVALID_ARG;
     if (!supported_length(p->nodes_x) || !supported_length(p->nodes_y) || !supported_length(p->nodes_z))
@@ -256,6 +261,7 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.b110 = p->b110; g.remesh_t = p->f_remesh_t;
     g.rk3_decide = (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) ? 1 : 0;
     g.bvol = (double)p->b110 * (double)p->b220 * (double)p->b330;
+    g.visc_if = p->rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR ? 1 : 0;
     {   // KMAX = min(KI_MAX, KJ_MAX, KK_MAX) (src/pg_domain.f90:231)
         const double kmax = (double)std::min(g.ki, std::min(g.kj, g.kk));
         g.dealias_cut = p->dealiasing == PANDORA_DEALIASING_SPHERICAL ? kmax
@@ -1213,6 +1219,7 @@ static bool same_class(const pandora_params* a, const pandora_params* b) {
     return a->nodes_x == b->nodes_x && a->nodes_y == b->nodes_y && a->nodes_z == b->nodes_z &&
            a->precision == b->precision && a->f_type == b->f_type && a->ns_deformed == b->ns_deformed &&
            a->b110 == b->b110 && a->b220 == b->b220 && a->b330 == b->b330 && a->dealiasing == b->dealiasing && a->les_cutoff == b->les_cutoff &&
+           a->rk3_viscous == b->rk3_viscous &&   // one update kernel per launch
            na == nb && (na == 0 || a->p_interp_order == b->p_interp_order) &&
            a->force_kf == b->force_kf;   // the forcing radius of the class geometry (mask kmag <= kf)
 }

@@ -36,6 +36,9 @@ struct Geo {
     // DEALIASING 2 (2/3 sphere) or 3 (LES cutoff): modes with |k_lab| above this are
     // zeroed (src/pf_arrays.f90:1865-1987); 0 for the 2/3 rule alone
     double dealias_cut;
+    // PANDORA_VISCOUS_INTEGRATING_FACTOR: the viscous term as exp(-nu k^2 dc dt) factors
+    // of u and the register per stage (isotropic flow), else explicit
+    int visc_if;
 };
 
 // Scalars of the running step kept in device memory so that a whole step can

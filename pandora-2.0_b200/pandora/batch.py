@@ -25,7 +25,7 @@ def class_key(p: Params) -> tuple:
     """The parameters that put two simulations in the same batch class."""
     npart = int(p.p_np_global) if p.p_track_part else 0
     return (p.nodes_x, p.nodes_y, p.nodes_z, p.precision, p.f_type, p.ns_deformed, p.b110, p.b220, p.b330,
-            p.dealiasing, p.les_cutoff, npart, p.p_interp_order if npart else 0, float(p.force_kf))
+            p.dealiasing, p.les_cutoff, p.rk3_viscous, npart, p.p_interp_order if npart else 0, float(p.force_kf))
 
 
 def batch_bytes(p: Params, capacity: int) -> int:

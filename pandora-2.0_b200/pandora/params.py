@@ -28,6 +28,8 @@ F_INIT_AHMED_ELGHOBASHI = 10
 P_INIT_RANDOM = 2
 PREC_FP64 = 0
 PREC_FP32_MIXED = 1   # FP32 fields and transforms, FP64 bookkeeping (include/pandora_gpu.h)
+VISCOUS_EXPLICIT = 0  # the reference's -F_NU k^2 u in every stage's right-hand side
+VISCOUS_INTEGRATING_FACTOR = 1   # exp(-F_NU k^2 dc dt) factors per stage (include/pandora_gpu.h)
 
 
 class Params(ctypes.Structure):
@@ -61,7 +63,7 @@ class Params(ctypes.Structure):
         ("seed_fluid", ctypes.c_uint64), ("seed_force", ctypes.c_uint64),
         ("seed_particles", ctypes.c_uint64),
         ("precision", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("rk3_viscous", ctypes.c_int32),
         ("les_cutoff", ctypes.c_double),
         ("reserved", ctypes.c_int32 * 4),
     ]

@@ -264,6 +264,14 @@ class Simulation:
     def nonlinear(self):
         return self._get3(self.L.pandora_nonlinear, self.shape, "pandora_nonlinear")
 
+    def device_state_ptrs(self):
+        """Device addresses of u1..u3 (zero-copy): S complex values each, double2 in the
+        FP64 form and float2 in the FP32-mixed form, valid until ``close``."""
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(self.L.pandora_state_device_ptrs(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                   "pandora_state_device_ptrs")
+        return a.value, b.value, c.value
+
     def physical_velocity(self):
         p = self.p
         out = [np.zeros((p.nodes_z, p.nodes_y, p.nodes_x)) for _ in range(3)]

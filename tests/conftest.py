@@ -11,6 +11,7 @@ for p in (os.path.join(ROOT, "pandora-2.0_b200"), os.path.join(ROOT, "oracle"), 
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA library")
+    config.addinivalue_line("markers", "slow: parity at the benchmark configurations' full sizes (minutes)")
 
 
 @pytest.fixture(scope="session")

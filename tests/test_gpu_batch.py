@@ -158,3 +158,24 @@ def test_batch_many_outstanding_tickets(gpu_lib):
             s.set_state(u)
             ek2, tke2, eps2, _ = s.stats()
         assert tke == pytest.approx(tke2, rel=1e-12) and eps == pytest.approx(eps2, rel=1e-12)
+
+
+def test_batch_integrating_factor_class(gpu_lib):
+    """Members in the integrating-factor form run in a batch of their own class (one
+    update kernel per launch) and equal their runs alone; an explicit member is refused."""
+    base = gpu_lib.workload_params("iso_decay", 32)
+    base.rk3_viscous = gpu_lib.VISCOUS_INTEGRATING_FACTOR
+    a, b = _member(base, 51), _member(base, 52, 0.02)
+    with gpu_lib.Batch(base, 2) as bt:
+        sa = bt.admit(a)
+        bt.step(2)
+        sb = bt.admit(b)
+        bt.step(3)
+        bt.sync()
+        assert _same(bt.get_state(sa), _alone(gpu_lib, a, 5)[0])
+        assert _same(bt.get_state(sb), _alone(gpu_lib, b, 3)[0])
+    ex = _member(base, 53)
+    ex.rk3_viscous = gpu_lib.VISCOUS_EXPLICIT
+    with gpu_lib.Batch(base, 1) as bt:
+        with pytest.raises(gpu_lib.PandoraError):
+            bt.admit(ex)

@@ -433,3 +433,64 @@ def test_x_correlation_parity(gpu_lib, case):
         assert d["r1i"][0] == pytest.approx(1.0, rel=1e-6 if case == "fp32" else 1e-12)
     s.close()
 
+
+
+@pytest.mark.parametrize("workload,n", [("iso_decay", 64), ("iso_forced_particles", 32)])
+def test_integrating_factor_parity(gpu_lib, workload, n):
+    """PANDORA_VISCOUS_INTEGRATING_FACTOR against the oracle's same mode: u, the RK
+    register and (forced case) the tracers after 1 and 10 steps; the explicit form of the
+    same run differs from it by the scheme's O(dt^3) local error, not by round-off."""
+    p = gpu_lib.workload_params(workload, n)
+    p.rk3_viscous = gpu_lib.VISCOUS_INTEGRATING_FACTOR
+    if p.p_track_part:
+        p.p_np_global = 2048
+    o, s = _pair(gpu_lib, p, init="gpu")
+    if p.p_track_part:
+        s.init_particles()
+        o.set_particles(*s.get_particles())
+    q = p.copy()
+    q.rk3_viscous = gpu_lib.VISCOUS_EXPLICIT
+    with gpu_lib.Simulation(q) as x:
+        x.set_state(s.get_state())
+        if p.p_track_part:
+            x.set_particles(*s.get_particles())
+        t = 0.0
+        for step in range(1, 11):
+            t, dt = o.step(step, t)
+            assert s.step(step) == dt
+            x.step(step)
+            if step in (1, 10):
+                assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10, step
+                assert rel_l2_fields(s.get_rk(), o.get_rk()) < 1e-10, step
+        dev = rel_l2_fields(x.get_state(), s.get_state())
+    assert 1e-12 < dev < 1e-4, dev
+    if p.p_track_part:
+        xg = s.get_particles()[0]
+        xo = o.get_particles(p.p_np_global)[0]
+        d = np.abs(xg - xo)
+        assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
+    s.close()
+
+
+def test_integrating_factor_mixed_and_shear_refused(gpu_lib):
+    """The FP32-mixed form of the integrating factor against the FP64 oracle (1e-5), and
+    the sheared flow refused (its wavenumbers move with the frame)."""
+    import oracle as O
+    p = gpu_lib.workload_params("iso_decay", 32)
+    p.rk3_viscous = gpu_lib.VISCOUS_INTEGRATING_FACTOR
+    o = O.Oracle(p)
+    o.init_fluid()
+    q = p.copy()
+    q.precision = gpu_lib.PREC_FP32_MIXED
+    with gpu_lib.Simulation(q) as s:
+        s.set_state(o.get_state())
+        t = 0.0
+        for step in range(1, 6):
+            t, _ = o.step(step, t)
+            s.step(step)
+        assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-5
+    r = gpu_lib.workload_params("shear", 32)
+    r.rk3_viscous = gpu_lib.VISCOUS_INTEGRATING_FACTOR
+    with pytest.raises(gpu_lib.PandoraError) as ei:
+        gpu_lib.Simulation(r)
+    assert ei.value.status == -10

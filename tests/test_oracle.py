@@ -106,6 +106,61 @@ def test_single_mode_viscous_decay_is_rk3_polynomial():
     assert max(np.abs(c).max() for c in (v[0], v[2])) < 1e-17
 
 
+def test_integrating_factor_single_mode_decays_exactly():
+    """The integrating-factor form integrates the viscous term exactly: a single mode
+    (whose projected nonlinear term is zero) decays by exp(-nu k^2 dt) per step, for any
+    dt, where the explicit form gives the RK3 polynomial."""
+    from pandora.params import default_params, RK3_TIMESTEP_FIXED, VISCOUS_INTEGRATING_FACTOR
+    for dt in (0.01, 0.5):
+        p = default_params(16)
+        p.f_nu, p.rk3_timestep, p.rk3_dt, p.force_stop = 0.05, RK3_TIMESTEP_FIXED, dt, 0
+        p.rk3_viscous = VISCOUS_INTEGRATING_FACTOR
+        o = _o(p)
+        u = [np.zeros(o.shape, complex) for _ in range(3)]
+        u[1][2, 0, 1] = 0.5 + 0.1j
+        o.set_state(u)
+        t = 0.0
+        for s in (1, 2):
+            t, _ = o.step(s, t)
+        want = (0.5 + 0.1j) * np.exp(-p.f_nu * 5 * 2 * dt)
+        v = o.get_state()
+        assert abs(v[1][2, 0, 1] - want) < 2e-16, dt
+        assert max(np.abs(c).max() for c in (v[0], v[2])) < 1e-17
+
+
+def test_integrating_factor_agrees_with_explicit_to_third_order():
+    """Both forms are third order in dt: on the same turbulent field over the same time,
+    halving dt divides their difference by about 8."""
+    from pandora.params import workload_params, VISCOUS_INTEGRATING_FACTOR
+    diffs = []
+    for dt, nsteps in ((0.01, 4), (0.005, 8)):
+        out = []
+        for visc in (0, VISCOUS_INTEGRATING_FACTOR):
+            p = workload_params("iso_decay", 16)
+            p.rk3_dt, p.rk3_viscous = dt, visc
+            o = _o(p)
+            o.init_fluid()
+            t = 0.0
+            for s in range(1, nsteps + 1):
+                t, _ = o.step(s, t)
+            out.append(o.get_state())
+            assert np.abs(divergence(p, out[-1])).max() < 1e-16
+        diffs.append(rel_l2_fields(out[1], out[0]))
+    assert 0 < diffs[1] < diffs[0] < 1e-5
+    assert 6.0 < diffs[0] / diffs[1] < 10.0, diffs
+
+
+def test_integrating_factor_isotropic_only():
+    from pandora.params import workload_params, VISCOUS_INTEGRATING_FACTOR
+    p = workload_params("shear", 16)
+    p.p_track_part = 0
+    p.rk3_viscous = VISCOUS_INTEGRATING_FACTOR
+    o = _o(p)
+    o.init_fluid()
+    with pytest.raises(RuntimeError):
+        o.step(1, 0.0)
+
+
 def test_step_invariants_and_fixture_decay():
     from pandora.params import workload_params
     g = np.load(os.path.join(HERE, "golden", "iso_decay_16_3.npz"))
