@@ -1277,7 +1277,10 @@ static void particles_stage(oracle* o, int stage, int tstep, double dt) {
         double* ur = o->uprk + 3 * n;
         double* pr = o->prk + 3 * n;
         double uf[3];
-        if (o->shear) {
+        /* the R forms: p_RK3SolveParticleR (src/pp_rk3.f90:307-403, dispatched at
+         * src/pp_control.f90:568-571) and p_ControlInitPartVelocityR (418-463) are the
+         * isotropic arithmetic on the laboratory components of the sheared grid */
+        if (o->shear && !o->rrot) {
             /* p_RK3SolveParticleBF (src/pp_rk3.f90:169-303): RK3 in the lab frame,
              * p_RK3Mov2Lab / p_RK3Lab2Mov (src/pp_rk3.f90:989-1042) */
             double ufm[3], xl[3] = {0, 0, 0}, ul[3] = {0, 0, 0};

@@ -172,7 +172,12 @@ __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ Me
 #pragma unroll
     for (int c = 0; c < 3; c++) { up[c] = P.up[c][nn]; ur[c] = P.uprk[c][nn]; pr[c] = P.prk[c][nn]; }
     double xw[3] = {xp[0], xp[1], xp[2]};   // frame in which the RK3 update runs
-    if (g.shear) {
+    // BF-rot shear transforms to the laboratory frame and back; the R forms
+    // (p_RK3SolveParticleR, src/pp_rk3.f90:307-403, dispatched at src/pp_control.f90:
+    // 568-571) interpolate laboratory components and advance the moving position with
+    // them directly, the isotropic arithmetic
+    const bool bfrot = g.shear && !g.rrot;
+    if (bfrot) {
         // p_RK3SolveParticleBF (src/pp_rk3.f90:169-303): velocity and position to
         // the laboratory frame (p_RK3Mov2Lab, src/pp_rk3.f90:989-1014), RK3 there,
         // back with p_RK3Lab2Mov (1016-1042) at the same B.
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ Me
         const double tau = ((dpv * dpv) / (18.0 * pp.f_nu)) * (pp.p_rho / pp.f_rho);
         // shear: minus the homogeneous source amat up (p_RK3ComputeHomogeneousSourceTerm,
         // src/pp_rk3.f90:1080-1102); amat has the single entry (1,3)
-        const double hs0 = g.shear ? g.shear_s * up[2] : 0.0;
+        const double hs0 = bfrot ? g.shear_s * up[2] : 0.0;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const double acc = ((uf[c] - up[c]) / tau) - (c == 0 ? hs0 : 0.0);
@@ -212,7 +217,7 @@ __global__ void __launch_bounds__(256, 2) k_particles(const __grid_constant__ Me
         ur[c] = (beta * ur[c]) + up[c];
         xw[c] = xw[c] + (gamma * dt * ur[c]);
     }
-    if (g.shear) {
+    if (bfrot) {
         const BF bf = make_bf(g, ck);
 #pragma unroll
         for (int a = 0; a < 3; a++) {

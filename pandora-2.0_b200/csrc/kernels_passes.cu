@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
 // bmat(d,j) u_j, then the forward transforms and split of K3.  One warp per line
 // over four arrays: the pairs (u1,u2) and (u3, du1/dx1) first; v and the partial sums
 // then stay in the arrays that the later pairs do not use, which are transformed two
-// and then one at a time.  Single simulations only.
+// and then one at a time.  Optionally writes the physical velocity (laboratory
+// components) for the particles.  Batches: the member is blockIdx.y, as in K3.
 // ---------------------------------------------------------------------------
 template <int N, class T> struct ConvCfg {
     static constexpr int per_warp = 4 * xas<N>() * (int)sizeof(typename Cplx<T>::type);
@@ -348,13 +349,16 @@ template <int N, class T> struct ConvCfg {
     static constexpr size_t smem = (size_t)NW * per_warp;
 };
 
-template <int NX, class T>
-__global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const __grid_constant__ MemberSet<T, 1> ms,
-                                                                          int want_cfl, long long pf_lines) {
+template <int NX, class T, int CAP>
+__global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const __grid_constant__ MemberSet<T, CAP> ms,
+                                                                          int want_phys, int want_cfl, long long pf_lines) {
     using C = typename FieldsT<T>::C;
     using XP = pdfft::FusedPlan<NX>;   // the backward plan r0, r1, r2 (run unfused here)
-    const Member<T>& mm = ms.m[0];
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
     if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>(), NW = ConvCfg<NX, T>::NW;
@@ -401,6 +405,11 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         C* e = s + prow<XPS>(n);
         const C a = e[0], c1 = e[XAS];
         const T u[3] = {a.x, a.y, c1.x};
+        if (want_phys) {
+            F.phys[q * NX + n] = u[0];
+            F.phys[g.R + q * NX + n] = u[1];
+            F.phys[2 * g.R + q * NX + n] = u[2];
+        }
         if (want_cfl) umax = fmax(umax, fabs(u[0]) + fabs(u[1]) + fabs(u[2]));
         T v[3];
 #pragma unroll
@@ -761,12 +770,12 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
 }
 
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
-// [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).  Six fields, or
-// nine in the R-conv form (single simulations).
+// [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).  nf = six fields, or
+// nine in the R-conv form, per member.
 template <int NY, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms) {
+__global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms,
+                                                                                                          int nf) {
     using C = typename FieldsT<T>::C;
-    const int nf = CAP == 1 ? pass_fields(ms.m[0].g) : 6;   // batches: no R-conv members
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / nf];
     if (!mm.active) return;
     if constexpr (CAP > 1) {   // a batch slot between members
@@ -900,9 +909,7 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
         if ((e = set_smem(k_zpass_inv<N, 0, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
         if ((e = set_smem(k_zpass_inv<N, 1, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
         if ((e = set_smem(k_zpass_inv<N, 2, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
-        if constexpr (CAP == 1) {                                                              \
-            if ((e = set_smem(k_zpass_inv<N, 3, T, CAP>, TCfg<N>::template smem<T>()))) return e; \
-        }                                                                                      \
+        if ((e = set_smem(k_zpass_inv<N, 3, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
         if ((e = set_smem(k_zpass_fwd<N, T, CAP>, TCfg<N, true>::template smem<T>()))) return e;        \
     }                                                                                          \
     if (g.ny == N) {                                                                           \
@@ -911,9 +918,7 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
     }                                                                                          \
     if (g.nx == N) {                                                                           \
         if ((e = set_smem(k_xpass<N, T, CAP>, smem_kx<N, T>()))) return e;                     \
-        if constexpr (CAP == 1) {                                                              \
-            if (g.rconv && (e = set_smem(k_xpass_conv<N, T>, ConvCfg<N, T>::smem))) return e;  \
-        }                                                                                      \
+        if (g.rconv && (e = set_smem(k_xpass_conv<N, T, CAP>, ConvCfg<N, T>::smem))) return e;    \
     }
 #define PD_CFG(N)                                                                              \
     PD_CFG1(N, 1)                                                                              \
@@ -954,7 +959,7 @@ cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage,
                 if (!g.shear) go(k_zpass_inv<N, 0, T, CAP>);                                      \
                 else if (!g.rrot) go(k_zpass_inv<N, 1, T, CAP>);                                  \
                 else if (!g.rconv) go(k_zpass_inv<N, 2, T, CAP>);                                 \
-                else if constexpr (CAP == 1) go(k_zpass_inv<N, 3, T, CAP>);                       \
+                else go(k_zpass_inv<N, 3, T, CAP>);                                               \
             }                                                                                     \
         });
         PD_FOR_EACH_N(PD_L)
@@ -970,7 +975,7 @@ template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
             if constexpr (CAP == 1 || batch_len<N>())                                             \
-                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, pass_fields(g) * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms); \
+                k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, pass_fields(g) * nb), TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms, pass_fields(g)); \
         });
         PD_FOR_EACH_N(PD_L)
 #undef PD_L
@@ -986,12 +991,12 @@ cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys,
     case N:                                                                                       \
         return for_member_sets(M, B, [&](const auto& ms, int nb) {                                \
             constexpr int CAP = PD_CAP(ms);                                                       \
-            if constexpr (CAP == 1) {                                                             \
-                if (g.rconv) {   /* R-conv: its own x pass, single simulations */                \
+            if constexpr (CAP == 1 || batch_len<N>()) {                                           \
+                if (g.rconv) {   /* R-conv: its own x pass */                                     \
                     constexpr int NW = ConvCfg<N, T>::NW;                                         \
                     const long long nl = (lines + NW - 1) / NW;                                   \
-                    const long long pf = NW * resident_ctas(k_xpass_conv<N, T>, 32 * NW, ConvCfg<N, T>::smem); \
-                    k_xpass_conv<N, T><<<dim3((unsigned)nl), 32 * NW, ConvCfg<N, T>::smem, st>>>(ms, want_cfl, pf); \
+                    const long long pf = CAP == 1 ? NW * resident_ctas(k_xpass_conv<N, T, CAP>, 32 * NW, ConvCfg<N, T>::smem) : 0; \
+                    k_xpass_conv<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * NW, ConvCfg<N, T>::smem, st>>>(ms, want_phys, want_cfl, pf); \
                     return;                                                                       \
                 }                                                                                 \
             }                                                                                     \

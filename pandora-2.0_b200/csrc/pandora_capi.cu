@@ -201,8 +201,6 @@ static int validate(const pandora_params* p) {
         if (p->ns_deformed != PANDORA_NS_BF_ROT && p->ns_deformed != PANDORA_NS_R_ROT &&
             p->ns_deformed != PANDORA_NS_R_CONV)
             return PANDORA_ERR_UNSUPPORTED;
-        // the R-form particle routines (p_RK3SolveParticleR, src/pp_control.f90:563-568) are not built
-        if (p->ns_deformed != PANDORA_NS_BF_ROT && p->p_track_part) return PANDORA_ERR_UNSUPPORTED;
         if (p->b110 < 1 || p->b220 < 1 || p->b330 < 1 || p->f_deform_s == 0.0 || p->f_remesh_t < 1)
             return PANDORA_ERR_INVALID_ARG;
     }
@@ -1301,8 +1299,6 @@ extern "C" int pandora_batch_create(const pandora_params* cls, int32_t capacity,
     *out = nullptr;
     int rc = validate(cls);
     if (rc) return rc;
-    // the R-conv x pass has single-simulation instantiations only
-    if (cls->f_type == PANDORA_F_SHEAR_DNS && cls->ns_deformed == PANDORA_NS_R_CONV) return PANDORA_ERR_UNSUPPORTED;
     pandora_batch* b = new (std::nothrow) pandora_batch();
     if (!b) return PANDORA_ERR_OOM;
     cudaGetDevice(&b->dev);

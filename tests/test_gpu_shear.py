@@ -1,5 +1,5 @@
-"""Homogeneous shear (Rogallo moving frame, BF-rot formulation) on the GPU
-against the oracle, through the C-ABI: state, statistics in the laboratory
+"""Homogeneous shear (Rogallo moving frame: the BF-rot, R-rot and R-conv forms) on the
+GPU against the oracle, through the C-ABI: state, statistics in the laboratory
 frame, frame tensors and particles, across a remesh."""
 import numpy as np
 import pytest
@@ -115,19 +115,65 @@ def test_rconv_nonlinear_every_length(gpu_lib, dims):
 
 
 @pytest.mark.parametrize("form", [2, 3])
-def test_rogallo_with_particles_unsupported(gpu_lib, form):
-    p = _shear(gpu_lib, 32, remesh_t=5, npart=256)
+def test_rogallo_particles_across_remesh(gpu_lib, form):
+    """Tracers in the R forms (p_RK3SolveParticleR, src/pp_rk3.f90:307-403): the
+    laboratory components of the sheared grid interpolated at the moving position, the
+    isotropic RK3 arithmetic, and x1 += x3 at the remesh (step 9 here); positions, the
+    state and the particle velocities against the oracle after 12 steps."""
+    import oracle as O
+    p = _shear(gpu_lib, 32, remesh_t=4, npart=2048)
     p.ns_deformed = form
-    with pytest.raises(gpu_lib.PandoraError):
-        gpu_lib.Simulation(p)
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    s.init_particles()
+    o.set_state(s.get_state())
+    o.set_particles(*s.get_particles())
+    t = 0.0
+    for step in range(1, 13):
+        t, _ = o.step(step, t)
+        s.step(step)
+    assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10
+    xg, ug = s.get_particles()[:2]
+    xo, uo = o.get_particles(p.p_np_global)[:2]
+    d = np.abs(xg - xo)
+    assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
+    assert rel_l2(ug, uo) < 1e-10
+    # the physical field the particles read is the laboratory velocity of the last stage
+    assert rel_l2_fields(s.physical_velocity(), o.get_physical()) < 1e-12
+    s.check_status()
+    s.close()
 
 
-def test_rconv_single_simulations_only(gpu_lib):
-    """R-conv has no batched x pass: a batch of R-conv members is refused."""
-    p = _shear(gpu_lib, 32, remesh_t=5)
+def test_rconv_batch_members_equal_alone_runs(gpu_lib):
+    """R-conv members in a batch (the batched four-array x pass and nine-field K1/K2),
+    one admitted mid-run, with tracers: each equals its run alone bit for bit."""
+    p = _shear(gpu_lib, 32, remesh_t=4, npart=256)
     p.ns_deformed = gpu_lib.NS_R_CONV
-    with pytest.raises(gpu_lib.PandoraError):
-        gpu_lib.Batch(p, 2)
+
+    def member(seed):
+        q = p.copy()
+        q.seed_fluid, q.seed_particles = seed, 500 + seed
+        return q
+
+    def alone(q, n):
+        with gpu_lib.Simulation(q) as s:
+            s.init_fluid()
+            s.init_particles()
+            for k in range(1, n + 1):
+                s.step(k)
+            return s.get_state(), s.get_particles()[0]
+
+    with gpu_lib.Batch(p, 2) as b:
+        s0 = b.admit(member(61))
+        b.step(3)
+        s1 = b.admit(member(62))
+        b.step(8)                       # the first member crosses its remesh at step 9
+        b.sync()
+        for slot, seed, n in ((s0, 61, 11), (s1, 62, 8)):
+            u, xp = alone(member(seed), n)
+            assert all(np.array_equal(x, y) for x, y in zip(b.get_state(slot), u)), seed
+            assert np.array_equal(b.get_particles(slot)[0], xp), seed
 
 
 def test_shear_particles(gpu_lib):
