@@ -32,11 +32,19 @@ sys.path.insert(0, os.path.join(ROOT, "pandora-2.0_b200"))
 
 METRIC = "Mpts·RK3steps/s"
 WORKLOAD = "shear"
-# DRAM traffic (read + write bytes) of one launch of a pass, from single-kernel ncu
-# captures of these workloads: (workload, N, form, pass) -> bytes.  The captures and
-# their commands are summarised under profiles/.
+# DRAM traffic (read + write bytes) of one launch of a pass in stages 2-3, from ncu
+# captures of dram__bytes_read.sum + dram__bytes_write.sum: (workload, N, form) -> pass ->
+# bytes.  256^3: captured at full size.  512^3: each 512-point pass captured on a case
+# whose other two axes are 128 points (512x128x128, 128x512x128, 128x128x512, tracers at
+# the same density) and scaled to the full grid by the ratio of algorithmic bytes; the
+# commands and the raw figures are summarised under profiles/.
 NCU_TRAFFIC_BYTES = {
-    ("iso_forced_particles", 256, "fp64_plain", "xpass_nl"): 553719296 + 627172608,
+    ("iso_forced_particles", 256, "fp64_plain"): {
+        "zpass_inv": 432157440, "ypass_inv": 862682752, "xpass_nl": 1177856256, "ypass_fwd": 417905024,
+        "zpass_fwd_update": 261682560 + 549060736, "particles": 605924864},
+    ("shear", 512, "fp64_plain"): {
+        "zpass_inv": 3199086129, "ypass_inv": 7047367930, "xpass_nl": 8904337408, "ypass_fwd": 3324333151,
+        "zpass_fwd_update": 1928149719 + 3921155948, "particles": 1473873920},
 }
 # Seconds of host work the reference arm spends on its timed steps at most (the
 # whole arm, warm-up and set-up included, stays within a few minutes).
@@ -402,6 +410,10 @@ def run_ours(a, p):
         dur = q0.elapsed_time(q1) / reps / 1e3
         b = sim.pass_bytes(pid)
         per_pass[name] = {"ms": dur * 1e3, "gbs": b / dur / 1e9, "bytes": b}
+    traffic = NCU_TRAFFIC_BYTES.get((a.workload, p.nodes_x, form_key(p)), {})
+    for name, v in per_pass.items():
+        if name in traffic:
+            v["traffic_over_alg"] = traffic[name] / v["bytes"]
     src = per_pass_live if per_pass_live else per_pass
     dom = passes[dom_pid] if passes[dom_pid] in src else max(src, key=lambda k: src[k]["ms"])
     dom_gbs = src[dom]["gbs"]
@@ -410,9 +422,13 @@ def run_ours(a, p):
                 "timed": ("dominant pass (of those with the GPU to themselves): event pair in the step graph, stages 2-3 of the last timed step; "
                           "other passes: the same in the last warm-up step") if per_pass_live
                          else "alone, 20 back-to-back launches",
-                "traffic": NCU_TRAFFIC_BYTES.get((a.workload, p.nodes_x, form_key(p), dom)),
+                "traffic": traffic.get(dom),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch (table in bench.py)"
+                                  if traffic else None,
                 "per_pass": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)} for k, v in src.items()},
-                "per_pass_alone": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)}
+                "per_pass_alone": {k: {"ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1),
+                                       **({"traffic/alg": round(v["traffic_over_alg"], 3)}
+                                          if "traffic_over_alg" in v else {})}
                                    for k, v in per_pass.items()}}
     launches = sim.launches_per_step()
     value = npts * a.steps * ws / (ms / 1e3) / 1e6

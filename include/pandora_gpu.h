@@ -268,7 +268,8 @@ int pandora_launches_per_step(pandora_handle* h, int32_t* n);
  * advance the state; use only on a scratch simulation. */
 int pandora_profile_pass(pandora_handle* h, int32_t pass, int32_t reps);
 /* Algorithmic HBM bytes of one launch of `pass` (each input read once, each
- * output written once, at the stored, unpadded extents). */
+ * output written once, at the stored, unpadded extents; for the particles the field
+ * values their stencils need, at most the whole field, and their state). */
 int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes);
 
 /* Instrumentation (no counterpart in the reference): every step records a CUDA

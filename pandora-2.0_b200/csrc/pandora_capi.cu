@@ -1115,7 +1115,11 @@ extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes
     case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? r8 * 3 * R : 0.0); break;
     case 4: *bytes = c16 * (3 * Y + 3 * Z); break;
     case 5: *bytes = c16 * (3 * Z + 3 * S) + c16 * (3 * S + 6 * S + 6 * S); break;   // K5a + K5b
-    case 6: *bytes = part ? r8 * 3 * R + 8.0 * 24.0 * (double)h->P.np : 0.0; break;
+    case 6: {   // the field values the stencils need (each read once at most) and the particle state
+        const double ord = (double)h->pp.order, np = (double)h->P.np;
+        *bytes = part ? r8 * 3 * std::min(R, np * ord * ord * ord) + 8.0 * 24.0 * np : 0.0;
+        break;
+    }
     case 7: *bytes = c16 * 3 * S; break;
     default: return PANDORA_ERR_INVALID_ARG;
     }
