@@ -341,10 +341,9 @@ def run_ours(a, p):
     sim.set_pass_timing(0x3F)
     sim.advance(max(a.warmup, 3), sync=True)
     warm = sim.pass_times()
-    # the dominant pass among those that have the GPU to themselves: with particles,
-    # K4 and K5 share it with the particle branch on the second stream, so their event
-    # pairs time both branches
-    solo = [1, 2, 3] if (p.p_track_part and p.p_np_global > 0) else [1, 2, 3, 4, 5]
+    # the dominant pass; its event pairs of stages 2 and 3 time it with the GPU to itself
+    # (the only second-stream work, the particle sort, runs beside stage 1)
+    solo = [1, 2, 3, 4, 5]
     dom_pid = max(solo, key=lambda q: warm[1:, q - 1].mean())
     sim.set_pass_timing(1 << (dom_pid - 1))
     sim.advance(3, sync=True)

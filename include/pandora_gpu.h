@@ -274,7 +274,7 @@ int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes);
 
 /* Instrumentation (no counterpart in the reference): every step records a CUDA
  * event pair around each pass p whose bit p-1 is set in `passes` (passes 1..6 as
- * in pandora_profile_pass; pass 6 on the particle stream), in each stage, inside
+ * in pandora_profile_pass), in each stage, inside
  * the step graph; passes = 0 turns it off.  pandora_pass_times waits for the
  * handle's stream and writes the durations of the most recent step,
  * ms[(stage-1)*6 + pass-1] in milliseconds (-1 where a pass was not timed). */

@@ -769,6 +769,155 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template
     TCfg<NZ>::template transform<+1, LT>(s, F.tw_z, ld, st, mid);
 }
 
+// ---------------------------------------------------------------------------
+// K1 with the velocity rows staged by the tensor-memory accelerator (FP64, single
+// simulations, z lines of ZStage<NZ>::enabled lengths).  One CTA per tile (8
+// consecutive i at one j) forms every field of the tile: the rows
+// u_c[i0..i0+7][j][0..NKK-1] of the three components arrive in shared memory by 3 x NB
+// tensor copies (cp.async.bulk.tensor, boxes of BK k x 1 j x 8 i, completion counted on
+// one mbarrier; rows past NKI and k past NKK are filled with zeros by the copy engine).
+// Each field's backward z transform then takes its first-pass inputs from that staging
+// (velocity, or vorticity / gradients formed on the fly) instead of from global memory,
+// and stores z rows of 8 i as K1 does.  u is read from HBM once per tile, in whole rows,
+// instead of element-wise by each field's CTA.
+// ---------------------------------------------------------------------------
+template <int NZ> struct ZStage {
+    static constexpr int NKK = 2 * (NZ / 3) + 1;
+    static constexpr int NB = (NKK + 127) / 128;                 // boxes along k (<= 128 complex each)
+    static constexpr int BK0 = (NKK + NB - 1) / NB;
+    static constexpr int BK = BK0 + (9 - BK0 % 8) % 8;           // = 1 mod 8: the 8 rows of a box on distinct banks
+    static_assert(BK <= 128, "tensor box wider than 256 doubles");
+    static constexpr int words = 3 * NB * 8 * BK;                // staged complex values
+    static constexpr size_t smem = sizeof(double2) * words + TCfg<NZ>::template smem<double>() + 16;
+    // measured at 512 only (one CTA of 512 threads per SM): as fast as the element-wise K1
+    // at 512^3, with u read from HBM once per tile in whole rows
+    static constexpr bool enabled = NZ == 512;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Wait for phase `parity` of the mbarrier for at most `limit` SM clocks.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > limit) return false;
+    return true;
+}
+
+template <int NZ, int FORM>
+__global__ void __launch_bounds__(TCfg<NZ>::template nt<double>(), 1) k_zpass_inv_tma(const __grid_constant__ MemberSet<double, 1> ms,
+                                                                                     const __grid_constant__ ZMaps maps,
+                                                                                     int stage) {
+    using C = double2;
+    using ZS = ZStage<NZ>;
+    constexpr int LT = 8, BK = ZS::BK, NB = ZS::NB;
+    constexpr int nf = FORM == 3 ? 9 : 6;
+    const Member<double>& mm = ms.m[0];
+    if (!mm.active) return;
+    const Fields F = mm.F;
+    const Geo g = mm.g;
+    C* stg = smem_as<C>();
+    C* s = stg + ZS::words;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(s + NZ * LT);
+    const int i0 = blockIdx.x * LT, j = blockIdx.y, tid = threadIdx.x;
+    if (stage == 1 && blockIdx.x == 0 && j == 0 && tid == 0) F.clock->ucfl_bits = 0ull;
+    const uint32_t ba = smem_u32(bar);
+    // tensor copies land on 128-byte boundaries: each box is 128 BK bytes from a staging
+    // base that must itself be aligned (the dynamic shared memory of this kernel, which has
+    // no static shared memory); otherwise no copy is issued and the status records it
+    if (smem_u32(stg) & 127u) {
+        if (tid == 0) atomicOr(&F.clock->status, PD_ST_TIMEOUT);
+        return;
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ba) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        constexpr uint32_t bytes = (uint32_t)(sizeof(C) * ZS::words);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ba), "r"(bytes) : "memory");
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(stg + (c * NB + b) * 8 * BK)),
+                    "l"(reinterpret_cast<uint64_t>(&maps.u[c])), "r"(2 * b * BK), "r"(j), "r"(i0), "r"(ba)
+                    : "memory");
+    }
+    // bounded wait (about 2 s of SM clocks); on a timeout the status word records it and,
+    // after a second bounded wait for the copies in flight, the CTA returns
+    constexpr long long kLimit = 4000000000ll;
+    if (!mbar_wait_bounded(ba, 0, kLimit)) {
+        if (tid == 0) atomicOr(&F.clock->status, PD_ST_TIMEOUT);
+        mbar_wait_bounded(ba, 0, kLimit);
+        return;
+    }
+    const int KK = g.kk;
+    const double k2 = wvn(j, g.kj);
+    BF bf;
+    if constexpr (FORM == 1 || FORM == 2) bf = make_bf(g, F.clock);
+    // staged value of component c at (line l, k)
+    auto su = [&](int c, int l, int k) -> C {
+        const int b = k / BK;
+        return stg[((c * NB + b) * 8 + l) * BK + (k - b * BK)];
+    };
+    const long long zs = (long long)g.nkj * g.nkip;
+#pragma unroll 1
+    for (int f = 0; f < nf; f++) {
+        auto ld = [&](int z, int l) -> C {
+            int k;
+            if (z <= KK) k = z;
+            else if (z >= NZ - KK) k = z - NZ + (2 * KK + 1);
+            else return mk(0.0, 0.0);
+            if constexpr (FORM == 3) {   // u_c, i k2 u_c, i k3 u_c (f_RK3Derivative, src/pf_rk3.f90:3735-3743)
+                const int c = f % 3;
+                const C uc = su(c, l, k);
+                if (f < 3) return uc;
+                const double kd = f < 6 ? k2 : wvn(k, KK);
+                return mk(-kd * uc.y, kd * uc.x);
+            } else {
+                if (f < 3) return su(f, l, k);
+                const double k1 = (double)(i0 + l), k3 = wvn(k, KK);
+                if constexpr (FORM == 1 || FORM == 2) {
+                    const double kv[3] = {k1, k2, k3};
+                    const C zero = mk(0.0, 0.0);
+                    const C uv[3] = {f != 3 ? su(0, l, k) : zero, f != 4 ? su(1, l, k) : zero, su(2, l, k)};
+                    C w3[3];
+                    if constexpr (FORM == 2) {
+                        if (f == 3) vort_rrot<0>(bf, uv, kv, w3);
+                        else if (f == 4) vort_rrot<1>(bf, uv, kv, w3);
+                        else vort_rrot<2>(bf, uv, kv, w3);
+                    } else {
+                        if (f == 3) vort_bf<0>(bf, uv, kv, w3);
+                        else if (f == 4) vort_bf<1>(bf, uv, kv, w3);
+                        else vort_bf<2>(bf, uv, kv, w3);
+                    }
+                    return f == 3 ? w3[0] : (f == 4 ? w3[1] : w3[2]);
+                } else {   // omega = i k x u (f_RK3PrepareVelocity, src/pf_rk3.f90:402-407,520-525,630-634)
+                    const double ka = (f == 3) ? k2 : ((f == 4) ? k3 : k1);
+                    const double kb = (f == 3) ? k3 : ((f == 4) ? k1 : k2);
+                    const int ca = (f == 3) ? 2 : ((f == 4) ? 0 : 1), cb = (f == 3) ? 1 : ((f == 4) ? 2 : 0);
+                    const C a = su(ca, l, k), bb = su(cb, l, k);
+                    return mk((-ka * a.y) - (-kb * bb.y), (ka * a.x) - (kb * bb.x));
+                }
+            }
+        };
+        C* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
+        auto st = [&](int z, int l, C v) { dst[z * zs + l] = v; };
+        TCfg<NZ>::template transform<+1, LT>(s, F.tw_z, ld, st);
+        __syncthreads();   // the tile buffer is read by the last pass before the next field's first pass
+    }
+}
+
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
 // [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).  nf = six fields, or
 // nine in the R-conv form, per member.
@@ -904,6 +1053,19 @@ template <int N> constexpr bool batch_len() { return N >= 32 && N <= 256; }
 
 template <class T> cudaError_t configure_kernels(const Geo& g) {
     cudaError_t e = cudaSuccess;
+    if constexpr (std::is_same<T, double>::value) {
+#define PD_CFGZ(N)                                                                                 \
+        if constexpr (ZStage<N>::enabled) {                                                        \
+            if (g.nz == N) {                                                                       \
+                if ((e = set_smem(k_zpass_inv_tma<N, 0>, ZStage<N>::smem))) return e;             \
+                if ((e = set_smem(k_zpass_inv_tma<N, 1>, ZStage<N>::smem))) return e;             \
+                if ((e = set_smem(k_zpass_inv_tma<N, 2>, ZStage<N>::smem))) return e;             \
+                if ((e = set_smem(k_zpass_inv_tma<N, 3>, ZStage<N>::smem))) return e;             \
+            }                                                                                      \
+        }
+        PD_FOR_EACH_N(PD_CFGZ)
+#undef PD_CFGZ
+    }
 #define PD_CFG1(N, CAP)                                                                        \
     if (g.nz == N) {                                                                           \
         if ((e = set_smem(k_zpass_inv<N, 0, T, CAP>, TCfg<N>::template smem<T>()))) return e;   \
@@ -935,13 +1097,36 @@ template <class T> cudaError_t configure_kernels(const Geo& g) {
 #define PD_CAP(S) std::decay_t<decltype(S)>::cap
 
 template <class T>
-cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st) {
+cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st, const ZMaps* maps) {
     // DEALIASING 2/3: f_RK3PrepareRealSpace first zeroes the modes outside the cutoff
     // (src/pf_rk3.f90:269-277): k_dealias writes those zeros (it reads nothing) ahead of
     // K1, whose loads then carry no mask test
     if (g.dealias_cut > 0.0) {
         const cudaError_t e = launch_dealias(g, M, B, st);
         if (e != cudaSuccess) return e;
+    }
+    if constexpr (std::is_same<T, double>::value) {
+        if (maps && B == 1) {
+            switch (g.nz) {
+#define PD_L(N)                                                                                   \
+    case N:                                                                                       \
+        if constexpr (ZStage<N>::enabled) {                                                       \
+            MemberSet<double, 1> one;                                                             \
+            one.m[0] = M[0];                                                                      \
+            const dim3 grid(TCfg<N>::template tiles<double>(g), g.nkj);                           \
+            constexpr int NT = TCfg<N>::template nt<double>();                                    \
+            if (!g.shear) k_zpass_inv_tma<N, 0><<<grid, NT, ZStage<N>::smem, st>>>(one, *maps, stage); \
+            else if (!g.rrot) k_zpass_inv_tma<N, 1><<<grid, NT, ZStage<N>::smem, st>>>(one, *maps, stage); \
+            else if (!g.rconv) k_zpass_inv_tma<N, 2><<<grid, NT, ZStage<N>::smem, st>>>(one, *maps, stage); \
+            else k_zpass_inv_tma<N, 3><<<grid, NT, ZStage<N>::smem, st>>>(one, *maps, stage);      \
+            return cudaGetLastError();                                                            \
+        }                                                                                         \
+        break;
+                PD_FOR_EACH_N(PD_L)
+#undef PD_L
+            default: break;
+            }
+        }
     }
     switch (g.nz) {
 #define PD_L(N)                                                                                   \
@@ -1078,6 +1263,53 @@ cudaError_t launch_zpass_fwd_update(const Geo& g, const Member<T>* M, int B, int
 }
 #undef PD_CAP
 
+// Tensor maps of the staged K1 (host).  The encoder is the driver's
+// cuTensorMapEncodeTiled, looked up through the runtime (no link against libcuda).
+typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                         const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                         CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                         CUtensorMapFloatOOBfill);
+
+cudaError_t make_zmaps(const Geo& g, double2* const* u, ZMaps* out, bool* ok) {
+    *ok = false;
+    int bk = 0;
+    switch (g.nz) {
+#define PD_L(N)                                          \
+    case N:                                              \
+        if constexpr (ZStage<N>::enabled) bk = ZStage<N>::BK; \
+        break;
+        PD_FOR_EACH_N(PD_L)
+#undef PD_L
+    default: break;
+    }
+    if (bk == 0) return cudaSuccess;
+    static TensorMapEncodeTiled encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return cudaSuccess;
+        }
+        encode = (TensorMapEncodeTiled)fn;
+    }
+    // u_c as a 3-D tensor of doubles: dim 0 the 2 NKK reals of a k row, dim 1 j, dim 2 i
+    const cuuint64_t dims[3] = {(cuuint64_t)2 * g.nkk, (cuuint64_t)g.nkj, (cuuint64_t)g.nki};
+    const cuuint64_t strides[2] = {(cuuint64_t)2 * g.nkk * sizeof(double),
+                                   (cuuint64_t)2 * g.nkk * g.nkj * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)(2 * bk), 1u, 8u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    for (int c = 0; c < 3; c++) {
+        if (encode(&out->u[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)u[c], dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaSuccess;
+    }
+    *ok = true;
+    return cudaSuccess;
+}
+
 // conversions at the FP64 boundary of the FP32-mixed form
 __global__ void k_to_f32(const double2* __restrict__ in, float2* __restrict__ out, long long n) {
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
@@ -1102,7 +1334,7 @@ cudaError_t launch_convert(const float2* in, double2* out, long long n, cudaStre
 
 #define PD_INST(T)                                                                                       \
     template cudaError_t configure_kernels<T>(const Geo&);                                               \
-    template cudaError_t launch_zpass_inv<T>(const Geo&, const Member<T>*, int, int, cudaStream_t);      \
+    template cudaError_t launch_zpass_inv<T>(const Geo&, const Member<T>*, int, int, cudaStream_t, const ZMaps*); \
     template cudaError_t launch_ypass_inv<T>(const Geo&, const Member<T>*, int, cudaStream_t);           \
     template cudaError_t launch_xpass<T>(const Geo&, const Member<T>*, int, int, int, cudaStream_t);     \
     template cudaError_t launch_xpass_stats<T>(const Geo&, const Member<T>*, double*, cudaStream_t);    \

@@ -56,6 +56,8 @@ struct pandora_handle {
     bool use_graph = true;
     int launches_per_step = 0;
     bool particles_on = false;
+    ZMaps zmaps{};                    // tensor maps of u for the staged K1 (FP64, z lengths that have it)
+    bool zmaps_ok = false;
 };
 
 static thread_local char g_errmsg[256];
@@ -371,6 +373,9 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     if ((e = configure_fluid_kernels(g, h->fp)) != cudaSuccess) {
         release(h); return cuda_fail(e, "configure_fluid_kernels");
     }
+    if (!h->mixed && (e = make_zmaps(g, h->F.u, &h->zmaps, &h->zmaps_ok)) != cudaSuccess) {
+        release(h); return cuda_fail(e, "make_zmaps");
+    }
     // zero state (the reference zero-initialises its Vecs and rk3 registers)
     if ((e = cudaMemsetAsync(h->fbuf, 0, ce * 6 * (size_t)g.S, h->st)) != cudaSuccess ||
         (e = cudaMemsetAsync(h->F.forcing, 0, sizeof(double2) * 3 * (size_t)h->nforce, h->st)) != cudaSuccess ||
@@ -608,11 +613,9 @@ extern "C" int pandora_init_particles(pandora_handle* h) {
 // f_RK3Stage{s} (src/pf_rk3.f90:40-200): [s=1: statistics of the state],
 // vorticity + z pass, y pass, x pass with NL (and CFL / physical velocity),
 // dt + forcing, particles, forward y, forward z + RK update, time advance.
-// One stage.  With particles the stage forks a second stream: at stage 1 the
-// spatial sort of the particles runs beside the statistics and the first three
-// passes, and every stage's particle advance (which needs the physical velocity
-// of K3 and the stage's dt) runs beside K4 and K5; the branch joins the main
-// stream before the stage clock advances.  Captured into the step graph, the
+// One stage.  With particles, stage 1 forks a second stream: the spatial sort of
+// the particles runs beside the statistics and the first three passes and joins
+// the main stream before the particle advance.  Captured into the step graph, the
 // fork and join become graph edges.
 // What one stage of a batch needs: the batch's geometry, its device member array
 // of B slots, the particles per member, the shell sums (B x shell_words,
@@ -631,6 +634,7 @@ template <class T> struct StepCtx {
     const PartSort* sort;        // null: no per-step particle sort (batches)
     const Particles* sortP;      // the particles the sort reorders
     pandora_handle* timing;      // null: no pass timing
+    const ZMaps* zmaps;          // null: K1 reads u element-wise (batches, FP32, other lengths)
 };
 
 template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, int* nlaunch) {
@@ -642,10 +646,12 @@ template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, 
     if (stage == 1 && g.shear) {
         PD_CK(launch_remesh(g, M, B, c.np, c.st)); n += part ? 2 : 1;
     }
-    if (stage == 1 && part && c.sort) {
+    const bool sorted = stage == 1 && part && c.sort;
+    if (sorted) {   // the spatial sort runs beside the statistics and K1-K3, joined before the advance
         PD_CK(cudaEventRecord(c.ev_fork, c.st));
         PD_CK(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
         PD_CK(launch_particle_sort(g, *c.sortP, *c.sort, c.side, &n));
+        PD_CK(cudaEventRecord(c.ev_join, c.side));
     }
     if (stage == 1) {
         PD_CK(launch_stats(g, M, B, c.shell, c.st)); n += 1;   // one kernel (plus a memset node)
@@ -660,7 +666,7 @@ template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, 
         return cudaEventRecordWithFlags(h->tev[stage - 1][ps - 1][end], s, cudaEventRecordExternal);
     };
     PD_CK(mark(1, 0, c.st));
-    PD_CK(launch_zpass_inv(g, M, B, stage, c.st)); n += g.dealias_cut > 0.0 ? 2 : 1;   // k_dealias first
+    PD_CK(launch_zpass_inv(g, M, B, stage, c.st, c.zmaps)); n += g.dealias_cut > 0.0 ? 2 : 1;   // k_dealias first
     PD_CK(mark(1, 1, c.st));
     PD_CK(mark(2, 0, c.st));
     PD_CK(launch_ypass_inv(g, M, B, c.st)); n++;
@@ -669,13 +675,14 @@ template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, 
     PD_CK(launch_xpass(g, M, B, part ? 1 : 0, stage == 1 ? 1 : 0, c.st)); n++;
     PD_CK(mark(3, 1, c.st));
     PD_CK(launch_stage_scalars(g, M, B, *c.fp, stage, c.st)); n++;
+    // The particle advance (it needs K3's physical velocity and the stage's dt) runs in
+    // the main stream between K3 and K4: on a second stream beside K4/K5 it slowed them
+    // by more than its own time (512^3 shear: K4 0.62 -> 0.85 ms beside a 0.08 ms advance).
     if (part) {
-        PD_CK(cudaEventRecord(c.ev_fork, c.st));
-        PD_CK(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
-        PD_CK(mark(6, 0, c.side));
-        PD_CK(launch_particles(g, M, B, c.np, c.order, stage, c.side)); n++;
-        PD_CK(mark(6, 1, c.side));
-        PD_CK(cudaEventRecord(c.ev_join, c.side));
+        if (sorted) PD_CK(cudaStreamWaitEvent(c.st, c.ev_join, 0));
+        PD_CK(mark(6, 0, c.st));
+        PD_CK(launch_particles(g, M, B, c.np, c.order, stage, c.st)); n++;
+        PD_CK(mark(6, 1, c.st));
     }
     PD_CK(mark(4, 0, c.st));
     PD_CK(launch_ypass_fwd(g, M, B, c.st)); n++;
@@ -683,7 +690,6 @@ template <class T> static int enqueue_stage_ctx(const StepCtx<T>& c, int stage, 
     PD_CK(mark(5, 0, c.st));
     PD_CK(launch_zpass_fwd_update(g, M, B, stage, 0, c.st)); n += 2;   // forward z FFT, RK update
     PD_CK(mark(5, 1, c.st));
-    if (part) PD_CK(cudaStreamWaitEvent(c.st, c.ev_join, 0));
     PD_CK(launch_advance_time(g, M, B, stage, c.st)); n++;
     if (nlaunch) *nlaunch += n;
     return PANDORA_OK;
@@ -706,6 +712,7 @@ template <class T> static int enqueue_stage_t(pandora_handle* h, int stage, int*
     c.sort = &h->sort;
     c.sortP = &h->P;
     c.timing = h;
+    c.zmaps = (h->zmaps_ok && !h->mixed) ? &h->zmaps : nullptr;
     return enqueue_stage_ctx(c, stage, nlaunch);
 }
 
@@ -894,7 +901,7 @@ extern "C" int pandora_nonlinear(pandora_handle* h, double* n1, double* n2, doub
     for (int c = 0; c < 3; c++) Fn.rk[c] = (double2*)h->nlbuf + c * h->g.S;
     const Member<double> mv = member_of<double>(h, Fn);
     const Member<double>* Mv = &mv;
-    PD_CK(launch_zpass_inv(h->g, Mv, 1, 0, h->st));
+    PD_CK(launch_zpass_inv(h->g, Mv, 1, 0, h->st, h->zmaps_ok ? &h->zmaps : nullptr));
     PD_CK(launch_ypass_inv(h->g, Mv, 1, h->st));
     PD_CK(launch_xpass(h->g, Mv, 1, 0, 0, h->st));
     PD_CK(launch_ypass_fwd(h->g, Mv, 1, h->st));
@@ -1077,7 +1084,7 @@ template <class T> static int profile_pass_t(pandora_handle* h, int32_t pass, in
     const Member<T>* Mv = &mv;
     for (int r = 0; r < reps; r++) {
         switch (pass) {
-        case 1: PD_CK(launch_zpass_inv(h->g, M, 1, 2, h->st)); break;
+        case 1: PD_CK(launch_zpass_inv(h->g, M, 1, 2, h->st, (h->zmaps_ok && !h->mixed) ? &h->zmaps : nullptr)); break;
         case 2: PD_CK(launch_ypass_inv(h->g, M, 1, h->st)); break;
         case 3: PD_CK(launch_xpass(h->g, M, 1, part ? 1 : 0, 0, h->st)); break;
         case 4: PD_CK(launch_ypass_fwd(h->g, M, 1, h->st)); break;

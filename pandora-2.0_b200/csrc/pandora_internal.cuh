@@ -1,6 +1,7 @@
 // pandora_internal.cuh -- device-side structures shared by the kernels and the
 // C-ABI layer.  Not part of the public boundary (include/pandora_gpu.h is).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "../../include/pandora_gpu.h"
@@ -224,7 +225,20 @@ template <class T, class Fn> inline cudaError_t for_member_sets(const Member<T>*
 // Launchers of the step kernels: g is the batch's geometry (grid sizes and flow
 // type, common to its members), M a host array of its B member descriptors
 // (passed by value to the kernels, kBatchChunk members per launch).
-template <class T> cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st);
+// Tensor maps of the three FP64 velocity components in the [i][j][k] layout (dims k as
+// 2 NKK doubles, j, i; boxes of BK k x 1 j x 8 i), for the K1 whose velocity rows are
+// staged by tensor copies.
+struct ZMaps {
+    CUtensorMap u[3];
+};
+// Fills *out for a single FP64 simulation whose z length has the staged K1; *ok = false
+// (and cudaSuccess) where it does not, or where the driver has no tensor-map encoder.
+cudaError_t make_zmaps(const Geo& g, double2* const* u, ZMaps* out, bool* ok);
+// K1: with `maps` (a single FP64 simulation, make_zmaps ok) the staged kernel, else the
+// kernel that reads its inputs element-wise from global memory.
+template <class T>
+cudaError_t launch_zpass_inv(const Geo& g, const Member<T>* M, int B, int stage, cudaStream_t st,
+                             const ZMaps* maps = nullptr);
 template <class T> cudaError_t launch_ypass_inv(const Geo& g, const Member<T>* M, int B, cudaStream_t st);
 template <class T>
 cudaError_t launch_xpass(const Geo& g, const Member<T>* M, int B, int want_phys, int want_cfl, cudaStream_t st);

@@ -196,3 +196,32 @@ def test_shear_particles(gpu_lib):
     assert d.max() < 1e-10, d.max()
     s.check_status()
     s.close()
+
+
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+@pytest.mark.parametrize("dims", [(32, 48, 512), (24, 16, 512)])
+def test_staged_k1_lengths_and_forms(gpu_lib, form, dims):
+    """z lines of 512 points in FP64 take the K1 whose velocity rows arrive by tensor
+    copies (one CTA per tile forming every field): isotropic (0), BF-rot (1), R-rot (2) and
+    R-conv (3) against the oracle after 3 steps, the last tile of i partial."""
+    import oracle as O
+    if form == 0:
+        p = gpu_lib.workload_params("iso_decay", 32)
+    else:
+        # dt = (0.5/S)/F_REMESH_T = 0.002: explicit viscosity stays stable at k3 = 170
+        p = _shear(gpu_lib, 32, remesh_t=250)
+        p.ns_deformed = {1: gpu_lib.NS_BF_ROT, 2: gpu_lib.NS_R_ROT, 3: gpu_lib.NS_R_CONV}[form]
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    o = O.Oracle(p)
+    s = gpu_lib.Simulation(p)
+    s.init_fluid()
+    o.set_state(s.get_state())
+    t = 0.0
+    for step in (1, 2, 3):
+        t, _ = o.step(step, t)
+        s.step(step)
+    assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10
+    o.set_state(s.get_state())
+    assert rel_l2_fields(s.nonlinear(), o.nonlinear()) < 1e-12
+    s.check_status()
+    s.close()
