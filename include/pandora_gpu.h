@@ -298,6 +298,8 @@ int pandora_pass_times(pandora_handle* h, float* ms);
 typedef struct pandora_batch pandora_batch;
 /* Device bytes a batch of this class and capacity allocates (for admission control). */
 int pandora_batch_bytes(const pandora_params* cls, int32_t capacity, int64_t* bytes);
+/* Capacity > 1 needs grid lengths of 32, 48, 64, 96, 128, 192 or 256 on every axis (the
+ * ensemble's sizes; other lengths: PANDORA_ERR_UNSUPPORTED, or capacity 1). */
 int pandora_batch_create(const pandora_params* cls, int32_t capacity, pandora_batch** out);
 int pandora_batch_destroy(pandora_batch* b);
 int pandora_batch_capacity(pandora_batch* b, int32_t* capacity, int32_t* free_slots);

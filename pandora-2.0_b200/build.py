@@ -15,8 +15,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libpandora_gpu.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["kernels_passes.cu", "kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu", "pandora_static.cu"]
-HEADERS = ["fft_core.cuh", "pandora_internal.cuh", "bfrot.cuh"]
+# the pass launchers of each group of transform lengths compile in their own unit (passes_n*.cu)
+PASS_GROUPS = "abcdefghijk"
+SOURCES = (["passes_n%s.cu" % g for g in PASS_GROUPS] +
+           ["kernels_passes.cu", "kernels_fluid.cu", "kernels_particles.cu", "pandora_capi.cu", "pandora_static.cu"])
+HEADERS = ["fft_core.cuh", "pandora_internal.cuh", "bfrot.cuh", "passes_kernels.cuh", "passes_n.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-v"]
@@ -46,7 +49,8 @@ def _compile(src: str) -> tuple[str, str]:
     return obj, r.stderr
 
 
-def build(force: bool = False, jobs: int = 4) -> str:
+def build(force: bool = False, jobs: int = 0) -> str:
+    jobs = jobs or max(1, min(len(SOURCES), os.cpu_count() or 4))
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= _deps_mtime():
         return OUT
     os.makedirs(BUILD, exist_ok=True)
@@ -64,6 +68,6 @@ def build(force: bool = False, jobs: int = 4) -> str:
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("-j", type=int, default=3)
+    ap.add_argument("-j", type=int, default=0, help="parallel compiles (default: the host's cores)")
     a = ap.parse_args()
     print(build(a.force, a.j))

@@ -263,8 +263,8 @@ template <int R, int S, class C> PD_HD void dft(C* v) {
     else static_assert(R == 2, "unsupported radix");
 }
 
-// Radix schedule per transform length.  Supported N: 2^a * {1,3,5,7} up to 1024 that
-// factor into the radices below (2, 3, 4, 5, 7, 8, 12, 16; 32 in warp plans) in at most three passes;
+// Radix schedule per transform length.  Supported N: 2^a * {1,3,5,7} from 16 to 1024,
+// factored into the radices below (2, 3, 4, 5, 7, 8, 12, 16; 32 in warp plans) in at most three passes;
 // lengths with a factor 3 take a radix-12 pass where that saves a pass.
 template <int N> struct Plan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
 #define PD_PLAN(N_, A, B, C) \
@@ -430,15 +430,25 @@ template <int N> struct WPlan { static constexpr int r0 = 0, r1 = 0, r2 = 0; };
 PD_WPLAN(16, 4, 4, 0)
 PD_WPLAN(24, 3, 8, 0)
 PD_WPLAN(32, 4, 8, 0)
+PD_WPLAN(40, 5, 8, 0)
 PD_WPLAN(48, 4, 12, 0)
+PD_WPLAN(56, 7, 8, 0)
 PD_WPLAN(64, 8, 8, 0)
+PD_WPLAN(80, 5, 16, 0)
 PD_WPLAN(96, 8, 12, 0)
+PD_WPLAN(112, 7, 16, 0)
 PD_WPLAN(128, 4, 4, 8)
+PD_WPLAN(160, 5, 4, 8)
 PD_WPLAN(192, 16, 12, 0)
+PD_WPLAN(224, 7, 4, 8)
 PD_WPLAN(256, 4, 8, 8)
+PD_WPLAN(320, 5, 8, 8)
 PD_WPLAN(384, 3, 8, 16)
+PD_WPLAN(448, 7, 8, 8)
 PD_WPLAN(512, 8, 8, 8)
+PD_WPLAN(640, 5, 8, 16)
 PD_WPLAN(768, 3, 16, 16)
+PD_WPLAN(896, 7, 8, 16)
 PD_WPLAN(1024, 16, 8, 8)
 #undef PD_WPLAN
 

@@ -1310,6 +1310,9 @@ extern "C" int pandora_batch_create(const pandora_params* cls, int32_t capacity,
     *out = nullptr;
     int rc = validate(cls);
     if (rc) return rc;
+    // more than one member per launch needs the batched kernels of every axis length
+    if (capacity > 1 && !(batched_length(cls->nodes_x) && batched_length(cls->nodes_y) && batched_length(cls->nodes_z)))
+        return PANDORA_ERR_UNSUPPORTED;
     pandora_batch* b = new (std::nothrow) pandora_batch();
     if (!b) return PANDORA_ERR_OOM;
     cudaGetDevice(&b->dev);

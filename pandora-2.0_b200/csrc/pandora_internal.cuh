@@ -188,6 +188,8 @@ template <class T, int CAP> struct MemberSet {
 };
 
 bool supported_length(int n);
+// Lengths whose kernels have batched (multi-member) instantiations: the ensemble's sizes.
+bool batched_length(int n);
 
 // Records "where: <CUDA error string>" as the message pandora_strerror returns for
 // PANDORA_ERR_CUDA (thread-local, the last failure wins) and returns PANDORA_ERR_CUDA.

@@ -251,8 +251,9 @@ int main() {
     RUN(16); RUN(24); RUN(32); RUN(40); RUN(48); RUN(56); RUN(64); RUN(80); RUN(96);
     RUN(112); RUN(128); RUN(160); RUN(192); RUN(224); RUN(256); RUN(320); RUN(384);
     RUN(448); RUN(512); RUN(640); RUN(768); RUN(896); RUN(1024);
-    RUNW(16); RUNW(24); RUNW(32); RUNW(48); RUNW(64); RUNW(96); RUNW(128); RUNW(192); RUNW(256);
-    RUNW(384); RUNW(512); RUNW(768); RUNW(1024);
+    RUNW(16); RUNW(24); RUNW(32); RUNW(40); RUNW(48); RUNW(56); RUNW(64); RUNW(80); RUNW(96); RUNW(112);
+    RUNW(128); RUNW(160); RUNW(192); RUNW(224); RUNW(256); RUNW(320); RUNW(384); RUNW(448); RUNW(512);
+    RUNW(640); RUNW(768); RUNW(896); RUNW(1024);
 #define RUNL(N)                                                                             \
     do {                                                                                    \
         double e1 = check<N, -1, 2, 3, true, true>(), e2 = check<N, +1, 2, 3, true, true>();   \
@@ -266,8 +267,9 @@ int main() {
         printf("direct tile N=%4d fwd %.2e bwd %.2e\n", N, e1, e2);                                 \
         if (!(e1 < 1e-14 && e2 < 1e-14)) bad++;                                                      \
     } while (0)
-    RUND(16); RUND(24); RUND(32); RUND(48); RUND(64); RUND(96); RUND(128); RUND(192); RUND(256);
-    RUND(384); RUND(512); RUND(768); RUND(1024);
+    RUND(16); RUND(24); RUND(32); RUND(40); RUND(48); RUND(56); RUND(64); RUND(80); RUND(96); RUND(112);
+    RUND(128); RUND(160); RUND(192); RUND(224); RUND(256); RUND(320); RUND(384); RUND(448); RUND(512);
+    RUND(640); RUND(768); RUND(896); RUND(1024);
 #define RUNP(N, PS)                                                          \
     do {                                                                     \
         double e1 = check_pair<N, -1, PS>(), e2 = check_pair<N, +1, PS>();   \
@@ -284,6 +286,8 @@ int main() {
     } while (0)
     RUNX(16, 2); RUNX(24, 3); RUNX(32, 2); RUNX(48, 2); RUNX(64, 3); RUNX(96, 3); RUNX(128, 4);
     RUNX(192, 4); RUNX(256, 4); RUNX(384, 5); RUNX(512, 5); RUNX(768, 4); RUNX(1024, 5);
+    RUNX(40, 4); RUNX(56, 4); RUNX(80, 4); RUNX(112, 4); RUNX(160, 4); RUNX(224, 4); RUNX(320, 4);
+    RUNX(448, 4); RUNX(640, 4); RUNX(896, 4);
     printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }

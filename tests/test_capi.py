@@ -53,7 +53,7 @@ def test_sizes():
 
 
 @pytest.mark.parametrize("field,value,status", [
-    ("nodes_x", 100, -6),         # no radix plan (2^2 * 5^2)
+    ("nodes_x", 100, -6),         # not 2^a x {1, 3, 5, 7} (2^2 * 5^2)
     ("rk3_cfl", 1.0, -7),         # g_RK3Check
     ("precision", 7, -10),
     ("f_type", 3, -10),           # RDT flow types are not in this library

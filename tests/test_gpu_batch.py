@@ -179,3 +179,17 @@ def test_batch_integrating_factor_class(gpu_lib):
     with gpu_lib.Batch(base, 1) as bt:
         with pytest.raises(gpu_lib.PandoraError):
             bt.admit(ex)
+
+
+def test_batch_lengths_without_batched_kernels_refused(gpu_lib):
+    """Lengths outside the ensemble's sizes have single-simulation kernels only: a batch
+    of several members is refused, a batch of one runs them."""
+    base = gpu_lib.workload_params("iso_decay", 80)
+    with pytest.raises(gpu_lib.PandoraError) as ei:
+        gpu_lib.Batch(base, 2)
+    assert ei.value.status == -10
+    with gpu_lib.Batch(base, 1) as b:
+        s0 = b.admit(_member(base, 71))
+        b.step(2)
+        b.sync()
+        assert _same(b.get_state(s0), _alone(gpu_lib, _member(base, 71), 2)[0])

@@ -45,7 +45,8 @@ def test_mixed_nonlinear(gpu_lib, n):
 
 
 @pytest.mark.parametrize("dims", [(64, 512, 16), (64, 16, 512), (512, 16, 16), (16, 1024, 16),
-                                  (16, 16, 1024), (1024, 16, 16), (256, 16, 32), (48, 192, 96)])
+                                  (16, 16, 1024), (1024, 16, 16), (256, 16, 32), (48, 192, 96),
+                                  (80, 112, 160), (640, 16, 56), (16, 896, 40)])
 def test_mixed_nonlinear_every_tile_shape(gpu_lib, dims):
     """Long lines in each direction of the FP32 form, including tiles of 16 lines
     whose last tile is partial (nkip = 24 at nx = 64)."""

@@ -59,10 +59,11 @@ def test_nonlinear_anisotropic_grid(gpu_lib):
 
 
 @pytest.mark.parametrize("axis", [0, 1, 2])
-@pytest.mark.parametrize("n", [96, 128, 192, 256, 384, 512, 768, 1024])
+@pytest.mark.parametrize("n", [40, 56, 80, 96, 112, 128, 160, 192, 224, 256, 320, 384, 448, 512, 640, 768, 896, 1024])
 def test_nonlinear_every_length(gpu_lib, n, axis):
     """Every supported transform length along each axis (x pass, y passes, z passes),
-    the other two axes 16 points long."""
+    the other two axes 16 points long; the lengths 2^a x {1, 3, 5, 7} of the reference's
+    size rule (src/pg_domain.f90:274-292)."""
     p = gpu_lib.workload_params("iso_decay", 32)
     dims = [16, 16, 16]
     dims[axis] = n
@@ -494,3 +495,30 @@ def test_integrating_factor_mixed_and_shear_refused(gpu_lib):
     with pytest.raises(gpu_lib.PandoraError) as ei:
         gpu_lib.Simulation(r)
     assert ei.value.status == -10
+
+
+@pytest.mark.parametrize("dims,workload", [((80, 80, 80), "iso_forced_particles"), ((112, 160, 224), "iso_decay"),
+                                           ((56, 40, 320), "shear")])
+def test_step_parity_factor_5_and_7_lengths(gpu_lib, dims, workload):
+    """Whole steps on grids with factors 5 and 7: forced flow with tracers, decaying flow on
+    an anisotropic grid, BF-rot shear; u (and tracers) against the oracle after 3 steps."""
+    p = gpu_lib.workload_params(workload, 32)
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    if p.p_track_part:
+        p.p_np_global = 1024
+    o, s = _pair(gpu_lib, p, init="gpu")
+    if p.p_track_part:
+        s.init_particles()
+        o.set_particles(*s.get_particles())
+    t = 0.0
+    for step in (1, 2, 3):
+        t, dt = o.step(step, t)
+        assert s.step(step) == dt
+    assert rel_l2_fields(s.get_state(), o.get_state()) < 1e-10
+    ek_g, _, eps_g, _ = s.stats()
+    ek_o, _, eps_o = o.stats()
+    assert rel_l2(ek_g, ek_o) < 1e-8 and abs(eps_g - eps_o) < 1e-8 * abs(eps_o)
+    if p.p_track_part:
+        d = np.abs(s.get_particles()[0] - o.get_particles(p.p_np_global)[0])
+        assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
+    s.close()
