@@ -1,13 +1,15 @@
-"""Error of the FP32-mixed form against the FP64 form of the same run.
+"""Deviation of a variant of the step from the FP64 explicit form of the same run: the
+FP32-mixed form (default), or the integrating-factor viscous form (``--viscous``).
 
-Both forms start from the same seeded field (the mixed form rounds the FP64
-initial field once), take the same steps on the same GPU, and are compared at
-the end: relative L2 of u over all stored modes, relative L2 of E(k), and the
-relative error of epsilon; both step times are reported.  The fields are compared
-on the device (views of the state buffers through __cuda_array_interface__), so a
-1024^3 state never crosses to the host.
+Both runs start from the same seeded field (the mixed form rounds the FP64 initial
+field once), take the same steps on the same GPU, and are compared at the end:
+relative L2 of u over all stored modes, relative L2 of E(k), and the relative error
+of epsilon; both step times are reported.  The fields are compared on the device
+(views of the state buffers through __cuda_array_interface__), so a 1024^3 state
+never crosses to the host.
 
     python -m pandora.mixed_error --workload iso_forced --n 1024 --steps 200
+    python -m pandora.mixed_error --workload iso_decay --n 64 --steps 100 --viscous
 """
 from __future__ import annotations
 
@@ -17,7 +19,7 @@ import sys
 
 import numpy as np
 
-from .params import PREC_FP32_MIXED, PREC_FP64, Params, workload_params
+from .params import PREC_FP32_MIXED, PREC_FP64, VISCOUS_EXPLICIT, VISCOUS_INTEGRATING_FACTOR, Params, workload_params
 from .rk3 import Simulation
 
 
@@ -39,13 +41,22 @@ def _state_views(sim: Simulation, mixed: bool):
     return [torch.as_tensor(_DeviceArray(q.value, n, ts), device="cuda") for q in ptrs]
 
 
-def compare(p: Params, steps: int) -> dict:
+def compare(p: Params, steps: int, viscous: bool = False) -> dict:
+    """viscous=False: FP32-mixed against FP64 (explicit viscosity); True: FP64 with the
+    integrating factor against FP64 explicit (the variant's figures keep the key names
+    of the mixed form: fp32_mixed = the variant)."""
     import torch
     q64 = Params.from_buffer_copy(p)
     q64.precision = PREC_FP64
+    q64.rk3_viscous = VISCOUS_EXPLICIT
     q32 = Params.from_buffer_copy(p)
-    q32.precision = PREC_FP32_MIXED
-    out = {"grid": [p.nodes_x, p.nodes_y, p.nodes_z], "steps": steps}
+    if viscous:
+        q32.precision = PREC_FP64
+        q32.rk3_viscous = VISCOUS_INTEGRATING_FACTOR
+    else:
+        q32.precision = PREC_FP32_MIXED
+    out = {"grid": [p.nodes_x, p.nodes_y, p.nodes_z], "steps": steps,
+           "variant": "integrating_factor" if viscous else "fp32_mixed"}
     sims = []
     for q in (q64, q32):
         s = Simulation(q)
@@ -64,7 +75,7 @@ def compare(p: Params, steps: int) -> dict:
         torch.cuda.synchronize()
         out[f"ms_per_step_{name}"] = e0.elapsed_time(e1) / max(steps - 2, 1)
     a, b = sims
-    ua, ub = _state_views(a, False), _state_views(b, True)
+    ua, ub = _state_views(a, False), _state_views(b, not viscous)
     num = sum(float(torch.sum((x - y.double()) ** 2)) for x, y in zip(ua, ub))
     den = sum(float(torch.sum(x ** 2)) for x in ua)
     out["rel_l2_u"] = (num / den) ** 0.5
@@ -84,12 +95,13 @@ def main(argv=None) -> int:
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--np", type=int, default=None, help="particles (workloads with tracers)")
     ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--viscous", action="store_true", help="the integrating-factor form against the explicit one")
     a = ap.parse_args(argv)
     p = workload_params(a.workload, a.n)
     if a.np is not None:
         p.p_np_global = a.np
         p.p_track_part = 1 if a.np > 0 else 0
-    r = compare(p, a.steps)
+    r = compare(p, a.steps, viscous=a.viscous)
     r["workload"] = a.workload
     print(json.dumps(r), flush=True)
     return 0
