@@ -508,19 +508,11 @@ template <class C> struct Out3 { C* p[3]; };
 // form loads FP32 values and rounds once on the store).
 // FORM: 0 isotropic, 1 BF-rot shear, 2 R-rot shear, 3 isotropic with the integrating
 // factor (its own instantiation, so the explicit forms carry no exponent code).
-template <int FORM, class T, int CAP>
-__global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+// The update of mode m = (i, j, k) (index in the [i][j][k] layout) from its NL-hat nl[3]:
+// the body of K5b.
+template <int FORM, class T>
+__device__ __forceinline__ void rk_mode(const FieldsT<T>& F, const Geo& g, int stage, long long m, const double2* nl) {
     using C = typename FieldsT<T>::C;
-    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
-    if (!mm.active) return;
-    if constexpr (CAP > 1) {   // a batch slot between members
-        if (mm.F.clock->status & PD_ST_IDLE) return;
-    }
-    const FieldsT<T> F = mm.F;
-    const Geo g = mm.g;
-    const C* __restrict__ nlh = F.yb;   // NL-hat from K5a
-    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= g.S) return;
     const int NKK = g.nkk;
     const int k = (int)(m % NKK);
     const long long ij = m / NKK;
@@ -532,9 +524,9 @@ __global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __gr
     rk_coeffs(stage, beta, gamma);
     const double dt = F.clock->dt;
     const double kv[3] = {k1, k2, k3};
-    double2 nl[3], uu[3], tot[3];
+    double2 uu[3], tot[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) { nl[c] = to_d(nlh[c * g.S + m]); uu[c] = to_d(F.u[c][m]); }
+    for (int c = 0; c < 3; c++) uu[c] = to_d(F.u[c][m]);
     BF bf;
     if constexpr (FORM == 1) {   // f_RK3FormFBFRot, F_SHEAR_DNS (no forcing)
         bf = make_bf(g, F.clock);
@@ -605,6 +597,25 @@ __global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __gr
 #pragma unroll
     for (int c = 0; c < 3; c++)
         F.u[c][m] = from_d<C>(mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2)));
+}
+
+template <int FORM, class T, int CAP>
+__global__ void __launch_bounds__(256, FORM == 1 ? 4 : 3) k_rk_update(const __grid_constant__ MemberSet<T, CAP> ms, int stage) {
+    using C = typename FieldsT<T>::C;
+    const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.y];
+    if (!mm.active) return;
+    if constexpr (CAP > 1) {   // a batch slot between members
+        if (mm.F.clock->status & PD_ST_IDLE) return;
+    }
+    const FieldsT<T> F = mm.F;
+    const Geo g = mm.g;
+    const C* __restrict__ nlh = F.yb;   // NL-hat from K5a
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= g.S) return;
+    double2 nl[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) nl[c] = to_d(nlh[c * g.S + m]);
+    rk_mode<FORM, T>(F, g, stage, m, nl);
 }
 
 // ---------------------------------------------------------------------------
@@ -1021,6 +1032,7 @@ __global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, tru
     };
     TCfg<NZ, true>::template transform<-1, LT>(s, F.tw_z, ld, st);
 }
+
 
 // Lengths with batched (kBatchChunk-member) instantiations: the ensemble's sizes.
 template <int N> constexpr bool batch_len() {
