@@ -4,9 +4,12 @@ smaller than the benchmark's.
 
     python -m pandora.run --workload shear --nodes 512 128 128 --steps 3
     python -m pandora.run --workload shear --nodes 512 512 512 --form r-conv --pass-times
+    python -m pandora.run --workload iso_decay --nodes 32 32 32 --batch 32 --steps 20
 
 ``--form`` picks the shear formulation (NS_DEFORMED); ``--pass-times`` times every
-pass of the last step with CUDA event pairs and prints them (ms, stage x pass).
+pass of the last step with CUDA event pairs and prints them (ms, stage x pass);
+``--batch CAP`` runs a batch of CAP members of the workload (own seeds) instead of one
+simulation and prints its member-steps/s.
 """
 from __future__ import annotations
 
@@ -29,12 +32,15 @@ def main(argv=None) -> int:
     ap.add_argument("--precision", choices=["fp64", "fp32_mixed"], default="fp64")
     ap.add_argument("--form", choices=sorted(FORMS), default="bf-rot", help="shear formulation")
     ap.add_argument("--pass-times", action="store_true", help="time each pass of the last step")
+    ap.add_argument("--batch", type=int, default=0, help="members of a batch (0: one simulation)")
     a = ap.parse_args(argv)
     p = workload_params(a.workload, a.nodes[0])
     p.nodes_x, p.nodes_y, p.nodes_z = a.nodes
     p.p_track_part, p.p_np_global = (1, a.np) if a.np > 0 else (0, 0)
     p.precision = PREC_FP32_MIXED if a.precision == "fp32_mixed" else PREC_FP64
     p.ns_deformed = FORMS[a.form]
+    if a.batch > 0:
+        return _run_batch(p, a)
     with Simulation(p) as s:
         s.init_fluid()
         if a.np > 0:
@@ -56,6 +62,25 @@ def main(argv=None) -> int:
         ek, tke, eps, _ = s.stats()
         s.check_status()
     print(f"{a.workload} {a.nodes[0]}x{a.nodes[1]}x{a.nodes[2]} {a.precision}: {a.steps} steps, tke {tke:.6e}, eps {eps:.6e}")
+    return 0
+
+
+def _run_batch(p, a) -> int:
+    import time
+    from .batch import Batch
+    with Batch(p, a.batch) as b:
+        for k in range(a.batch):
+            q = p.copy()
+            q.seed_fluid, q.seed_force, q.seed_particles = 1 + k, 1000 + k, 2000 + k
+            b.admit(q)
+        b.step(1)
+        b.sync()
+        t0 = time.perf_counter()
+        b.step(a.steps)
+        b.sync()
+        secs = time.perf_counter() - t0
+    print(f"{a.workload} {a.nodes[0]}x{a.nodes[1]}x{a.nodes[2]} {a.precision} batch of {a.batch}: "
+          f"{a.steps} steps, {a.batch * a.steps / secs:.0f} member-steps/s")
     return 0
 
 

@@ -335,6 +335,7 @@ def test_run_module(gpu_lib):
     assert run.main(["--workload", "shear", "--nodes", "64", "32", "48", "--steps", "2"]) == 0
     assert run.main(["--workload", "iso_forced_particles", "--nodes", "32", "32", "32", "--steps", "1",
                      "--np", "256", "--precision", "fp32_mixed"]) == 0
+    assert run.main(["--workload", "iso_decay", "--nodes", "32", "32", "32", "--steps", "2", "--batch", "4"]) == 0
 
 
 @pytest.mark.parametrize("mode,cut", [(2, 1.0), (3, 0.7)])
