@@ -130,7 +130,11 @@ typedef struct pandora_params {
     int32_t rk3_viscous;
     /* nl_numerics LES_CUTOFF: cutoff of DEALIASING = 3 as a multiple of KMAX */
     double  les_cutoff;
-    int32_t reserved[4];
+    /* schedule of the x pass (no counterpart in the reference; results do not depend on
+     * it): x lines per warp, 1, 2 or 4 for x lengths of at most 64 points (0: the
+     * library's choice for the length); other lengths take 0 or 1 */
+    int32_t x_lines_per_warp;
+    int32_t reserved[3];
 } pandora_params;
 
 typedef struct pandora_handle pandora_handle;

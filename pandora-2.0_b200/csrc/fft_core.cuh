@@ -515,21 +515,23 @@ __device__ __forceinline__ void wpass(C* s, const C* __restrict__ tw, int lane) 
 // independent work of a single line, which fills the lanes a radix-16 pass of
 // one line leaves idle.
 // KL / KS: band of the loads / stores (see in_band).
-template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0, int KL = 0, int KS = 0, class C>
+// W: lanes per line group (32: the whole warp; 32 / W groups of a warp each transform
+// their own lines, `lane` being the lane within the group).
+template <int N, int R, int NS, int S, int LP, int PS, int NA, int AS = 0, int KL = 0, int KS = 0, int W = 32, class C>
 __device__ __forceinline__ void wpass_n(C* s, const C* __restrict__ tw, int lane) {
     constexpr int WORK = (N / R) * NA;
-    constexpr int IT = (WORK + 31) / 32;
+    constexpr int IT = (WORK + W - 1) / W;
     C v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; it++) {
-        const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS, AS, KL>(s, tw, w, v[it]);
+        const int w = lane + it * W;
+        if (WORK % W == 0 || w < WORK) pass_load<N, R, NS, S, NA, LP, PS, AS, KL>(s, tw, w, v[it]);
     }
     __syncwarp();
 #pragma unroll
     for (int it = 0; it < IT; it++) {
-        const int w = lane + it * 32;
-        if (WORK % 32 == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS, AS, KS>(s, w, v[it]);
+        const int w = lane + it * W;
+        if (WORK % W == 0 || w < WORK) pass_store<N, R, NS, NA, LP, PS, AS, KS>(s, w, v[it]);
     }
     __syncwarp();
 }
@@ -538,12 +540,12 @@ __device__ __forceinline__ void wpass_n(C* s, const C* __restrict__ tw, int lane
 // warp: pass p has radix Rp and NS = the product of the radices before it.  The
 // plan's first pass reads the band KL, its last pass writes the band KS.
 template <int N, int S, int LP, int PS, int NA, int AS, int R0, int R1, int R2, int P0, int P1,
-          int KL = 0, int KS = 0, class C>
+          int KL = 0, int KS = 0, int W = 32, class C>
 __device__ __forceinline__ void wpasses(C* s, const C* __restrict__ tw, int lane) {
     constexpr int NP = R2 ? 3 : (R1 ? 2 : 1);
-    if constexpr (P0 <= 0 && 0 < P1) wpass_n<N, R0, 1, S, LP, PS, NA, AS, KL, NP == 1 ? KS : 0>(s, tw, lane);
-    if constexpr (P0 <= 1 && 1 < P1 && NP > 1) wpass_n<N, R1, R0, S, LP, PS, NA, AS, 0, NP == 2 ? KS : 0>(s, tw, lane);
-    if constexpr (P0 <= 2 && 2 < P1 && NP > 2) wpass_n<N, R2, R0 * R1, S, LP, PS, NA, AS, 0, KS>(s, tw, lane);
+    if constexpr (P0 <= 0 && 0 < P1) wpass_n<N, R0, 1, S, LP, PS, NA, AS, KL, NP == 1 ? KS : 0, W>(s, tw, lane);
+    if constexpr (P0 <= 1 && 1 < P1 && NP > 1) wpass_n<N, R1, R0, S, LP, PS, NA, AS, 0, NP == 2 ? KS : 0, W>(s, tw, lane);
+    if constexpr (P0 <= 2 && 2 < P1 && NP > 2) wpass_n<N, R2, R0 * R1, S, LP, PS, NA, AS, 0, KS, W>(s, tw, lane);
 }
 
 template <int N, int S, int LP, int PS, int NA, bool LOWPASS = false, int AS = 0, class C>

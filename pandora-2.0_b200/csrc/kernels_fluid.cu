@@ -132,9 +132,22 @@ __global__ void __launch_bounds__(256) k_stats(const __grid_constant__ MemberSet
             }
         }
     }
-    atomicAdd(&sp[0], p11);
-    atomicAdd(&sp[1], p22);
-    atomicAdd(&sp[2], p33);
+    // the three second moments: summed within each warp, then the warps' sums added in warp
+    // order by one thread (not 256 atomics on the same three shared words)
+    __shared__ double wp[8][3];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        p11 += __shfl_xor_sync(0xffffffffu, p11, o);
+        p22 += __shfl_xor_sync(0xffffffffu, p22, o);
+        p33 += __shfl_xor_sync(0xffffffffu, p33, o);
+    }
+    if (lane == 0) { wp[wib][0] = p11; wp[wib][1] = p22; wp[wib][2] = p33; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double a = 0.0;
+        for (int v = 0; v < nw; v++) a += wp[v][threadIdx.x];
+        sp[threadIdx.x] = a;
+    }
     __syncthreads();
     double* part = reinterpret_cast<double*>(F.yb) + (size_t)blockIdx.x * nsh;
     for (int q = threadIdx.x; q < nsh; q += blockDim.x) part[q] = sh[q];

@@ -212,6 +212,9 @@ static int validate(const pandora_params* p) {
     if (p->rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR && p->f_type != PANDORA_F_ISOTROPIC)
         return PANDORA_ERR_UNSUPPORTED;
     if (p->dealiasing < PANDORA_DEALIASING_23 || p->dealiasing > PANDORA_DEALIASING_LES) return PANDORA_ERR_UNSUPPORTED;
+    if (p->x_lines_per_warp != 0 && p->x_lines_per_warp != 1 && p->x_lines_per_warp != 2 && p->x_lines_per_warp != 4)
+        return PANDORA_ERR_INVALID_ARG;
+    if (p->x_lines_per_warp > 1 && p->nodes_x > 64) return PANDORA_ERR_INVALID_ARG;
     if (p->dealiasing == PANDORA_DEALIASING_LES && !(p->les_cutoff > 0.0)) return PANDORA_ERR_INVALID_ARG;
     if (!supported_length(p->nodes_x) || !supported_length(p->nodes_y) || !supported_length(p->nodes_z))
         return PANDORA_ERR_BAD_LAYOUT;
@@ -262,6 +265,7 @@ extern "C" int pandora_create(const pandora_params* p, pandora_handle** out) {
     g.rk3_decide = (p->rk3_timestep == PANDORA_RK3_TIMESTEP_DECIDE) ? 1 : 0;
     g.bvol = (double)p->b110 * (double)p->b220 * (double)p->b330;
     g.visc_if = p->rk3_viscous == PANDORA_VISCOUS_INTEGRATING_FACTOR ? 1 : 0;
+    g.xlpw = p->x_lines_per_warp;
     {   // KMAX = min(KI_MAX, KJ_MAX, KK_MAX) (src/pg_domain.f90:231)
         const double kmax = (double)std::min(g.ki, std::min(g.kj, g.kk));
         g.dealias_cut = p->dealiasing == PANDORA_DEALIASING_SPHERICAL ? kmax

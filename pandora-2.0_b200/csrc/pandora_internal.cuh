@@ -40,6 +40,8 @@ struct Geo {
     // PANDORA_VISCOUS_INTEGRATING_FACTOR: the viscous term as exp(-nu k^2 dc dt) factors
     // of u and the register per stage (isotropic flow), else explicit
     int visc_if;
+    // x lines per warp of the x pass (0: the library's choice for the length)
+    int xlpw;
 };
 
 // Scalars of the running step kept in device memory so that a whole step can

@@ -134,7 +134,9 @@ __device__ __forceinline__ void rs_point(double* acc, double* mx, bool shear, co
 
 // RS: the real-space statistics pass (the same transforms, plus the moments of every
 // point, reduced per warp into one of kRsSlots copies of the sums in `rs`).
-template <int NX, class T, int CAP, bool RS = false>
+// LPW: lines per warp (LPW > 1 for short, unfused lines: each group of 32 / LPW lanes
+// transforms its own line).
+template <int NX, class T, int CAP, bool RS = false, int LPW = 1>
 __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>()) k_xpass(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                         int want_phys,
                                                                                         int want_cfl,
@@ -151,13 +153,18 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     const Geo g = mm.g;
     constexpr int XPS = xps<NX>(), XAS = xas<NX>(), NA = xna<NX>();
     constexpr int KB = NX / 3;   // the kept band of the x spectrum, i <= KI
+    static_assert(LPW == 1 || (!XP::fused && !RS), "several lines per warp: unfused plans, no statistics");
+    constexpr int W = 32 / LPW;  // lanes per line
     C* smem = smem_as<C>();
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int tid = threadIdx.x, lane = (tid & 31) % W, sub = (tid & 31) / W, w = tid >> 5;
     const long long lines = (long long)g.ny * g.nz;
     const C* tw = F.tw_x;
-    const long long q = (long long)blockIdx.x * Cfg<NX>::NWX + w;
-    if (q >= lines) return;                       // whole warp; no block barrier follows
-    C* s = smem + (size_t)w * 3 * XAS;
+    const long long qw = ((long long)blockIdx.x * Cfg<NX>::NWX + w) * LPW;   // the warp's first line
+    if (qw >= lines) return;                      // whole warp; no block barrier follows
+    // a group past the last line transforms the last line again and stores nothing
+    const bool valid = qw + sub < lines;
+    const long long q = valid ? qw + sub : lines - 1;
+    C* s = smem + ((size_t)w * LPW + sub) * 3 * XAS;
     const long long fstride = lines * g.nkip;     // distance between fields in yb
     const int NKI = g.nki;
     C* b = F.yb + q * g.nkip;
@@ -177,14 +184,14 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     // of up to IB rounds of m are issued before any of their stores, so a line waits
     // on HBM about twice rather than once per round.
     {
-        constexpr int ITM = (NX / 3 + 1 + 31) / 32;       // rounds of m (NKI = NX/3 + 1)
+        constexpr int ITM = (NX / 3 + 1 + W - 1) / W;     // rounds of m (NKI = NX/3 + 1)
         constexpr int IB = NX >= 384 ? (ITM + 1) / 2 : 1;
 #pragma unroll
         for (int i0 = 0; i0 < ITM; i0 += IB) {
             C X[IB][6];
 #pragma unroll
             for (int it = 0; it < IB; it++) {
-                const int m = lane + 32 * (i0 + it);
+                const int m = lane + W * (i0 + it);
                 if (i0 + it < ITM && m < NKI) {
 #pragma unroll
                     for (int c = 0; c < 6; c++) X[it][c] = b[c * fstride + m];
@@ -201,7 +208,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
             }
 #pragma unroll
             for (int it = 0; it < IB; it++) {
-                const int m = lane + 32 * (i0 + it);
+                const int m = lane + W * (i0 + it);
                 if (i0 + it < ITM && m < NKI) {
 #pragma unroll
                     for (int p = 0; p < 3; p++) {
@@ -217,10 +224,10 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     __syncwarp();
     constexpr int R0 = XP::r0, R1 = XP::r1, R2 = XP::r2, NP = XP::np;
     if constexpr (NA == 2) {
-        pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB>(s, tw, lane);
+        pdfft::wpasses<NX, +1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, KB, 0, W>(s, tw, lane);
     } else {   // one array at a time, one copy of the code (instruction-cache footprint)
 #pragma unroll 1
-        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + a * XAS, tw, lane);
+        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB, 0, W>(s + a * XAS, tw, lane);
     }
     T umax = T(0);
     if constexpr (XP::fused) {
@@ -259,12 +266,12 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
         }
         __syncwarp();
     } else {
-        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB>(s + 2 * XAS, tw, lane);
-        for (int n = lane; n < NX; n += 32) {
+        pdfft::wpasses<NX, +1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, KB, 0, W>(s + 2 * XAS, tw, lane);
+        for (int n = lane; n < NX; n += W) {
             C* e = s + prow<XPS>(n);
             const C a = e[0], bb = e[XAS], c = e[2 * XAS];
             const T u1 = a.x, u2 = a.y, u3 = bb.x, w1 = bb.y, w2 = c.x, w3 = c.y;
-            if (want_phys) {
+            if (want_phys && valid) {
                 F.phys[q * NX + n] = u1;
                 F.phys[g.R + q * NX + n] = u2;
                 F.phys[2 * g.R + q * NX + n] = u3;
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     }
     if (want_cfl) {
         for (int o = 16; o > 0; o >>= 1) umax = fmax(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-        if (lane == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
+        if ((tid & 31) == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
     }
     if constexpr (RS) {   // the warp's sums into slot q % kRsSlots
         double* slot = rs + (size_t)(q % kRsSlots) * kRsWords;
@@ -301,18 +308,18 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     // the CTA that takes it starts about when this one ends) are prefetched into
     // L2, one bulk prefetch per row, while this line's forward transforms run:
     // that CTA's loads then wait on L2 rather than HBM.
-    if (pf_lines > 0 && q + pf_lines < lines && lane < 6)
+    if (pf_lines > 0 && valid && q + pf_lines < lines && lane < 6)
         prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
     // forward transforms of the product arrays; only the band is written
     constexpr int F0 = XP::f0, F1 = XP::f1, F2 = XP::f2, P0 = XP::fused ? 1 : 0;
     if constexpr (NA == 2) {
-        pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, F0, F1, F2, P0, NP, 0, KB>(s, tw, lane);
+        pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, F0, F1, F2, P0, NP, 0, KB, W>(s, tw, lane);
     } else {
 #pragma unroll 1
-        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB>(s + a * XAS, tw, lane);
+        for (int a = 0; a < 2; a++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB, W>(s + a * XAS, tw, lane);
     }
     const T half = T(0.5);
-    for (int m = lane; m < g.nkip; m += 32) {
+    for (int m = lane; m < g.nkip && valid; m += W) {
         C n1 = mk(T(0), T(0)), n2 = n1, n3 = n1;
         if (m < NKI) {
             const int mc = (NX - m) % NX;
@@ -1033,6 +1040,12 @@ __global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, tru
     TCfg<NZ, true>::template transform<-1, LT>(s, F.tw_z, ld, st);
 }
 
+
+// x lengths whose x pass has instantiations with several lines per warp (short, unfused
+// lines, where one line leaves most lanes idle in its loads and passes).
+template <int N> constexpr bool xlpw_len() { return N <= 64; }
+// Lines per warp of the x pass when the simulation leaves the choice to the library.
+template <int N, class T, int CAP> constexpr int default_xlpw() { return 1; }
 
 // Lengths with batched (kBatchChunk-member) instantiations: the ensemble's sizes.
 template <int N> constexpr bool batch_len() {

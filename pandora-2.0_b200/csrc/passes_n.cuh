@@ -5,8 +5,8 @@
 
 namespace pd {
 
-template <int N, class T> static size_t smem_kx() {
-    return sizeof(typename Cplx<T>::type) * ((size_t)Cfg<N>::NWX * 3 * xas<N>());
+template <int N, class T, int LPW = 1> static size_t smem_kx() {
+    return sizeof(typename Cplx<T>::type) * ((size_t)Cfg<N>::NWX * LPW * 3 * xas<N>());
 }
 
 // CTAs of `kernel` resident on the whole device at once.
@@ -44,6 +44,10 @@ template <int N, class T, int CAP> static cudaError_t configure_cap(const Geo& g
     }
     if (g.nx == N) {
         if ((e = set_smem(k_xpass<N, T, CAP>, smem_kx<N, T>()))) return e;
+        if constexpr (xlpw_len<N>()) {
+            if ((e = set_smem(k_xpass<N, T, CAP, false, 2>, smem_kx<N, T, 2>()))) return e;
+            if ((e = set_smem(k_xpass<N, T, CAP, false, 4>, smem_kx<N, T, 4>()))) return e;
+        }
         if (g.rconv && (e = set_smem(k_xpass_conv<N, T, CAP>, ConvCfg<N, T>::smem))) return e;
     }
     return cudaSuccess;
@@ -126,12 +130,25 @@ cudaError_t xpass_n(const Geo& g, const Member<T>* M, int B, int want_phys, int 
                                                                                                   want_cfl, pf);
                 return;
             }
-            const long long nl = (lines + Cfg<N>::NWX - 1) / Cfg<N>::NWX;
-            // L2 prefetch distance: one wave of resident CTAs (single simulations)
-            const long long pf =
-                CAP == 1 ? Cfg<N>::NWX * resident_ctas(k_xpass<N, T, CAP>, 32 * Cfg<N>::NWX, smem_kx<N, T>()) : 0;
-            k_xpass<N, T, CAP><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T>(), st>>>(ms, want_phys, want_cfl,
-                                                                                                 pf, nullptr);
+            auto go = [&](auto lpwc) {
+                constexpr int LPW = decltype(lpwc)::value;
+                constexpr int LB = Cfg<N>::NWX * LPW;   // lines per CTA
+                const long long nl = (lines + LB - 1) / LB;
+                // L2 prefetch distance: one wave of resident CTAs (single simulations)
+                const long long pf = CAP == 1 ? LB * resident_ctas(k_xpass<N, T, CAP, false, LPW>, 32 * Cfg<N>::NWX,
+                                                                   smem_kx<N, T, LPW>())
+                                              : 0;
+                k_xpass<N, T, CAP, false, LPW><<<dim3((unsigned)nl, nb), 32 * Cfg<N>::NWX, smem_kx<N, T, LPW>(), st>>>(
+                    ms, want_phys, want_cfl, pf, nullptr);
+            };
+            if constexpr (xlpw_len<N>()) {
+                const int lpw = g.xlpw > 0 ? g.xlpw : default_xlpw<N, T, CAP>();
+                if (lpw == 4) go(std::integral_constant<int, 4>{});
+                else if (lpw == 2) go(std::integral_constant<int, 2>{});
+                else go(std::integral_constant<int, 1>{});
+            } else {
+                go(std::integral_constant<int, 1>{});
+            }
         }
     });
 }

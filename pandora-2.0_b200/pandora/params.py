@@ -65,7 +65,8 @@ class Params(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("rk3_viscous", ctypes.c_int32),
         ("les_cutoff", ctypes.c_double),
-        ("reserved", ctypes.c_int32 * 4),
+        ("x_lines_per_warp", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
     def copy(self) -> "Params":

@@ -193,3 +193,21 @@ def test_batch_lengths_without_batched_kernels_refused(gpu_lib):
         b.step(2)
         b.sync()
         assert _same(b.get_state(s0), _alone(gpu_lib, _member(base, 71), 2)[0])
+
+
+@pytest.mark.parametrize("lpw", [2, 4])
+def test_batch_x_lines_per_warp(gpu_lib, lpw):
+    """A batch whose x pass runs several lines per warp: members equal their runs alone
+    (with the default schedule) bit for bit."""
+    base = gpu_lib.workload_params("iso_forced_particles", 32)
+    base.p_np_global = 128
+    cls = base.copy()
+    cls.x_lines_per_warp = lpw
+    with gpu_lib.Batch(cls, 3) as b:
+        slots = [b.admit(_member(cls, 81 + k)) for k in range(3)]
+        b.step(3)
+        b.sync()
+        for k, sl in enumerate(slots):
+            u, xp = _alone(gpu_lib, _member(base, 81 + k), 3)
+            assert _same(b.get_state(sl), u), k
+            assert np.array_equal(b.get_particles(sl)[0], xp), k

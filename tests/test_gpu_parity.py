@@ -523,3 +523,57 @@ def test_step_parity_factor_5_and_7_lengths(gpu_lib, dims, workload):
         d = np.abs(s.get_particles()[0] - o.get_particles(p.p_np_global)[0])
         assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
     s.close()
+
+
+@pytest.mark.parametrize("dims,workload", [((16, 16, 16), "iso_forced_particles"), ((24, 32, 16), "iso_decay"),
+                                           ((32, 32, 32), "shear"), ((48, 24, 32), "iso_forced_particles"),
+                                           ((64, 32, 48), "shear"), ((56, 40, 16), "iso_decay")])
+def test_x_lines_per_warp_schedules_agree(gpu_lib, dims, workload):
+    """The x pass with 1, 2 or 4 lines per warp (x lengths up to 64) does the same
+    arithmetic per line: the states (and tracers) after 3 steps are equal bit for bit,
+    and equal the oracle's to 1e-10."""
+    p = gpu_lib.workload_params(workload, 32)
+    p.nodes_x, p.nodes_y, p.nodes_z = dims
+    if p.p_track_part:
+        p.p_np_global = 512
+    out = []
+    for lpw in (1, 2, 4):
+        q = p.copy()
+        q.x_lines_per_warp = lpw
+        with gpu_lib.Simulation(q) as s:
+            s.init_fluid()
+            if q.p_track_part:
+                s.init_particles()
+            s.advance(3)
+            out.append((s.get_state(), s.get_particles()[0] if q.p_track_part else None, s.stats()))
+    for u, xp, st in out[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(u, out[0][0]))
+        if xp is not None:
+            assert np.array_equal(xp, out[0][1])
+        assert st[1] == pytest.approx(out[0][2][1], rel=1e-13)
+    import oracle as O
+    o = O.Oracle(p)
+    with gpu_lib.Simulation(p) as s:
+        s.init_fluid()
+        o.set_state(s.get_state())
+        if p.p_track_part:
+            s.init_particles()
+            o.set_particles(*s.get_particles())
+    t = 0.0
+    for step in (1, 2, 3):
+        t, _ = o.step(step, t)
+    assert rel_l2_fields(out[2][0], o.get_state()) < 1e-10
+    if p.p_track_part:
+        d = np.abs(out[2][1] - o.get_particles(p.p_np_global)[0])
+        assert np.minimum(d, 2 * np.pi - d).max() < 1e-10
+
+
+def test_x_lines_per_warp_validation(gpu_lib):
+    p = gpu_lib.workload_params("iso_decay", 32)
+    p.x_lines_per_warp = 3
+    with pytest.raises(gpu_lib.PandoraError):
+        gpu_lib.Simulation(p)
+    p = gpu_lib.workload_params("iso_decay", 96)
+    p.x_lines_per_warp = 2
+    with pytest.raises(gpu_lib.PandoraError):
+        gpu_lib.Simulation(p)
