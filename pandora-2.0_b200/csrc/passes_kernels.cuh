@@ -1044,8 +1044,14 @@ __global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, tru
 // x lengths whose x pass has instantiations with several lines per warp (short, unfused
 // lines, where one line leaves most lanes idle in its loads and passes).
 template <int N> constexpr bool xlpw_len() { return N <= 64; }
-// Lines per warp of the x pass when the simulation leaves the choice to the library.
-template <int N, class T, int CAP> constexpr int default_xlpw() { return 1; }
+// Lines per warp of the x pass when the simulation leaves the choice to the library,
+// measured on B200 (decaying flow, FP64): batches of 32 members run 4 lines per warp up to
+// 48 points (32^3: 80K -> 106K member-steps/s, 48^3: 22.2K -> 27.1K) and 2 at 64 points
+// (17.0K -> 21.2K); a single simulation, whose step is bound by its launches at these
+// sizes, 2 from 48 points (64^3: 0.109 -> 0.101 ms per step).
+template <int N, class T, int CAP> constexpr int default_xlpw() {
+    return CAP > 1 ? (N <= 48 ? 4 : 2) : (N >= 48 ? 2 : 1);
+}
 
 // Lengths with batched (kBatchChunk-member) instantiations: the ensemble's sizes.
 template <int N> constexpr bool batch_len() {

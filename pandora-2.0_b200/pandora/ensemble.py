@@ -9,9 +9,10 @@ the room).  The loop is continuous batching: an arriving request takes a free
 slot of its class at once, even while the other members are mid-run; every batch
 with occupied slots is advanced a few steps at a time on its own stream, so the
 classes' work overlaps on the GPU; a member that reaches its step count is read
-out and its slot freed for the next request.  Batch capacities (members per
-class) come from a small autotuner that measures member-steps/s per (grid,
-precision) at several capacities and keeps the best.
+out and its slot freed for the next request.  Batch schedules come from an
+autotuner that measures member-steps/s per (grid, precision) at several capacities
+(members per launch) and, for lines of up to 64 points, x-pass schedules (1, 2 or 4
+lines per warp), and keeps the best pair.
 
     python -m pandora.ensemble --requests 2000 --load 0.8 --budget-gb 150
 """
@@ -97,31 +98,42 @@ def make_trace(n_requests: int, seed: int = 7, rate: float | None = None, steps:
 # ---------------------------------------------------------------------------
 def tune_capacity(n: int, precision: int, caps=(1, 2, 4, 8, 16, 32, 64), steps: int = 6,
                   max_bytes: int = 40 << 30) -> dict:
-    """Member-steps/s of a full batch of decaying-isotropic members at each capacity;
-    returns {"best": cap, "rates": {cap: member-steps/s}}."""
+    """The batch schedule of a class: member-steps/s of a full batch of decaying-isotropic
+    members at each capacity, for each x-pass schedule the length has (x lines per warp
+    1, 2, 4 up to 64 points); returns {"best": cap, "xlpw": lines per warp,
+    "rates": {cap: member-steps/s of the best schedule}, "rates_by_xlpw": {...}}."""
     import torch
-    rates = {}
-    best, best_rate = 1, 0.0
-    for cap in caps:
-        p = request_params(n, False, 0, precision, seed=1)
-        if batch_bytes(p, cap) > max_bytes:
-            break
-        with Batch(p, cap) as b:
-            for k in range(cap):
-                b.admit(request_params(n, False, 0, precision, seed=1 + k))
-            b.step(2)
-            b.sync()
-            t0 = time.perf_counter()
-            b.step(steps)
-            b.sync()
-            rate = cap * steps / (time.perf_counter() - t0)
-        rates[cap] = rate
-        if rate > best_rate * 1.05:
-            best, best_rate = cap, rate
-        elif rate < best_rate:
-            break
+    lpws = (1, 2, 4) if n <= 64 else (1,)
+    by_lpw = {}
+    best, best_lpw, best_rate = 1, lpws[0], 0.0
+    for lpw in lpws:
+        rates = {}
+        top = 0.0
+        for cap in caps:
+            p = request_params(n, False, 0, precision, seed=1)
+            p.x_lines_per_warp = lpw
+            if batch_bytes(p, cap) > max_bytes:
+                break
+            with Batch(p, cap) as b:
+                for k in range(cap):
+                    q = request_params(n, False, 0, precision, seed=1 + k)
+                    q.x_lines_per_warp = lpw
+                    b.admit(q)
+                b.step(2)
+                b.sync()
+                t0 = time.perf_counter()
+                b.step(steps)
+                b.sync()
+                rate = cap * steps / (time.perf_counter() - t0)
+            rates[cap] = rate
+            if rate > best_rate * 1.05:
+                best, best_lpw, best_rate = cap, lpw, rate
+            if rate < top:
+                break
+            top = max(top, rate)
+        by_lpw[lpw] = rates
     torch.cuda.synchronize()
-    return {"best": best, "rates": rates}
+    return {"best": best, "xlpw": best_lpw, "rates": by_lpw[best_lpw], "rates_by_xlpw": by_lpw}
 
 
 # Capacities measured on a B200 by tune_capacity (the starting table of autotune).
@@ -176,6 +188,10 @@ class Server:
     def _cap(self, p: Params) -> int:
         return int(self.capacity.get(f"{p.nodes_x}/{p.precision}", {"best": 1}).get("best", 1))
 
+    def _xlpw(self, p: Params) -> int:
+        """The class's x-pass schedule from the autotuner (0: the library's choice)."""
+        return int(self.capacity.get(f"{p.nodes_x}/{p.precision}", {}).get("xlpw", 0))
+
     def _busy(self, key) -> bool:
         return bool(self.members[key]) or any(f[0] == key for f in self.finishing)
 
@@ -194,7 +210,9 @@ class Server:
             self.batches.pop(k).close()
             self.bytes.pop(k)
             self.tickets.pop(k, None)
-        b = Batch(req.params, cap)
+        cls = req.params.copy()
+        cls.x_lines_per_warp = self._xlpw(req.params)
+        b = Batch(cls, cap)
         self.batches[key] = b
         self.bytes[key] = need
         self.peak_bytes = max(self.peak_bytes, sum(self.bytes.values()))
@@ -216,7 +234,7 @@ class Server:
                 b = self._batch_for(r)
                 if b is None or not b.free:
                     continue
-                slot = b.admit(r.params, b.free[0])
+                slot = b.admit(r.params, b.free[0])   # the schedule is the batch's (results do not depend on it)
                 r.admitted = time.perf_counter() - t0
                 self.members[class_key(r.params)][slot] = [r, r.steps]
                 del waiting[rid]
@@ -351,7 +369,8 @@ def main(argv=None) -> int:
            "served": res, "serial": base,
            "speedup_vs_serial": res["mpts_rk3steps_per_s"] / base["mpts_rk3steps_per_s"],
            "saturated_vs_serial": sat["mpts_rk3steps_per_s"] / base["mpts_rk3steps_per_s"],
-           "batch_capacity": {k: v["best"] for k, v in caps.items()}}
+           "batch_capacity": {k: v["best"] for k, v in caps.items()},
+           "x_lines_per_warp": {k: v.get("xlpw", 0) for k, v in caps.items()}}
     print(json.dumps(out), flush=True)
     return 0
 
