@@ -679,9 +679,12 @@ template <int N, bool TWO = false> struct TCfg {
 // of a tile are adjacent in launch order, so the three that read a velocity
 // component run together and two of the three reads hit L2.  FORM (compile time, so
 // that each instantiation carries only its own derivative code): 0 isotropic, 1 BF-rot,
-// 2 R-rot, 3 R-conv.
+// 2 R-rot, 3 R-conv.  The batched shear forms at 256 points in FP64 ask for one CTA per SM
+// fewer than the others: the member index and frame tensors spilled at five.
 template <int NZ, int FORM, class T, int CAP>
-__global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(), TCfg<NZ>::template minb<T>()) k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
+__global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
+                                  TCfg<NZ>::template minb<T>() - ((CAP > 1 && FORM != 0 && sizeof(T) == 8 && NZ == 256) ? 1 : 0))
+    k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
                                                                                                    long long pf_ctas) {
     using C = typename FieldsT<T>::C;
     constexpr bool SHEAR = FORM != 0;
