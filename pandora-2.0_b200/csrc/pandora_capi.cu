@@ -1121,9 +1121,9 @@ extern "C" int pandora_pass_bytes(pandora_handle* h, int32_t pass, double* bytes
     const double R = (double)g.R;
     const bool part = h->particles_on && h->P.np > 0;
     switch (pass) {
-    case 1: *bytes = c16 * (3 * S + 6 * Z); break;
-    case 2: *bytes = c16 * (6 * Z + 6 * Y); break;
-    case 3: *bytes = c16 * (6 * Y + 3 * Y) + (part ? r8 * 3 * R : 0.0); break;
+    case 1: *bytes = c16 * (3 * S + pass_fields(g) * Z); break;   // 6 fields, 9 in the R-conv form
+    case 2: *bytes = c16 * (pass_fields(g) * Z + pass_fields(g) * Y); break;
+    case 3: *bytes = c16 * (pass_fields(g) * Y + 3 * Y) + (part ? r8 * 3 * R : 0.0); break;
     case 4: *bytes = c16 * (3 * Y + 3 * Z); break;
     case 5: *bytes = c16 * (3 * Z + 3 * S) + c16 * (3 * S + 6 * S + 6 * S); break;   // K5a + K5b
     case 6: {   // the field values the stencils need (each read once at most) and the particle state
