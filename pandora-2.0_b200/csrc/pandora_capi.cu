@@ -224,6 +224,8 @@ static int validate(const pandora_params* p) {
     if (p->f_nu < 0.0) return PANDORA_ERR_INVALID_ARG;
     if (p->p_track_part) {
         if (p->p_np_global < 0 || p->p_interp_order < 1 || p->p_interp_order > 6) return PANDORA_ERR_INVALID_ARG;
+        // the spatial sort counts and offsets particles in 32 bits
+        if (p->p_np_global > 0x7fffffffll) return PANDORA_ERR_INVALID_ARG;
         if (p->p_dia_vals > 0.0 && (p->f_nu <= 0.0 || p->f_rho <= 0.0)) return PANDORA_ERR_INVALID_ARG;
     }
     return PANDORA_OK;

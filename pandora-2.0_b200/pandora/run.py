@@ -19,7 +19,7 @@ import sys
 from .params import NS_BF_ROT, NS_R_CONV, NS_R_ROT, PREC_FP32_MIXED, PREC_FP64, workload_params
 
 FORMS = {"bf-rot": NS_BF_ROT, "r-conv": NS_R_CONV, "r-rot": NS_R_ROT}
-PASSES = ("zpass_inv", "ypass_inv", "xpass", "ypass_fwd", "zpass_fwd", "rk_update")
+PASSES = ("zpass_inv", "ypass_inv", "xpass", "ypass_fwd", "zpass_fwd_update", "particles")
 from .rk3 import Simulation
 
 
@@ -54,7 +54,7 @@ def main(argv=None) -> int:
             s.advance(1)
             t = s.pass_times()
             s.set_pass_timing(0)
-            for name, col in zip(PASSES, t.T):   # -1: not run on its own (K5b inside K5a's pair)
+            for name, col in zip(PASSES, t.T):   # -1: not timed (no particles)
                 if (col < 0).all():
                     continue
                 print(f"{name:10s} " + " ".join(f"{v:8.3f}" for v in col) + f"   sum {col[col > 0].sum():8.3f} ms")
