@@ -162,9 +162,12 @@ __device__ __forceinline__ void rhs_rrot(const BF& f, double nu, const double* k
                 }
             }
         }
+    // one reciprocal for the three components (FP64 division is a long instruction
+    // sequence; the product differs from the quotient by at most an ulp)
+    const double ip4 = (p4 > 0.0) ? 1.0 / p4 : 0.0;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] / p4) * (p2.x + p3.x), (p1[a] / p4) * (p2.y + p3.y))
+        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] * ip4) * (p2.x + p3.x), (p1[a] * ip4) * (p2.y + p3.y))
                                       : make_double2(0.0, 0.0);
         const double2 hom = (a == 0) ? make_double2(f.a13 * u[2].x, f.a13 * u[2].y) : make_double2(0.0, 0.0);
         tot[a] = make_double2(visc[a].x - nl[a].x + pr.x + 0.0 - hom.x, visc[a].y - nl[a].y + pr.y + 0.0 - hom.y);
@@ -182,10 +185,11 @@ __device__ __forceinline__ void contfix_rrot(const BF& f, const double* k, doubl
             if (bex(a, b)) { um[a].x = um[a].x + (f.bm[a][b] * u[b].x); um[a].y = um[a].y + (f.bm[a][b] * u[b].y); }
     const double2 kdu = make_double2(k[0] * um[0].x + k[1] * um[1].x + k[2] * um[2].x,
                                      k[0] * um[0].y + k[1] * um[1].y + k[2] * um[2].y);
+    const double ik2 = 1.0 / kmag2;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        um[a].x = um[a].x - (k[a] * kdu.x / kmag2);
-        um[a].y = um[a].y - (k[a] * kdu.y / kmag2);
+        um[a].x = um[a].x - (k[a] * kdu.x * ik2);
+        um[a].y = um[a].y - (k[a] * kdu.y * ik2);
     }
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -293,9 +297,12 @@ __device__ __forceinline__ void rhs_bf(const BF& f, double nu, const double* k, 
             for (int n = 0; n < 3; n++)
                 if (bex(n, jj)) vc += nu * f.bm[l][jj] * f.bm[n][jj] * k[l] * k[n];
         }
+    // one reciprocal for the three components (FP64 division is a long instruction
+    // sequence; the product differs from the quotient by at most an ulp)
+    const double ip4 = (p4 > 0.0) ? 1.0 / p4 : 0.0;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] / p4) * (p2.x + p3.x), (p1[a] / p4) * (p2.y + p3.y))
+        const double2 pr = (p4 > 0.0) ? make_double2((p1[a] * ip4) * (p2.x + p3.x), (p1[a] * ip4) * (p2.y + p3.y))
                                       : make_double2(0.0, 0.0);
         tot[a] = make_double2(-vc * u[a].x - nl[a].x + pr.x - hom[a].x, -vc * u[a].y - nl[a].y + pr.y - hom[a].y);
     }

@@ -527,6 +527,7 @@ __device__ __forceinline__ void rk_mode(const FieldsT<T>& F, const Geo& g, int s
     const double k1 = (double)i, k2 = wvn(j, g.kj), k3 = wvn(k, g.kk);
     const double kmag2 = (k1 * k1) + (k2 * k2) + (k3 * k3);
     if (!(kmag2 > 0.0)) return;
+    const double ik2 = 1.0 / kmag2;   // the mode's one FP64 division (products below)
     double beta, gamma;
     rk_coeffs(stage, beta, gamma);
     const double dt = F.clock->dt;
@@ -559,19 +560,19 @@ __device__ __forceinline__ void rk_mode(const FieldsT<T>& F, const Geo& g, int s
                                        k1 * fv[0].y + k2 * fv[1].y + k3 * fv[2].y);
 #pragma unroll
                 for (int c = 0; c < 3; c++)
-                    force[c] = mk(fv[c].x - ((kv[c] / kmag2) * kdb.x), fv[c].y - ((kv[c] / kmag2) * kdb.y));
+                    force[c] = mk(fv[c].x - ((kv[c] * ik2) * kdb.x), fv[c].y - ((kv[c] * ik2) * kdb.y));
             }
         }
         if constexpr (FORM == 3) {   // integrating factor: the viscous term leaves the right-hand side
 #pragma unroll
             for (int c = 0; c < 3; c++)
-                tot[c] = mk(-nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
-                            -nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+                tot[c] = mk(-nl[c].x + (kv[c] * ik2) * kdn.x + force[c].x,
+                            -nl[c].y + (kv[c] * ik2) * kdn.y + force[c].y);
         } else {
 #pragma unroll
             for (int c = 0; c < 3; c++)
-                tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] / kmag2) * kdn.x + force[c].x,
-                            -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] / kmag2) * kdn.y + force[c].y);
+                tot[c] = mk(-g.nu * kmag2 * uu[c].x - nl[c].x + (kv[c] * ik2) * kdn.x + force[c].x,
+                            -g.nu * kmag2 * uu[c].y - nl[c].y + (kv[c] * ik2) * kdn.y + force[c].y);
         }
     }
     // Integrating factor (isotropic flow): E = exp(-nu k^2 (c_{s+1} - c_s) dt), c = 0, 1/3,
@@ -603,7 +604,7 @@ __device__ __forceinline__ void rk_mode(const FieldsT<T>& F, const Geo& g, int s
     const double2 kdu = mk(k1 * uu[0].x + k2 * uu[1].x + k3 * uu[2].x, k1 * uu[0].y + k2 * uu[1].y + k3 * uu[2].y);
 #pragma unroll
     for (int c = 0; c < 3; c++)
-        F.u[c][m] = from_d<C>(mk(uu[c].x - (kv[c] * kdu.x / kmag2), uu[c].y - (kv[c] * kdu.y / kmag2)));
+        F.u[c][m] = from_d<C>(mk(uu[c].x - (kv[c] * kdu.x * ik2), uu[c].y - (kv[c] * kdu.y * ik2)));
 }
 
 template <int FORM, class T, int CAP>
