@@ -1,7 +1,7 @@
 """The FP32-mixed form (PANDORA_PREC_FP32_MIXED) against the FP64 oracle.
 
 Fields, transforms and the nonlinear term run in FP32; the boundary stays FP64.
-The bars are the north star's for this form: E(k) within 1e-4 relative of the FP64
+The bars of this form: E(k) within 1e-4 relative of the FP64
 oracle, plus u within 1e-5 relative L2, epsilon within 1e-4 and particle positions
 within 1e-6 (about 10 FP32 roundings of O(1) quantities over a few steps).
 """

@@ -9,7 +9,7 @@ after the small ones):
 * 512^3 homogeneous shear (BF-rot, B110 = 2, 2^18 tracers): 2 steps;
 * 128^3 homogeneous shear with B110 = 2 at dt = 0.002, across its first remesh;
 * 1024^3 forced flow: the FP32-mixed form against the FP64 form of the same seed on
-  the same GPU (the north star's oracle for this configuration), 3 steps;
+  the same GPU (the FP64 form is the reference for this form at this size), 3 steps;
 * the CFL-driven time steps (RK3_TIMESTEP_CFL, and RK3_TIMESTEP_DECIDE for isotropic
   flow, both branches of its cap), src/pf_rk3.f90:3852-3948.
 
@@ -150,7 +150,7 @@ class _DeviceArray:
 
 def test_config3_mixed_1024_against_fp64(gpu_lib):
     """FP32 fields and transforms against the FP64 form of the same seed, 3 steps at
-    1024^3: E(k) within 1e-4 relative (the north star's bar), u within 1e-5 relative L2,
+    1024^3: E(k) within 1e-4 relative (the mixed form's stated bar), u within 1e-5 relative L2,
     epsilon within 1e-4.  u is compared on the device."""
     import torch
     p = gpu_lib.workload_params("iso_forced", 1024)
