@@ -46,6 +46,7 @@ class Request:
     admitted: float | None = None
     done: float | None = None
     result: dict = field(default_factory=dict)
+    key: tuple | None = None       # class_key(params), computed once by the server
 
     @property
     def points(self) -> int:
@@ -211,7 +212,7 @@ class Server:
         return bool(self.members[key]) or any(f[0] == key for f in self.finishing)
 
     def _batch_for(self, req: Request) -> Batch | None:
-        key = class_key(req.params)
+        key = req.key
         b = self.batches.get(key)
         if b is not None:
             return b
@@ -235,24 +236,32 @@ class Server:
 
     def run(self, requests: list[Request], realtime: bool = True) -> dict:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
-        waiting: collections.OrderedDict[int, Request] = collections.OrderedDict()
+        # waiting requests, one arrival-ordered queue per class: an admission pass looks at
+        # each class with waiting requests once (the classes in the order of their oldest
+        # waiting request), not at every waiting request
+        waiting: dict[tuple, collections.deque] = {}
         t0 = time.perf_counter()
         left = len(requests)
         while left:
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 r = pending.popleft()
-                waiting[r.rid] = r
-            # admission: any waiting request whose class has a free slot
-            for rid in list(waiting):
-                r = waiting[rid]
-                b = self._batch_for(r)
-                if b is None or not b.free:
+                if r.key is None:
+                    r.key = class_key(r.params)
+                waiting.setdefault(r.key, collections.deque()).append(r)
+            # admission: waiting requests of classes with a free slot
+            for key in sorted(waiting, key=lambda k: waiting[k][0].arrival):
+                q = waiting[key]
+                b = self._batch_for(q[0])
+                if b is None:
                     continue
-                slot = b.admit(r.params, b.free[0])   # the schedule is the batch's (results do not depend on it)
-                r.admitted = time.perf_counter() - t0
-                self.members[class_key(r.params)][slot] = [r, r.steps]
-                del waiting[rid]
+                while q and b.free:
+                    r = q.popleft()
+                    slot = b.admit(r.params, b.free[0])   # the schedule is the batch's (results do not depend on it)
+                    r.admitted = time.perf_counter() - t0
+                    self.members[key][slot] = [r, r.steps]
+                if not q:
+                    del waiting[key]
             # keep `inflight` step chunks queued per batch; a member's finish follows
             # the chunk that completes it in stream order
             progressed = False
