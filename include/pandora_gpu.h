@@ -116,7 +116,7 @@ typedef struct pandora_params {
     /* nl_particle / nl_part_properties */
     int32_t p_track_part;
     int32_t p_init_type;
-    int64_t p_np_global;
+    int64_t p_np_global;    /* at most 2^31 - 1 (the per-step spatial sort counts in 32 bits) */
     int32_t p_interp_order;
     int32_t p_ts_release;
     double  p_rho;

@@ -577,3 +577,12 @@ def test_x_lines_per_warp_validation(gpu_lib):
     p.x_lines_per_warp = 2
     with pytest.raises(gpu_lib.PandoraError):
         gpu_lib.Simulation(p)
+
+
+def test_particle_count_limit(gpu_lib):
+    """More tracers than the per-step sort's 32-bit offsets can count is refused at create,
+    before any allocation."""
+    p = gpu_lib.workload_params("iso_forced_particles", 32)
+    p.p_np_global = 1 << 31
+    with pytest.raises(gpu_lib.PandoraError):
+        gpu_lib.Simulation(p)
