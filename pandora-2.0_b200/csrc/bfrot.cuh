@@ -219,14 +219,12 @@ __device__ __forceinline__ bool dealias_drop(const Geo& g, const BF& f, double k
 // f_RK3ComputeNonlinearBFRot (src/pf_rk3.f90:1634-1711), pointwise in physical space.
 template <class R>
 __device__ __forceinline__ void nl_bf(const BFT<R>& f, const R* u, const R* om, R* nl) {
-    R n1 = R(0), n2 = R(0), n3 = R(0);
-#pragma unroll
-    for (int m = 0; m < 3; m++) {
-        if (bex(0, m)) { n3 -= om[1] * f.bi[0][m] * u[m]; n2 += om[2] * f.bi[0][m] * u[m]; }
-        if (bex(1, m)) { n1 -= om[2] * f.bi[1][m] * u[m]; n3 += om[0] * f.bi[1][m] * u[m]; }
-        if (bex(2, m)) { n1 += om[1] * f.bi[2][m] * u[m]; n2 -= om[0] * f.bi[2][m] * u[m]; }
-    }
-    nl[0] = n1; nl[1] = n2; nl[2] = n3;
+    // omega x (binv u): the laboratory velocity first (binv has the diagonal and (1,3)),
+    // then the cross product -- the reference's sum over the entries of binv, regrouped
+    const R v0 = f.bi[0][0] * u[0] + f.bi[0][2] * u[2], v1 = f.bi[1][1] * u[1], v2 = f.bi[2][2] * u[2];
+    nl[0] = om[1] * v2 - om[2] * v1;
+    nl[1] = om[2] * v0 - om[0] * v2;
+    nl[2] = om[0] * v1 - om[1] * v0;
 }
 
 // Right-hand side of f_RK3FormFBFRot for F_SHEAR_DNS (src/pf_rk3.f90:2494-2673):

@@ -702,7 +702,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
     const int f = blockIdx.x % nf, i0 = blockIdx.y * LT, j = blockIdx.z;
     const int lmax = g.nkip - i0;   // lines of this tile inside the i padding
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
-    const int KK = g.kk, NKK = g.nkk, nki = g.nki;
+    constexpr int KK = NZ / 3, NKK = 2 * KK + 1;   // g.kk, g.nkk (the 2/3 rule)
+    const int nki = g.nki;
     const double k2 = wvn(j, g.kj);
     const T k2t = (T)k2;
     const long long istride = (long long)g.nkj * NKK;
@@ -880,7 +881,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<double>(), 1) k_zpass_in
         mbar_wait_bounded(ba, 0, kLimit);
         return;
     }
-    const int KK = g.kk;
+    constexpr int KK = NZ / 3;   // g.kk (the 2/3 rule)
     const double k2 = wvn(j, g.kj);
     BF bf;
     if constexpr (FORM == 1 || FORM == 2) bf = make_bf(g, F.clock);
@@ -955,7 +956,7 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
     constexpr int LT = TCfg<NY>::template lines<T>();
     const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % nf;
     const int lmax = g.nkip - i0;
-    const int KJ = g.kj, NKJ = g.nkj;
+    constexpr int KJ = NY / 3, NKJ = 2 * KJ + 1;   // g.kj, g.nkj (the 2/3 rule)
     const long long rs = g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
     C* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
@@ -988,7 +989,7 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
     constexpr int LT = TCfg<NY>::template lines<T>();
     const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % 3;
     const int lmax = g.nkip - i0;
-    const int KJ = g.kj, NKJ = g.nkj;
+    constexpr int KJ = NY / 3, NKJ = 2 * KJ + 1;   // g.kj, g.nkj (the 2/3 rule)
     const long long rs = g.nkip;
     const C* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
     C* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
@@ -1023,7 +1024,8 @@ __global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, tru
     // NL-hat into the y-pencil buffer, or (mode 1) into rk
     Out3<C> nlh;
     for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? F.rk[c] : F.yb + c * g.S;
-    const int KK = g.kk, NKK = g.nkk, nki = g.nki;
+    constexpr int KK = NZ / 3, NKK = 2 * KK + 1;   // g.kk, g.nkk (the 2/3 rule)
+    const int nki = g.nki;
     const long long zs = (long long)g.nkj * g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
     C* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
