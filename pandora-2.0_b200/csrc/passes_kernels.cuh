@@ -165,9 +165,9 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     const bool valid = qw + sub < lines;
     const long long q = valid ? qw + sub : lines - 1;
     C* s = smem + ((size_t)w * LPW + sub) * 3 * XAS;
-    const long long fstride = lines * g.nkip;     // distance between fields in yb
-    const int NKI = g.nki;
-    C* b = F.yb + q * g.nkip;
+    constexpr int NKI = NX / 3 + 1, NKIP = (NKI + 7) / 8 * 8;   // g.nki, g.nkip
+    const long long fstride = lines * NKIP;       // distance between fields in yb
+    C* b = F.yb + q * NKIP;
     BFT<T> bf;
     if (g.shear) bf = bf_as<T>(make_bf(g, F.clock));
     double racc[RS ? kRsSums : 1], rmax[RS ? kRsMax : 1];
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
     // L2, one bulk prefetch per row, while this line's forward transforms run:
     // that CTA's loads then wait on L2 rather than HBM.
     if (pf_lines > 0 && valid && q + pf_lines < lines && lane < 6)
-        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
+        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * NKIP, NKI * sizeof(C));
     // forward transforms of the product arrays; only the band is written
     constexpr int F0 = XP::f0, F1 = XP::f1, F2 = XP::f2, P0 = XP::fused ? 1 : 0;
     if constexpr (NA == 2) {
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(32 * Cfg<NX>::NWX, Cfg<NX>::template minbx<T>(
         for (int a = 0; a < 2; a++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, F0, F1, F2, P0, NP, 0, KB, W>(s + a * XAS, tw, lane);
     }
     const T half = T(0.5);
-    for (int m = lane; m < g.nkip && valid; m += W) {
+    for (int m = lane; m < NKIP && valid; m += W) {
         C n1 = mk(T(0), T(0)), n2 = n1, n3 = n1;
         if (m < NKI) {
             const int mc = (NX - m) % NX;
@@ -374,9 +374,9 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
     const long long q = (long long)blockIdx.x * NW + w;
     if (q >= lines) return;                       // whole warp; no block barrier follows
     C* s = smem_as<C>() + (size_t)w * 4 * XAS;
-    const long long fstride = lines * g.nkip;
-    const int NKI = g.nki;
-    C* b = F.yb + q * g.nkip;
+    constexpr int NKI = NX / 3 + 1, NKIP = (NKI + 7) / 8 * 8;   // g.nki, g.nkip
+    const long long fstride = lines * NKIP;
+    C* b = F.yb + q * NKIP;
     const BFT<T> bf = bf_as<T>(make_bf(g, F.clock));
     // the Hermitian extension of the half spectra of fields fa and fb into array p, as K3;
     // xa, xb: i m times the field (its x derivative)
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         if (threadIdx.x % 32 == 0) atomicMax(&F.clock->ucfl_bits, (unsigned long long)__double_as_longlong((double)umax));
     }
     if (pf_lines > 0 && q + pf_lines < lines && lane < 9)
-        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * g.nkip, NKI * sizeof(C));
+        prefetch_l2(F.yb + lane * fstride + (q + pf_lines) * NKIP, NKI * sizeof(C));
     if constexpr (NA == 2) {
         pdfft::wpasses<NX, -1, 1, XPS, 2, XAS, R0, R1, R2, 0, NP, 0, KB>(s, tw, lane);
     } else {
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(32 * ConvCfg<NX, T>::NW, 1) k_xpass_conv(const
         for (int r = 0; r < 2; r++) pdfft::wpasses<NX, -1, 1, XPS, 1, 0, R0, R1, R2, 0, NP, 0, KB>(s + r * XAS, tw, lane);
     }
     const T half = T(0.5);
-    for (int m = lane; m < g.nkip; m += 32) {
+    for (int m = lane; m < NKIP; m += 32) {
         C n1 = mk(T(0), T(0)), n2 = n1, n3 = n1;
         if (m < NKI) {
             const int mc = (NX - m) % NX;
@@ -1024,8 +1024,7 @@ __global__ void __launch_bounds__(TCfg<NZ, true>::template nt<T>(), TCfg<NZ, tru
     // NL-hat into the y-pencil buffer, or (mode 1) into rk
     Out3<C> nlh;
     for (int c = 0; c < 3; c++) nlh.p[c] = (mode == 1) ? F.rk[c] : F.yb + c * g.S;
-    constexpr int KK = NZ / 3, NKK = 2 * KK + 1;   // g.kk, g.nkk (the 2/3 rule)
-    const int nki = g.nki;
+    const int KK = g.kk, NKK = g.nkk, nki = g.nki;
     const long long zs = (long long)g.nkj * g.nkip;
     const C* __restrict__ src = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
     C* dst = (f == 0 ? nlh.p[0] : (f == 1 ? nlh.p[1] : nlh.p[2])) + ((long long)i0 * g.nkj + j) * NKK;
