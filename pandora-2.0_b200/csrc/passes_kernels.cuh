@@ -682,7 +682,7 @@ template <int N, bool TWO = false> struct TCfg {
 // that each instantiation carries only its own derivative code): 0 isotropic, 1 BF-rot,
 // 2 R-rot, 3 R-conv.  The batched shear forms at 256 points in FP64 ask for one CTA per SM
 // fewer than the others: the member index and frame tensors spilled at five.
-template <int NZ, int FORM, class T, int CAP>
+template <int NZ, int FORM, class T, int CAP, int CN = 0>
 __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
                                   TCfg<NZ>::template minb<T>() - ((CAP > 1 && FORM != 0 && sizeof(T) == 8 && NZ == 256) ? 1 : 0))
     k_zpass_inv(const __grid_constant__ MemberSet<T, CAP> ms, int stage,
@@ -697,17 +697,20 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
     }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
+    // CN > 0: a cubic grid of CN points a side, every size a compile-time constant
+    const int nkj_ = CN ? 2 * (CN / 3) + 1 : g.nkj, kj_ = CN ? CN / 3 : g.kj;
+    const int nki_ = CN ? CN / 3 + 1 : g.nki, nkip_ = CN ? (CN / 3 + 1 + 7) / 8 * 8 : g.nkip;
     C* s = smem_as<C>();
     constexpr int LT = TCfg<NZ>::template lines<T>();
     const int f = blockIdx.x % nf, i0 = blockIdx.y * LT, j = blockIdx.z;
-    const int lmax = g.nkip - i0;   // lines of this tile inside the i padding
+    const int lmax = nkip_ - i0;   // lines of this tile inside the i padding
     if (stage == 1 && f == 0 && blockIdx.y == 0 && j == 0 && threadIdx.x == 0) F.clock->ucfl_bits = 0ull;
     constexpr int KK = NZ / 3, NKK = 2 * KK + 1;   // g.kk, g.nkk (the 2/3 rule)
-    const int nki = g.nki;
-    const double k2 = wvn(j, g.kj);
+    const int nki = nki_;
+    const double k2 = wvn(j, kj_);
     const T k2t = (T)k2;
-    const long long istride = (long long)g.nkj * NKK;
-    const long long row0 = ((long long)i0 * g.nkj + j) * NKK;
+    const long long istride = (long long)nkj_ * NKK;
+    const long long row0 = ((long long)i0 * nkj_ + j) * NKK;
     // velocity: u_f; vorticity omega_{f-3} = i (ka a - kb b): omega1 = i (k2 u3 - k3 u2),
     // omega2 = i (k3 u1 - k1 u3), omega3 = i (k1 u2 - k2 u1).  R-conv: fields 3 + c and
     // 6 + c are d u_c / dy and d u_c / dz (d u_c / dx is formed in the x pass).
@@ -760,8 +763,8 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
             return mk((-ka * a.y) - (-kb * b.y), (ka * a.x) - (kb * b.x));
         }
     };
-    C* dst = F.zb + (((long long)f * NZ) * g.nkj + j) * g.nkip + i0;
-    const long long zs = (long long)g.nkj * g.nkip;
+    C* dst = F.zb + (((long long)f * NZ) * nkj_ + j) * nkip_ + i0;
+    const long long zs = (long long)nkj_ * nkip_;
     auto st = [&](int z, int l, C v) {
         if (LT > 8 && l >= lmax) return;
         dst[z * zs + l] = v;
@@ -773,7 +776,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<T>(),
     const C* const u0 = F.u[0];
     const C* const u1 = F.u[1];
     const C* const u2 = F.u[2];
-    const int nkj = g.nkj;
+    const int nkj = nkj_;
     auto mid = [pf_ctas, nki, nkj, NKK, u0, u1, u2]() {
         if (pf_ctas <= 0) return;
         const long long nblk = (long long)nf * gridDim.y * gridDim.z;
@@ -941,7 +944,7 @@ __global__ void __launch_bounds__(TCfg<NZ>::template nt<double>(), 1) k_zpass_in
 // K2: backward y transforms of field f = blockIdx.z, j zero-padded into
 // [KJ+1, NY-KJ-1] (f_RK3TransformjiFs2Rs, src/pf_rk3.f90:1458-1473).  nf = six fields, or
 // nine in the R-conv form, per member.
-template <int NY, class T, int CAP>
+template <int NY, class T, int CAP, int CN = 0>
 __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_inv(const __grid_constant__ MemberSet<T, CAP> ms,
                                                                                                           int nf) {
     using C = typename FieldsT<T>::C;
@@ -952,14 +955,16 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
     }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
+    // CN > 0: a cubic grid of CN points a side, every size a compile-time constant
+    const int nz_ = CN ? CN : g.nz, nkip_ = CN ? (CN / 3 + 1 + 7) / 8 * 8 : g.nkip;
     C* s = smem_as<C>();
     constexpr int LT = TCfg<NY>::template lines<T>();
     const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % nf;
-    const int lmax = g.nkip - i0;
+    const int lmax = nkip_ - i0;
     constexpr int KJ = NY / 3, NKJ = 2 * KJ + 1;   // g.kj, g.nkj (the 2/3 rule)
-    const long long rs = g.nkip;
-    const C* __restrict__ src = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
-    C* dst = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
+    const long long rs = nkip_;
+    const C* __restrict__ src = F.zb + (((long long)f * nz_ + z) * NKJ) * rs + i0;
+    C* dst = F.yb + (((long long)f * nz_ + z) * NY) * rs + i0;
     auto ld = [&](int y, int l) -> C {
         if (LT > 8 && l >= lmax) return mk(T(0), T(0));
         if (y <= KJ) return src[y * rs + l];
@@ -975,7 +980,7 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
 
 // K4: forward y transforms of NL field f = blockIdx.z, truncated to j
 // (f_RK3TransformjiRs2Fs, src/pf_rk3.f90:1902-1938).
-template <int NY, class T, int CAP>
+template <int NY, class T, int CAP, int CN = 0>
 __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, true>::template minb<T>()) k_ypass_fwd(const __grid_constant__ MemberSet<T, CAP> ms) {
     using C = typename FieldsT<T>::C;
     const Member<T>& mm = ms.m[CAP == 1 ? 0 : blockIdx.z / 3];
@@ -985,14 +990,16 @@ __global__ void __launch_bounds__(TCfg<NY, true>::template nt<T>(), TCfg<NY, tru
     }
     const FieldsT<T> F = mm.F;
     const Geo g = mm.g;
+    // CN > 0: a cubic grid of CN points a side, every size a compile-time constant
+    const int nz_ = CN ? CN : g.nz, nkip_ = CN ? (CN / 3 + 1 + 7) / 8 * 8 : g.nkip;
     C* s = smem_as<C>();
     constexpr int LT = TCfg<NY>::template lines<T>();
     const int i0 = blockIdx.x * LT, z = blockIdx.y, f = blockIdx.z % 3;
-    const int lmax = g.nkip - i0;
+    const int lmax = nkip_ - i0;
     constexpr int KJ = NY / 3, NKJ = 2 * KJ + 1;   // g.kj, g.nkj (the 2/3 rule)
-    const long long rs = g.nkip;
-    const C* __restrict__ src = F.yb + (((long long)f * g.nz + z) * NY) * rs + i0;
-    C* dst = F.zb + (((long long)f * g.nz + z) * NKJ) * rs + i0;
+    const long long rs = nkip_;
+    const C* __restrict__ src = F.yb + (((long long)f * nz_ + z) * NY) * rs + i0;
+    C* dst = F.zb + (((long long)f * nz_ + z) * NKJ) * rs + i0;
     auto ld = [&](int y, int l) -> C {
         if (LT > 8 && l >= lmax) return mk(T(0), T(0));
         return src[y * rs + l];
@@ -1057,6 +1064,16 @@ template <int N> constexpr bool xlpw_len() { return N <= 64; }
 template <int N, class T, int CAP> constexpr int default_xlpw() {
     return CAP > 1 ? (N <= 48 ? 4 : 2) : (N >= 48 ? 2 : 1);
 }
+
+// Lengths whose K1, K2 and K4 have instantiations for cubic grids (every size a
+// compile-time constant, so the index arithmetic folds): FP32-mixed, the benchmark and
+// ensemble sizes.  Measured at 512^3 shear: K1 0.74 -> 0.69, K2 0.70 -> 0.58, K4 0.32 ->
+// 0.30 ms per stage; the FP64 passes, bound by their arithmetic, do not gain.
+template <int N, class T> constexpr bool cube_len() {
+    return std::is_same<T, float>::value && (N == 32 || N == 48 || N == 64 || N == 96 || N == 128 || N == 192 ||
+                                             N == 256 || N == 512 || N == 1024);
+}
+__host__ __device__ inline bool is_cube(const Geo& g, int n) { return g.nx == n && g.ny == n && g.nz == n; }
 
 // Lengths with batched (kBatchChunk-member) instantiations: the ensemble's sizes.
 template <int N> constexpr bool batch_len() {

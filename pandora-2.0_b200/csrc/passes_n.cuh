@@ -31,6 +31,16 @@ template <typename K> static cudaError_t set_smem(K kernel, size_t bytes) {
 // member sets of CAP.
 template <int N, class T, int CAP> static cudaError_t configure_cap(const Geo& g) {
     cudaError_t e;
+    if constexpr (cube_len<N, T>()) {
+        if (is_cube(g, N)) {
+            if ((e = set_smem(k_zpass_inv<N, 0, T, CAP, N>, TCfg<N>::template smem<T>()))) return e;
+            if ((e = set_smem(k_zpass_inv<N, 1, T, CAP, N>, TCfg<N>::template smem<T>()))) return e;
+            if ((e = set_smem(k_zpass_inv<N, 2, T, CAP, N>, TCfg<N>::template smem<T>()))) return e;
+            if ((e = set_smem(k_zpass_inv<N, 3, T, CAP, N>, TCfg<N>::template smem<T>()))) return e;
+            if ((e = set_smem(k_ypass_inv<N, T, CAP, N>, TCfg<N, true>::template smem<T>()))) return e;
+            if ((e = set_smem(k_ypass_fwd<N, T, CAP, N>, TCfg<N, true>::template smem<T>()))) return e;
+        }
+    }
     if (g.nz == N) {
         if ((e = set_smem(k_zpass_inv<N, 0, T, CAP>, TCfg<N>::template smem<T>()))) return e;
         if ((e = set_smem(k_zpass_inv<N, 1, T, CAP>, TCfg<N>::template smem<T>()))) return e;
@@ -98,10 +108,17 @@ cudaError_t zpass_inv_n(const Geo& g, const Member<T>* M, int B, int stage, cuda
                 const long long pf = CAP == 1 ? resident_ctas(kern, NT, sm) : 0;
                 kern<<<grid, NT, sm, st>>>(ms, stage, pf);
             };
-            if (!g.shear) go(k_zpass_inv<N, 0, T, CAP>);
-            else if (!g.rrot) go(k_zpass_inv<N, 1, T, CAP>);
-            else if (!g.rconv) go(k_zpass_inv<N, 2, T, CAP>);
-            else go(k_zpass_inv<N, 3, T, CAP>);
+            auto form = [&](auto cn) {
+                constexpr int CN = decltype(cn)::value;
+                if (!g.shear) go(k_zpass_inv<N, 0, T, CAP, CN>);
+                else if (!g.rrot) go(k_zpass_inv<N, 1, T, CAP, CN>);
+                else if (!g.rconv) go(k_zpass_inv<N, 2, T, CAP, CN>);
+                else go(k_zpass_inv<N, 3, T, CAP, CN>);
+            };
+            if constexpr (cube_len<N, T>()) {
+                if (is_cube(g, N)) { form(std::integral_constant<int, N>{}); return; }
+            }
+            form(std::integral_constant<int, 0>{});
         }
     });
 }
@@ -109,10 +126,15 @@ cudaError_t zpass_inv_n(const Geo& g, const Member<T>* M, int B, int stage, cuda
 template <int N, class T> cudaError_t ypass_inv_n(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
     return for_member_sets(M, B, [&](const auto& ms, int nb) {
         constexpr int CAP = PD_CAP(ms);
-        if constexpr (CAP == 1 || batch_len<N>())
-            k_ypass_inv<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, pass_fields(g) * nb),
-                                     TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(
-                ms, pass_fields(g));
+        if constexpr (CAP == 1 || batch_len<N>()) {
+            const dim3 grid(TCfg<N, true>::template tiles<T>(g), g.nz, pass_fields(g) * nb);
+            constexpr int NT = TCfg<N, true>::template nt<T>();
+            constexpr size_t sm = TCfg<N, true>::template smem<T>();
+            if constexpr (cube_len<N, T>()) {
+                if (is_cube(g, N)) { k_ypass_inv<N, T, CAP, N><<<grid, NT, sm, st>>>(ms, pass_fields(g)); return; }
+            }
+            k_ypass_inv<N, T, CAP><<<grid, NT, sm, st>>>(ms, pass_fields(g));
+        }
     });
 }
 
@@ -169,9 +191,15 @@ template <int N, class T> cudaError_t xpass_stats_n(const Geo& g, const Member<T
 template <int N, class T> cudaError_t ypass_fwd_n(const Geo& g, const Member<T>* M, int B, cudaStream_t st) {
     return for_member_sets(M, B, [&](const auto& ms, int nb) {
         constexpr int CAP = PD_CAP(ms);
-        if constexpr (CAP == 1 || batch_len<N>())
-            k_ypass_fwd<N, T, CAP><<<dim3(TCfg<N, true>::template tiles<T>(g), g.nz, 3 * nb),
-                                     TCfg<N, true>::template nt<T>(), TCfg<N, true>::template smem<T>(), st>>>(ms);
+        if constexpr (CAP == 1 || batch_len<N>()) {
+            const dim3 grid(TCfg<N, true>::template tiles<T>(g), g.nz, 3 * nb);
+            constexpr int NT = TCfg<N, true>::template nt<T>();
+            constexpr size_t sm = TCfg<N, true>::template smem<T>();
+            if constexpr (cube_len<N, T>()) {
+                if (is_cube(g, N)) { k_ypass_fwd<N, T, CAP, N><<<grid, NT, sm, st>>>(ms); return; }
+            }
+            k_ypass_fwd<N, T, CAP><<<grid, NT, sm, st>>>(ms);
+        }
     });
 }
 
