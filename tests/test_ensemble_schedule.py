@@ -31,3 +31,82 @@ def test_committed_table_is_complete():
         for prec in (0, 1):
             entry = table[f"{n}/{prec}"]
             assert entry["best"] == ensemble.pick_capacity(entry["rates"])
+
+
+class _FakeBatch:
+    """Stand-in for pandora.batch.Batch on the host: slots, tickets that complete at once,
+    and a record of which requests each slot held (no device work)."""
+    live = []
+
+    def __init__(self, cls, capacity):
+        self.cls, self.capacity = cls, capacity
+        self.free = list(range(capacity))
+        self.members = {}
+        self.max_members = 0
+        self.admitted = []
+        _FakeBatch.live.append(self)
+
+    def admit(self, p, slot=None):
+        slot = self.free[0] if slot is None else slot
+        self.free.remove(slot)
+        self.members[slot] = p.seed_fluid
+        self.admitted.append(p.seed_fluid)
+        self.max_members = max(self.max_members, len(self.members))
+        return slot
+
+    def step(self, n=1):
+        return 0
+
+    def done(self, ticket):
+        return True
+
+    def finish(self, slot):
+        self.members.pop(slot)
+        return 0
+
+    def reuse(self, slot):
+        self.free.append(slot)
+
+    def result_stats(self, slot):
+        return [0.0], 0.0, 0.0
+
+    def sync(self):
+        pass
+
+    def close(self):
+        pass
+
+
+def test_server_admits_in_arrival_order_within_capacity(monkeypatch):
+    monkeypatch.setattr(ensemble, "Batch", _FakeBatch)
+    _FakeBatch.live = []
+    trace = ensemble.make_trace(60, seed=3, rate=None, steps=20, sizes=(32, 48, 64))
+    caps = {f"{n}/{p}": {"best": 2, "xlpw": 0} for n in (32, 48, 64) for p in (0, 1)}
+    srv = ensemble.Server(1 << 40, caps)
+    res = srv.run(trace, realtime=False)
+    srv.close()
+    assert res["requests"] == len(trace)
+    assert all(r.done is not None and r.admitted is not None for r in trace)
+    by_class = {}
+    for r in sorted(trace, key=lambda r: (r.arrival, r.rid)):
+        by_class.setdefault(r.key, []).append(r.params.seed_fluid)
+    admitted = {}
+    for b in _FakeBatch.live:
+        assert b.max_members <= b.capacity
+        admitted.setdefault(ensemble.class_key(b.cls), []).extend(b.admitted)
+    for key, seeds in by_class.items():   # every request once, first come first served in its class
+        assert admitted[key] == seeds
+
+
+def test_server_keeps_batches_within_budget(monkeypatch):
+    monkeypatch.setattr(ensemble, "Batch", _FakeBatch)
+    _FakeBatch.live = []
+    trace = ensemble.make_trace(40, seed=5, rate=None, steps=10, sizes=(32, 48))
+    caps = {f"{n}/{p}": {"best": 4, "xlpw": 0} for n in (32, 48) for p in (0, 1)}
+    big = max(ensemble.batch_bytes(r.params, 4) for r in trace)
+    srv = ensemble.Server(big + 1, caps)   # room for one batch at a time
+    res = srv.run(trace, realtime=False)
+    srv.close()
+    assert res["requests"] == len(trace) and all(r.done is not None for r in trace)
+    assert res["peak_batch_bytes"] <= big + 1
+    assert len(_FakeBatch.live) > 4      # classes took turns, idle batches closed for others
